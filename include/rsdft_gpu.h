@@ -1,0 +1,157 @@
+/*
+ * rsdft_gpu.h - C ABI of the B200 (sm_100a) Kohn-Sham eigensolver inner loop.
+ *
+ * Drop-in for the real Gamma-point (-D_DRSDFT_) call surfaces of RSDFT
+ * (j-iwata/RSDFT v1.3.0, paths relative to its src/ directory).  The Fortran
+ * side binds these with ISO_C_BINDING (bind(C), scalars by value, arrays as
+ * plain addresses); every entry returns an int status (0 = OK, < 0 = error,
+ * detail in rsdft_gpu_last_error()).
+ *
+ * Conventions
+ *   - Arrays are Fortran column-major; a wavefunction block is (ld x nb)
+ *     doubles, grid index x fastest (kinetic_sol_module.f90:85).
+ *   - Band/k/spin indices are 1-based as in Fortran.  Only k = 1 (Gamma) is
+ *     supported; s selects the spin column of Vloc.
+ *   - A wavefunction pointer may be device memory, a host address inside a
+ *     range registered with rsdft_gpu_register_wf (then its device mirror is
+ *     used and kept current; rsdft_gpu_sync_to_host copies it back), or plain
+ *     host memory (copied in and out around the call).
+ *   - Small arrays (esp, res, occ, Hsub, Vsub, forces, tables) may be host or
+ *     device memory.
+ *   - No entry falls back to a CPU implementation.
+ *   - Not thread-safe; one CUDA stream per process (rsdft_gpu_set_stream).
+ */
+#ifndef RSDFT_GPU_H
+#define RSDFT_GPU_H
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* status codes */
+#define RSDFT_OK 0
+#define RSDFT_EINVAL (-1)    /* bad argument (size, index, NULL) */
+#define RSDFT_ENOTINIT (-2)  /* rsdft_gpu_init / set_grid not called */
+#define RSDFT_ECUDA (-3)     /* CUDA / cuBLAS error */
+#define RSDFT_ESOLVER (-4)   /* cuSOLVER failure or info != 0 (e.g. overlap not SPD) */
+#define RSDFT_ENOMEM (-5)    /* device allocation failed */
+#define RSDFT_EUNSUP (-6)    /* unsupported option (k != 1, Md > 8, ...) */
+
+/* precision modes of the eigensolver entries */
+#define RSDFT_MODE_FP64 0        /* plain all-FP64 form */
+#define RSDFT_MODE_MIXED_BF16 1  /* split-BF16 tensor-core contractions, FP32 CG sweeps */
+#define RSDFT_MODE_MIXED_FP32 2  /* FP32 contractions, FP32 CG sweeps */
+
+/* ---------------------------------------------------------------- set-up */
+
+/* Bind the library to a CUDA device.  (replaces the MPI/OpenMP start-up the
+ * reference does in main.f90:34-60; one rank per GPU) */
+int rsdft_gpu_init(int device);
+int rsdft_gpu_finalize(void);
+const char *rsdft_gpu_last_error(void);
+/* Launch on this cudaStream_t from now on (NULL: the library's own stream). */
+int rsdft_gpu_set_stream(void *stream);
+int rsdft_gpu_synchronize(void);
+/* Number of this library's own kernels launched since it was loaded
+ * (diagnostics; library calls such as cuBLAS are not counted).  (no
+ * reference counterpart; the reference's timers are watch_module.f90) */
+long long rsdft_gpu_kernel_launches(void);
+
+/* Grid and FD kinetic coefficients: Ngrid(1:3), Md, coef_lap0, coef_lap(3,Md)
+ * (axis-major: coef_lap[axis*Md + m-1]), Hgrid(1:3), ggg(1:3), dV.
+ * (replaces init_kinetic, kinetic_module.f90:20-153, and the module state of
+ * kinetic_variables.f90 / rgrid_module read by op_kinetic_sol) */
+int rsdft_gpu_set_grid(const int *ngrid, int md, double coef_lap0, const double *coef_lap,
+                       const double *hgrid, const double *ggg, double dv);
+
+/* Local potential Vloc(ML, nspin).  (replaces Vloc of localpot_module.f90:18-25) */
+int rsdft_gpu_set_vloc(const double *vloc, long ml, int nspin);
+
+/* Nonlocal KB tables in projector-major CSR (0-based): lma_ptr[nzlma+1],
+ * jjp[nnz] (grid index, ascending per projector), uv[nnz], iuv[nzlma] (+-1),
+ * amap[nzlma] (0-based atom), duvdr[nnz*3] (d uV / d R_atom, may be NULL).
+ * (replaces uVk, JJP, MJJ, iuV, amap of ps_nloc2_variables.f90:3-28 filled by
+ * prep_ps_nloc2 / prep_uvk_ps_nloc2, ps_nloc2_module.f90:56-1190, and the
+ * duVdR table of calc_force_ps_nloc2 :1489-1586) */
+int rsdft_gpu_set_nonlocal(int nzlma, const int *lma_ptr, const int *jjp, const double *uv,
+                           const int *iuv, const int *amap, int natom, const double *duvdr);
+
+/* Device mirror of a host wavefunction array unk(ML, MB) (copied in now).
+ * (replaces the residency of wf_module's unk(ML_0:ML_1, MB, MK, MS),
+ * wf_module.f90:118) */
+int rsdft_gpu_register_wf(double *unk, long ml, int mb);
+int rsdft_gpu_unregister_wf(double *unk);
+int rsdft_gpu_sync_to_host(double *unk);
+int rsdft_gpu_sync_to_device(double *unk);
+
+/* ----------------------------------------------------------- hot path */
+
+/* htpsi(n1:n2, ib1:ib2) = H tpsi: FD kinetic + Vloc + nonlocal KB.
+ * (replaces hamiltonian(k,s,tpsi,htpsi,n1,n2,ib1,ib2),
+ * hamiltonian_module.f90:20-72) */
+int rsdft_gpu_hamiltonian(int k, int s, const double *tpsi, double *htpsi, int n1, int n2, int ib1,
+                          int ib2);
+
+/* Band-by-band preconditioned CG, all bands advanced concurrently (exact:
+ * SWGS = 0 keeps bands independent).  ncg line steps, mloop preconditioner
+ * sweeps, ipc = 4 (hprsdft preconditioner) or 0 (none); mode per above.
+ * (replaces conjugate_gradient(n1,n2,MB,k,s,unk,esp,res), cg_module.f90:54-94
+ * -> conjugate_gradient_1 :97-430, preconditioning cgpc_module.f90:126-155 ->
+ * precond_hprsdft cgpc_hprsdft_module.f90:126-263) */
+int rsdft_gpu_conjugate_gradient(int n1, int n2, int mb, int k, int s, double *unk, double *esp,
+                                 double *res, int ncg, int mloop, int ipc, int mode);
+
+/* Orthonormalise unk(:, n0:n1) in the dV metric; the result is the unique Q
+ * of the QR factorisation with positive diag(R), the output of the recursive
+ * blocked Gram-Schmidt.  nblk/nblk1 are accepted for interface parity.
+ * (replaces gram_schmidt(n0,n1,k,s) -> gram_schmidt_t,
+ * gram_schmidt_module.f90:28-56, gram_schmidt_t_module.f90:84-316) */
+int rsdft_gpu_gram_schmidt(int n0, int n1, int k, int s, double *unk, long ld, int nblk, int nblk1,
+                           int mode);
+
+/* Hsub = dV * psi^T (H psi), lower triangle (upper set to zero), MB x MB with
+ * leading dimension ldh.  (replaces subspace_mate_sl(k,s),
+ * subspace_mate_sl_module.f90:27-366, on a 1x1 process grid) */
+int rsdft_gpu_subspace_mate(int k, int s, const double *unk, long ld, int mb, double *hsub, int ldh);
+
+/* Eigen-decomposition of the symmetric Hsub (lower triangle read): esp(MB)
+ * ascending, Vsub(MB, MB) eigenvectors.  (replaces subspace_solv_sl(k,s),
+ * subspace_solv_sl_module.f90:15-134, pdsyevd on a 1x1 grid) */
+int rsdft_gpu_subspace_solv(int mb, const double *hsub, int ldh, double *esp, double *vsub, int ldv);
+
+/* unk <- unk * Vsub.  (replaces subspace_rotv_sl(k,s),
+ * subspace_rotv_sl_module.f90:24-135) */
+int rsdft_gpu_subspace_rotv(int k, int s, double *unk, long ld, int mb, const double *vsub, int ldv);
+
+/* Rayleigh-Ritz in span(unk): Hsub = dV/2 (psi^T H psi + (H psi)^T psi),
+ * eigen-decomposition, rotation; esp(MB) out.  (replaces subspace_diag(k,s)
+ * -> subspace_diag_la, subspace_diag_module.f90:17-25,
+ * subspace_diag_la_module.f90:18-232) */
+int rsdft_gpu_subspace_diag(int k, int s, double *unk, long ld, int mb, double *esp, int mode);
+
+/* Norm-conserving nonlocal force force2(3, MI) (column-major, i.e. xyz of
+ * atom 1 first) for bands with occ(n) != 0.  (replaces
+ * calc_force_ps_nloc2(MI,force2), ps_nloc2_module.f90:1281-1811) */
+int rsdft_gpu_force_nloc(int mi, const double *unk, long ld, int mb, const double *occ,
+                         double *force2);
+
+/* Adjoint (vector-Jacobian product) of hpsi with respect to the local
+ * potential and the atom positions.  For y = H psi and cotangent chi:
+ *   dL_dv[r]    += sum_n chi_n(r) psi_n(r)                     (ML)
+ *   dL_dr[3a+k] += sum_n sum_{lma in a} iuV dV [ (chi.d_k uV)(uV.psi)
+ *                                              + (chi.uV)(d_k uV.psi) ]
+ * If chi == NULL, chi_n = occ[n] * dV * psi_n, which makes the outputs the
+ * gradients of E = sum_n occ_n <psi_n|H|psi_n> dV (then -dL_dr is the
+ * Hellmann-Feynman nonlocal force).  The outputs are overwritten.
+ * (no single reference routine: differentiates op_localpot,
+ * localpot_module.f90:27-81, and op_ps_nloc2_hp, ps_nloc2_op_module.f90:136-270;
+ * the position part is the contraction of calc_force_ps_nloc2,
+ * ps_nloc2_module.f90:1601-1773) */
+int rsdft_gpu_hpsi_adjoint(const double *psi, const double *chi, long ld, int nb, const double *occ,
+                           double *dl_dv, double *dl_dr);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* RSDFT_GPU_H */

@@ -1,0 +1,177 @@
+"""Host-side mirror of RSDFT's eigensolver call surfaces on the B200 library.
+
+Method names, argument order and meaning follow the Fortran routines they
+replace (j-iwata/RSDFT v1.3.0, src/):
+
+====================================  ==========================================
+``RsdftGpu`` method                   reference routine
+====================================  ==========================================
+``hamiltonian(k,s,tpsi,htpsi,...)``   hamiltonian_module.f90:20
+``conjugate_gradient(n1,n2,MB,...)``  cg_module.f90:54
+``gram_schmidt(n0,n1,k,s,unk)``       gram_schmidt_module.f90:28 -> gram_schmidt_t
+``subspace_diag(k,s,unk,esp)``        subspace_diag_module.f90:17 -> subspace_diag_la
+``subspace_mate_sl(k,s,unk,hsub)``    subspace_mate_sl_module.f90:27
+``subspace_solv_sl(hsub,esp,vsub)``   subspace_solv_sl_module.f90:15
+``subspace_rotv_sl(k,s,unk,vsub)``    subspace_rotv_sl_module.f90:24
+``calc_force_ps_nloc2(MI,force2,..)`` ps_nloc2_module.f90:1281
+``hpsi_adjoint(psi, ...)``            (adjoint of op_localpot + op_ps_nloc2_hp)
+====================================  ==========================================
+
+The reference routines read module state (``unk``, ``Vloc``, the projector
+tables, ``occ``); here that state is set once with ``setup(cell)`` and the
+arrays are passed explicitly.  Wavefunction arrays are Fortran-ordered
+``(ML, nb)`` float64: numpy arrays (host) or torch tensors (device or host)
+with strides ``(1, ML)`` (``fortran_empty`` makes one).  Every call raises
+``RsdftError`` on a non-zero status; nothing falls back to the CPU.
+"""
+from __future__ import annotations
+
+import numpy as np
+
+from . import _lib
+from ._lib import RsdftError  # noqa: F401  (re-export)
+
+MODE_FP64 = 0
+MODE_MIXED_BF16 = 1
+MODE_MIXED_FP32 = 2
+
+
+def _is_torch(a) -> bool:
+    return type(a).__module__.startswith("torch")
+
+
+def _ptr(a, *, name="array", shape=None, dtype="float64"):
+    """Address of a numpy array or torch tensor, checking dtype and layout."""
+    if a is None:
+        return None
+    if _is_torch(a):
+        import torch
+
+        want = {"float64": torch.float64, "int32": torch.int32}[dtype]
+        if a.dtype != want:
+            raise TypeError(f"{name}: dtype {a.dtype}, expected {want}")
+        if a.dim() == 2:
+            if not (a.stride(0) == 1 and a.stride(1) >= a.shape[0]):
+                raise ValueError(f"{name}: torch tensor must be Fortran-ordered (ML, nb)")
+        elif not a.is_contiguous():
+            raise ValueError(f"{name}: tensor must be contiguous")
+        return a.data_ptr()
+    if not isinstance(a, np.ndarray):
+        raise TypeError(f"{name}: expected numpy array or torch tensor, got {type(a)}")
+    if a.dtype != np.dtype(dtype):
+        raise TypeError(f"{name}: dtype {a.dtype}, expected {dtype}")
+    if not a.flags.f_contiguous:
+        raise ValueError(f"{name}: array must be Fortran-contiguous")
+    return a.ctypes.data
+
+
+def fortran_empty(ml: int, nb: int, device="cuda", dtype=None):
+    """torch tensor of shape (ml, nb) with column-major strides."""
+    import torch
+
+    return torch.empty((nb, ml), dtype=dtype or torch.float64, device=device).t()
+
+
+def _ld(a) -> int:
+    if _is_torch(a):
+        return int(a.stride(1)) if a.dim() == 2 else int(a.shape[0])
+    return int(a.strides[1] // a.itemsize) if a.ndim == 2 else int(a.shape[0])
+
+
+class RsdftGpu:
+    """One device context of the B200 eigensolver library."""
+
+    def __init__(self, device: int = 0):
+        _lib.call("rsdft_gpu_init", device)
+        self.device = device
+        self.cell = None
+        self._keep = []
+
+    # ----------------------------------------------------------- set-up
+    def setup(self, cell, *, with_forces: bool = True) -> None:
+        """Upload grid, FD weights, Vloc and the projector tables of ``cell``."""
+        ng = np.asarray(cell.ngrid, dtype=np.int32)
+        coef = np.asfortranarray(np.ascontiguousarray(cell.coef_lap).ravel(), dtype=np.float64)
+        h = np.asarray(cell.h, dtype=np.float64)
+        ggg = np.ones(3)
+        _lib.call("rsdft_gpu_set_grid", ng.ctypes.data, cell.md, cell.coef_lap0, coef.ctypes.data, h.ctypes.data,
+                  ggg.ctypes.data, cell.dV)
+        v = np.ascontiguousarray(cell.vloc, dtype=np.float64)
+        _lib.call("rsdft_gpu_set_vloc", v.ctypes.data, cell.ML, 1)
+        lp = np.ascontiguousarray(cell.lma_ptr, dtype=np.int32)
+        jj = np.ascontiguousarray(cell.jjp, dtype=np.int32)
+        uv = np.ascontiguousarray(cell.uv, dtype=np.float64)
+        iu = np.ascontiguousarray(cell.iuv, dtype=np.int32)
+        am = np.ascontiguousarray(cell.amap, dtype=np.int32)
+        duv = np.ascontiguousarray(cell.duv, dtype=np.float64) if with_forces and cell.duv.size else None
+        _lib.call("rsdft_gpu_set_nonlocal", cell.nzlma, lp.ctypes.data, jj.ctypes.data, uv.ctypes.data,
+                  iu.ctypes.data, am.ctypes.data, cell.natom, duv.ctypes.data if duv is not None else None)
+        self.cell = cell
+
+    def set_stream(self, stream) -> None:
+        """Launch on a cudaStream_t (e.g. ``torch.cuda.current_stream().cuda_stream``)."""
+        _lib.call("rsdft_gpu_set_stream", stream)
+
+    def synchronize(self) -> None:
+        _lib.call("rsdft_gpu_synchronize")
+
+    def register_wf(self, unk: np.ndarray) -> None:
+        _lib.call("rsdft_gpu_register_wf", _ptr(unk, name="unk"), unk.shape[0], unk.shape[1])
+        self._keep.append(unk)
+
+    def unregister_wf(self, unk: np.ndarray) -> None:
+        _lib.call("rsdft_gpu_unregister_wf", _ptr(unk, name="unk"))
+
+    def sync_to_host(self, unk: np.ndarray) -> None:
+        _lib.call("rsdft_gpu_sync_to_host", _ptr(unk, name="unk"))
+
+    def sync_to_device(self, unk: np.ndarray) -> None:
+        _lib.call("rsdft_gpu_sync_to_device", _ptr(unk, name="unk"))
+
+    # ---------------------------------------------------------- hot path
+    def hamiltonian(self, k, s, tpsi, htpsi, n1, n2, ib1, ib2) -> None:
+        _lib.call("rsdft_gpu_hamiltonian", k, s, _ptr(tpsi, name="tpsi"), _ptr(htpsi, name="htpsi"), n1, n2, ib1,
+                  ib2)
+
+    def conjugate_gradient(self, n1, n2, MB, k, s, unk, esp, res, *, ncg=3, mloop=3, ipc=4,
+                           mode=MODE_FP64) -> None:
+        """Reference defaults: Ncg = 3 (cg_module.f90:23), mloop = 3, IPC = 4."""
+        _lib.call("rsdft_gpu_conjugate_gradient", n1, n2, MB, k, s, _ptr(unk, name="unk"), _ptr(esp, name="esp"),
+                  _ptr(res, name="res"), ncg, mloop, ipc, mode)
+
+    def gram_schmidt(self, n0, n1, k, s, unk, *, nblk=0, nblk1=4, mode=MODE_FP64) -> None:
+        _lib.call("rsdft_gpu_gram_schmidt", n0, n1, k, s, _ptr(unk, name="unk"), _ld(unk), nblk, nblk1, mode)
+
+    def subspace_diag(self, k, s, unk, esp, *, mode=MODE_FP64) -> None:
+        _lib.call("rsdft_gpu_subspace_diag", k, s, _ptr(unk, name="unk"), _ld(unk), unk.shape[1],
+                  _ptr(esp, name="esp"), mode)
+
+    def subspace_mate_sl(self, k, s, unk, hsub) -> None:
+        _lib.call("rsdft_gpu_subspace_mate", k, s, _ptr(unk, name="unk"), _ld(unk), unk.shape[1],
+                  _ptr(hsub, name="hsub"), _ld(hsub))
+
+    def subspace_solv_sl(self, hsub, esp, vsub) -> None:
+        _lib.call("rsdft_gpu_subspace_solv", hsub.shape[0], _ptr(hsub, name="hsub"), _ld(hsub),
+                  _ptr(esp, name="esp"), _ptr(vsub, name="vsub"), _ld(vsub))
+
+    def subspace_rotv_sl(self, k, s, unk, vsub) -> None:
+        _lib.call("rsdft_gpu_subspace_rotv", k, s, _ptr(unk, name="unk"), _ld(unk), unk.shape[1],
+                  _ptr(vsub, name="vsub"), _ld(vsub))
+
+    def calc_force_ps_nloc2(self, MI, force2, unk, occ) -> None:
+        """force2 is (3, MI) Fortran-ordered (xyz of atom 1 first)."""
+        _lib.call("rsdft_gpu_force_nloc", MI, _ptr(unk, name="unk"), _ld(unk), unk.shape[1],
+                  _ptr(occ, name="occ"), _ptr(force2, name="force2"))
+
+    def hpsi_adjoint(self, psi, *, chi=None, occ=None, dl_dv=None, dl_dr=None) -> None:
+        _lib.call("rsdft_gpu_hpsi_adjoint", _ptr(psi, name="psi"), _ptr(chi, name="chi"), _ld(psi), psi.shape[1],
+                  _ptr(occ, name="occ"), _ptr(dl_dv, name="dl_dv"), _ptr(dl_dr, name="dl_dr"))
+
+    # --------------------------------------------------------- composite
+    def eigensolver_iteration(self, unk, esp, res, *, ncg=4, mloop=3, mode=MODE_FP64) -> None:
+        """One sweep iteration as calc_sweep runs it (sweep_module.f90:150-155):
+        conjugate_gradient -> gram_schmidt -> subspace_diag."""
+        ml, mb = unk.shape
+        self.conjugate_gradient(1, ml, mb, 1, 1, unk, esp, res, ncg=ncg, mloop=mloop, mode=mode)
+        self.gram_schmidt(1, mb, 1, 1, unk, mode=mode)
+        self.subspace_diag(1, 1, unk, esp, mode=mode)

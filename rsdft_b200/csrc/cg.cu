@@ -1,0 +1,563 @@
+// Preconditioned CG eigensolver sweep (conjugate_gradient_1, cg_module.f90:
+// 97-430, with precond_hprsdft, cgpc_hprsdft_module.f90:126-348), all bands
+// at once.  The reference runs bands one after another (MB_d = 1) and, with
+// SWGS = 0 (cggs_module.f90:24-25), a band's update never reads another
+// band, so advancing every band concurrently performs the same arithmetic.
+// Every per-band branch of the reference (early exit, 2x2 eigen-pair choice,
+// sign fix, 1e8 rejection, preconditioner early exit) is kept per band in
+// device arrays; the loop needs no host synchronisation.
+//
+// Vector kernels share one decomposition (CTA = 2048 points of one band) so
+// that dot products leave per-CTA partial sums that k_finish adds in a fixed
+// order: results are bit-reproducible run to run.
+#include <cmath>
+
+#include "common.cuh"
+#include "kernels.cuh"
+
+namespace rsdft {
+
+constexpr int VT = 256;           // threads per vector CTA
+constexpr int VITEMS = 8;         // elements per thread
+constexpr int VCHUNK = VT * VITEMS;
+
+struct CGScal {
+    double *E, *E1, *rb, *gkgk, *res, *u11, *u21, *W, *rr0, *rr1, *pa, *pb, *bk, *dots;
+    int *active, *pc_active, *reject;
+};
+
+template <typename T>
+struct CGVec {
+    T *x, *hx, *hp, *g, *Pg, *p, *r, *q;  // q = preconditioner search direction
+};
+
+// ----------------------------------------------------------- reductions
+__global__ void k_finish(const double* __restrict__ part, int nchunk, int K, int nb, double scale,
+                         double* __restrict__ out, const int* __restrict__ active) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= nb * K) return;
+    int b = i / K, k = i - b * K;
+    if (active && !active[b]) return;
+    const double* p = part + (long)b * nchunk * K + k;
+    double s = 0.0;
+    for (int c = 0; c < nchunk; ++c) s += p[(long)c * K];
+    out[i] = s * scale;
+}
+
+template <int K>
+struct DotPairs {
+    int a[K], b[K];
+};
+
+// K dot products per band among up to 4 vectors, one read of each vector.
+template <typename T, int NV, int K>
+__global__ void __launch_bounds__(VT) k_multidot(const T* v0, const T* v1, const T* v2, const T* v3, long ld,
+                                                 long n, DotPairs<K> pr, double* __restrict__ part,
+                                                 const int* __restrict__ active) {
+    __shared__ double sh[VT / 32];
+    const int b = blockIdx.y;
+    if (active && !active[b]) return;
+    const T* vs[4] = {v0, v1, v2, v3};
+    double acc[K];
+#pragma unroll
+    for (int k = 0; k < K; ++k) acc[k] = 0.0;
+    const long base = (long)blockIdx.x * VCHUNK;
+#pragma unroll
+    for (int it = 0; it < VITEMS; ++it) {
+        const long i = base + it * VT + threadIdx.x;
+        if (i < n) {
+            double v[NV];
+#pragma unroll
+            for (int q = 0; q < NV; ++q) v[q] = (double)vs[q][(long)b * ld + i];
+#pragma unroll
+            for (int k = 0; k < K; ++k) acc[k] = fma(v[pr.a[k]], v[pr.b[k]], acc[k]);
+        }
+    }
+#pragma unroll
+    for (int k = 0; k < K; ++k) {
+        double s = block_sum<VT>(acc[k], sh);
+        if (threadIdx.x == 0) part[((long)b * gridDim.x + blockIdx.x) * K + k] = s;
+    }
+}
+
+// g = -c1 (hx - E x); partial |g|^2 (cg_module.f90:186-190)
+template <typename T>
+__global__ void __launch_bounds__(VT) k_cg_g(CGVec<T> v, long ld, long n, const double* __restrict__ E,
+                                             double* __restrict__ part, const int* __restrict__ active) {
+    __shared__ double sh[VT / 32];
+    const int b = blockIdx.y;
+    if (active && !active[b]) return;
+    const double e = E[b];
+    double acc = 0.0;
+    const long base = (long)blockIdx.x * VCHUNK, off = (long)b * ld;
+#pragma unroll
+    for (int it = 0; it < VITEMS; ++it) {
+        const long i = base + it * VT + threadIdx.x;
+        if (i < n) {
+            const T g = (T)(-2.0) * (v.hx[off + i] - (T)e * v.x[off + i]);
+            v.g[off + i] = g;
+            acc = fma((double)g, (double)g, acc);
+        }
+    }
+    double s = block_sum<VT>(acc, sh);
+    if (threadIdx.x == 0) part[(long)b * gridDim.x + blockIdx.x] = s;
+}
+
+// 7-point operator of precond_cg_mat2_omp at point i (E0 = 0)
+template <typename T>
+__device__ __forceinline__ T pc_apply(const T* __restrict__ f, long i, int n1, int n2, int n3, T d, T c1, T c2,
+                                      T c3) {
+    const long pl = (long)n1 * n2;
+    const int i1 = (int)(i % n1);
+    const int i2 = (int)((i / n1) % n2);
+    const int i3 = (int)(i / pl);
+    const long xm = i1 == 0 ? i + n1 - 1 : i - 1, xp = i1 == n1 - 1 ? i - n1 + 1 : i + 1;
+    const long ym = i2 == 0 ? i + pl - n1 : i - n1, yp = i2 == n2 - 1 ? i - pl + n1 : i + n1;
+    const long zm = i3 == 0 ? i + pl * (n3 - 1) : i - pl, zp = i3 == n3 - 1 ? i - pl * (n3 - 1) : i + pl;
+    T v = d * f[i];
+    v = v + c1 * (__ldg(f + xp) + __ldg(f + xm)) + c2 * (__ldg(f + yp) + __ldg(f + ym)) +
+        c3 * (__ldg(f + zp) + __ldg(f + zm));
+    return v;
+}
+
+struct PcArgs {
+    int n1, n2, n3;
+    double d, c1, c2, c3;
+};
+
+// P0: Pg = g; r = g - A g; q = r; partial |r|^2  (cgpc_hprsdft_module.f90:161-175)
+template <typename T>
+__global__ void __launch_bounds__(VT) k_pc0(CGVec<T> v, long ld, long n, PcArgs pa, double* __restrict__ part,
+                                            const int* __restrict__ active) {
+    __shared__ double sh[VT / 32];
+    const int b = blockIdx.y;
+    if (active && !active[b]) return;
+    const long off = (long)b * ld, base = (long)blockIdx.x * VCHUNK;
+    const T* g = v.g + off;
+    double acc = 0.0;
+#pragma unroll
+    for (int it = 0; it < VITEMS; ++it) {
+        const long i = base + it * VT + threadIdx.x;
+        if (i < n) {
+            const T gi = g[i];
+            const T f = pc_apply<T>(g, i, pa.n1, pa.n2, pa.n3, (T)pa.d, (T)pa.c1, (T)pa.c2, (T)pa.c3);
+            const T r = gi - f;
+            v.Pg[off + i] = gi;
+            v.r[off + i] = r;
+            v.q[off + i] = r;
+            acc = fma((double)r, (double)r, acc);
+        }
+    }
+    double s = block_sum<VT>(acc, sh);
+    if (threadIdx.x == 0) part[(long)b * gridDim.x + blockIdx.x] = s;
+}
+
+// P1: ft = A q; partial q.ft  (ft stored in hp, which is free until hpsi(p))
+template <typename T>
+__global__ void __launch_bounds__(VT) k_pc1(CGVec<T> v, long ld, long n, PcArgs pa, double* __restrict__ part,
+                                            const int* __restrict__ active) {
+    __shared__ double sh[VT / 32];
+    const int b = blockIdx.y;
+    if (active && !active[b]) return;
+    const long off = (long)b * ld, base = (long)blockIdx.x * VCHUNK;
+    const T* q = v.q + off;
+    double acc = 0.0;
+#pragma unroll
+    for (int it = 0; it < VITEMS; ++it) {
+        const long i = base + it * VT + threadIdx.x;
+        if (i < n) {
+            const T f = pc_apply<T>(q, i, pa.n1, pa.n2, pa.n3, (T)pa.d, (T)pa.c1, (T)pa.c2, (T)pa.c3);
+            v.hp[off + i] = f;
+            acc = fma((double)q[i], (double)f, acc);
+        }
+    }
+    double s = block_sum<VT>(acc, sh);
+    if (threadIdx.x == 0) part[(long)b * gridDim.x + blockIdx.x] = s;
+}
+
+// P2: Pg += a q; (not last) r -= a ft; partial |r|^2
+template <typename T>
+__global__ void __launch_bounds__(VT) k_pc2(CGVec<T> v, long ld, long n, const double* __restrict__ pa_,
+                                            int last, double* __restrict__ part, const int* __restrict__ active) {
+    __shared__ double sh[VT / 32];
+    const int b = blockIdx.y;
+    if (active && !active[b]) return;
+    const long off = (long)b * ld, base = (long)blockIdx.x * VCHUNK;
+    const T a = (T)pa_[b];
+    double acc = 0.0;
+#pragma unroll
+    for (int it = 0; it < VITEMS; ++it) {
+        const long i = base + it * VT + threadIdx.x;
+        if (i < n) {
+            const T qi = v.q[off + i];
+            v.Pg[off + i] = v.Pg[off + i] + a * qi;
+            if (!last) {
+                const T r = v.r[off + i] - a * v.hp[off + i];
+                v.r[off + i] = r;
+                acc = fma((double)r, (double)r, acc);
+            }
+        }
+    }
+    if (!last) {
+        double s = block_sum<VT>(acc, sh);
+        if (threadIdx.x == 0) part[(long)b * gridDim.x + blockIdx.x] = s;
+    }
+}
+
+// P3: q = r + b q
+template <typename T>
+__global__ void __launch_bounds__(VT) k_pc3(CGVec<T> v, long ld, long n, const double* __restrict__ pb_,
+                                            const int* __restrict__ active) {
+    const int b = blockIdx.y;
+    if (active && !active[b]) return;
+    const long off = (long)b * ld, base = (long)blockIdx.x * VCHUNK;
+    const T bb = (T)pb_[b];
+#pragma unroll
+    for (int it = 0; it < VITEMS; ++it) {
+        const long i = base + it * VT + threadIdx.x;
+        if (i < n) v.q[off + i] = v.r[off + i] + bb * v.q[off + i];
+    }
+}
+
+// p = Pg + bk p (icg > 1) or p = Pg (cg_module.f90:247-261)
+template <typename T>
+__global__ void __launch_bounds__(VT) k_cg_p(CGVec<T> v, long ld, long n, const double* __restrict__ bk_,
+                                             int first, const int* __restrict__ active) {
+    const int b = blockIdx.y;
+    if (active && !active[b]) return;
+    const long off = (long)b * ld, base = (long)blockIdx.x * VCHUNK;
+    const T bk = (T)bk_[b];
+#pragma unroll
+    for (int it = 0; it < VITEMS; ++it) {
+        const long i = base + it * VT + threadIdx.x;
+        if (i < n) v.p[off + i] = first ? v.Pg[off + i] : v.Pg[off + i] + bk * v.p[off + i];
+    }
+}
+
+// hx = u11 hx + u21 hp; g = -c1 (hx - W (u11 x + u21 p)); partial |g|^2 (:337-347)
+template <typename T>
+__global__ void __launch_bounds__(VT) k_cg_upd1(CGVec<T> v, long ld, long n, CGScal s, double* __restrict__ part,
+                                                const int* __restrict__ active) {
+    __shared__ double sh[VT / 32];
+    const int b = blockIdx.y;
+    if (active && !active[b]) return;
+    const long off = (long)b * ld, base = (long)blockIdx.x * VCHUNK;
+    const T u11 = (T)s.u11[b], u21 = (T)s.u21[b], w = (T)s.W[b];
+    double acc = 0.0;
+#pragma unroll
+    for (int it = 0; it < VITEMS; ++it) {
+        const long i = base + it * VT + threadIdx.x;
+        if (i < n) {
+            const T hx = u11 * v.hx[off + i] + u21 * v.hp[off + i];
+            v.hx[off + i] = hx;
+            const T g = (T)(-2.0) * (hx - w * (u11 * v.x[off + i] + u21 * v.p[off + i]));
+            v.g[off + i] = g;
+            acc = fma((double)g, (double)g, acc);
+        }
+    }
+    double r = block_sum<VT>(acc, sh);
+    if (threadIdx.x == 0) part[(long)b * gridDim.x + blockIdx.x] = r;
+}
+
+// x = u11 x + u21 p unless rejected (:366-369)
+template <typename T>
+__global__ void __launch_bounds__(VT) k_cg_upd2(CGVec<T> v, long ld, long n, CGScal s,
+                                                const int* __restrict__ active) {
+    const int b = blockIdx.y;
+    if (active && !active[b]) return;
+    if (s.reject[b]) return;
+    const long off = (long)b * ld, base = (long)blockIdx.x * VCHUNK;
+    const T u11 = (T)s.u11[b], u21 = (T)s.u21[b];
+#pragma unroll
+    for (int it = 0; it < VITEMS; ++it) {
+        const long i = base + it * VT + threadIdx.x;
+        if (i < n) v.x[off + i] = u11 * v.x[off + i] + u21 * v.p[off + i];
+    }
+}
+
+// ---------------------------------------------------- per-band scalars
+__global__ void s_init(CGScal s, int nb) {
+    int b = blockIdx.x * blockDim.x + threadIdx.x;
+    if (b >= nb) return;
+    s.E1[b] = 1e10;
+    s.gkgk[b] = 0.0;
+    s.active[b] = 1;
+    s.reject[b] = 0;
+    s.res[b] = 0.0;
+}
+
+// top of the icg loop (cg_module.f90:205-219)
+__global__ void s_top(CGScal s, int nb, int last) {
+    int b = blockIdx.x * blockDim.x + threadIdx.x;
+    if (b >= nb || !s.active[b]) return;
+    const double rb = s.rb[b];
+    s.res[b] = rb / 4.0;
+    if (rb < 0.0 || fabs(s.E[b] - s.E1[b]) < 1e-15 || last) s.active[b] = 0;
+}
+
+__global__ void s_pc0(CGScal s, int nb) {
+    int b = blockIdx.x * blockDim.x + threadIdx.x;
+    if (b >= nb) return;
+    s.pc_active[b] = s.active[b] && !(s.rr1[b] < 1e-24);
+}
+
+__global__ void s_pc1(CGScal s, int nb) {  // rr0 = rr1; a = rr0/pAp (pAp in dots[b])
+    int b = blockIdx.x * blockDim.x + threadIdx.x;
+    if (b >= nb || !s.pc_active[b]) return;
+    s.rr0[b] = s.rr1[b];
+    s.pa[b] = s.rr0[b] / s.dots[b];
+}
+
+__global__ void s_pc2(CGScal s, int nb) {  // b = rr1/rr0
+    int b = blockIdx.x * blockDim.x + threadIdx.x;
+    if (b >= nb || !s.pc_active[b]) return;
+    s.pb[b] = s.rr1[b] / s.rr0[b];
+}
+
+__global__ void s_p(CGScal s, int nb, int first) {  // bk = rb/gkgk; gkgk = rb
+    int b = blockIdx.x * blockDim.x + threadIdx.x;
+    if (b >= nb || !s.active[b]) return;
+    s.bk[b] = first ? 0.0 : s.rb[b] / s.gkgk[b];
+    s.gkgk[b] = s.rb[b];
+}
+
+// Smallest-eigenvalue pair of the 2x2 pencil (A, B), B = U^T U, B-normalised.
+// Closed form: Cholesky of B, C = U^-T A U^-1, symmetric 2x2 eigen-pairs
+// with the cancellation-free root and the better-conditioned eigenvector
+// formula, back-transform x = U^-1 z.
+__device__ void eig2(double a11, double a12, double a22, double b11, double b12, double b22, double* W,
+                     double* X /* 2x2 column-major */, int* info) {
+    *info = 0;
+    if (!(b11 > 0.0)) { *info = 1; return; }
+    const double u11 = sqrt(b11), u12 = b12 / u11, t = b22 - u12 * u12;
+    if (!(t > 0.0)) { *info = 2; return; }
+    const double u22 = sqrt(t);
+    const double c11 = a11 / b11;
+    const double r12 = a12 / u11;
+    const double c12 = (r12 - c11 * u12) / u22;
+    const double c22 = (a22 - 2.0 * u12 * r12 + u12 * u12 * c11) / (u22 * u22);
+    const double m = 0.5 * (c11 + c22), d = 0.5 * (c11 - c22);
+    const double rt = hypot(d, c12);
+    const double det = c11 * c22 - c12 * c12;
+    double lo, hi;
+    if (m > 0.0) { hi = m + rt; lo = det / hi; }
+    else if (m < 0.0) { lo = m - rt; hi = det / lo; }
+    else { lo = -rt; hi = rt; }
+    double z0, z1;
+    if (rt == 0.0) {
+        z0 = 1.0; z1 = 0.0;
+    } else {
+        // eigenvector of lo: (c12, lo - c11) or (lo - c22, c12), the larger one
+        const double p0 = c12, p1 = lo - c11, q0 = lo - c22, q1 = c12;
+        if (p0 * p0 + p1 * p1 >= q0 * q0 + q1 * q1) { z0 = p0; z1 = p1; } else { z0 = q0; z1 = q1; }
+        const double nz = hypot(z0, z1);
+        z0 /= nz; z1 /= nz;
+    }
+    // second pair orthogonal in the reduced space
+    const double y0 = -z1, y1 = z0;
+    W[0] = lo; W[1] = hi;
+    X[1] = z1 / u22; X[0] = (z0 - u12 * X[1]) / u11;
+    X[3] = y1 / u22; X[2] = (y0 - u12 * X[3]) / u11;
+}
+
+// 2x2 Rayleigh-Ritz, pair choice and sign fix (cg_module.f90:299-333)
+__global__ void s_eig(CGScal s, int nb) {
+    int b = blockIdx.x * blockDim.x + threadIdx.x;
+    if (b >= nb || !s.active[b]) return;
+    const double* v = s.dots + 6L * b;  // xx, px, pp, xHx, pHx, pHp
+    double W[2], X[4];
+    int info;
+    eig2(v[3], v[4], v[5], v[0], v[1], v[2], W, X, &info);
+    if (info != 0) {  // B not positive definite: keep x (no update)
+        W[0] = s.E[b]; X[0] = 1.0; X[1] = 0.0;
+    } else if (fabs(W[0] - s.E[b]) > 1e-1 && fabs(W[1] - s.E[b]) <= 1e-1) {
+        X[0] = X[2]; X[1] = X[3]; W[0] = W[1];
+    }
+    if (X[0] < 0.0) { X[0] = -X[0]; X[1] = -X[1]; }
+    s.E1[b] = s.E[b];
+    s.E[b] = W[0];
+    s.W[b] = W[0];
+    s.u11[b] = X[0];
+    s.u21[b] = X[1];
+}
+
+__global__ void s_rej(CGScal s, int nb) {  // cg_module.f90:359-365
+    int b = blockIdx.x * blockDim.x + threadIdx.x;
+    if (b >= nb || !s.active[b]) return;
+    s.reject[b] = 0;
+    if (s.rb[b] / s.res[b] > 1e8) {
+        s.E[b] = s.E1[b];
+        s.reject[b] = 1;
+    }
+}
+
+template <typename T>
+__global__ void k_convert(const double* __restrict__ a, T* __restrict__ b, long n) {
+    long i = (long)blockIdx.x * blockDim.x + threadIdx.x;
+    for (; i < n; i += (long)gridDim.x * blockDim.x) b[i] = (T)a[i];
+}
+
+template <typename T>
+__global__ void k_convert_back(const T* __restrict__ a, double* __restrict__ b, long n) {
+    long i = (long)blockIdx.x * blockDim.x + threadIdx.x;
+    for (; i < n; i += (long)gridDim.x * blockDim.x) b[i] = (double)a[i];
+}
+
+// ------------------------------------------------------------ driver
+template <typename T>
+static int cg_run(T* x, long ld, int mb, int spin, double* esp, double* res, int ncg, int mloop, int ipc) {
+    Context& c = ctx();
+    cudaStream_t st = c.stream;
+    const long n = c.ml;
+    const int nchunk = div_up(n, VCHUNK);
+    const size_t vec = (size_t)ld * mb;
+    CGVec<T> v{};
+    v.x = x;
+    T* base = nullptr;
+    RS_CHECK(workspace_t("cg_vec", vec * 7, &base));
+    v.hx = base;
+    v.hp = base + vec;
+    v.g = base + 2 * vec;
+    v.Pg = base + 3 * vec;
+    v.p = base + 4 * vec;
+    v.r = base + 5 * vec;
+    v.q = base + 6 * vec;
+    double* scal = nullptr;
+    RS_CHECK(workspace_t("cg_scal", (size_t)mb * 20, &scal));
+    CGScal s{};
+    s.E = scal; s.E1 = scal + mb; s.rb = scal + 2 * mb; s.gkgk = scal + 3 * mb; s.res = scal + 4 * mb;
+    s.u11 = scal + 5 * mb; s.u21 = scal + 6 * mb; s.W = scal + 7 * mb; s.rr0 = scal + 8 * mb;
+    s.rr1 = scal + 9 * mb; s.pa = scal + 10 * mb; s.pb = scal + 11 * mb; s.bk = scal + 12 * mb;
+    s.dots = scal + 13 * mb;  // 6 per band
+    int* flags = nullptr;
+    RS_CHECK(workspace_t("cg_flags", (size_t)mb * 3, &flags));
+    s.active = flags; s.pc_active = flags + mb; s.reject = flags + 2 * mb;
+    double* part = nullptr;
+    RS_CHECK(workspace_t("cg_part", (size_t)mb * nchunk * 6, &part));
+
+    const dim3 vg(nchunk, mb);
+    const int sb = div_up(mb, 128);
+    const double dV = c.dV;
+    PcArgs pa{c.n1, c.n2, c.n3, c.pc.c - 0.0, c.pc.c1, c.pc.c2, c.pc.c3};
+    auto finish = [&](int K, double scale, double* out, const int* act) {
+        launch(k_finish, div_up((long)mb * K, 128), 128, 0, st, part, nchunk, K, mb, scale, out, act);
+    };
+
+    launch(s_init, sb, 128, 0, st, s, mb);
+    RS_CHECK(hpsi_device<T>(x, v.hx, ld, mb, spin, nullptr));
+    {
+        DotPairs<1> pr{{0}, {1}};
+        launch(k_multidot<T, 2, 1>, vg, VT, 0, st, x, v.hx, nullptr, nullptr, ld, n, pr, part, nullptr);
+        finish(1, dV, s.E, nullptr);
+    }
+    launch(k_cg_g<T>, vg, VT, 0, st, v, ld, n, s.E, part, nullptr);
+    finish(1, dV, s.rb, nullptr);
+    RS_LAUNCH();
+
+    for (int icg = 1; icg <= ncg + 1; ++icg) {
+        const int last = icg == ncg + 1;
+        launch(s_top, sb, 128, 0, st, s, mb, last);
+        if (last) break;
+        // --- preconditioning (Pgk = gk on entry)
+        if (ipc == 4 && mloop > 0) {
+            launch(k_pc0<T>, vg, VT, 0, st, v, ld, n, pa, part, s.active);
+            finish(1, 1.0, s.rr1, s.active);
+            launch(s_pc0, sb, 128, 0, st, s, mb);
+            for (int il = 1; il <= mloop; ++il) {
+                launch(k_pc1<T>, vg, VT, 0, st, v, ld, n, pa, part, s.pc_active);
+                finish(1, 1.0, s.dots, s.pc_active);
+                launch(s_pc1, sb, 128, 0, st, s, mb);
+                const int lastl = il == mloop;
+                launch(k_pc2<T>, vg, VT, 0, st, v, ld, n, s.pa, lastl, part, s.pc_active);
+                if (lastl) break;
+                finish(1, 1.0, s.rr1, s.pc_active);
+                launch(s_pc2, sb, 128, 0, st, s, mb);
+                launch(k_pc3<T>, vg, VT, 0, st, v, ld, n, s.pb, s.pc_active);
+            }
+        } else {
+            RS_CUDA(cudaMemcpyAsync(v.Pg, v.g, vec * sizeof(T), cudaMemcpyDeviceToDevice, st));
+        }
+        RS_LAUNCH();
+        // --- rb = <Pg|g> dV; search direction
+        {
+            DotPairs<1> pr{{0}, {1}};
+            launch(k_multidot<T, 2, 1>, vg, VT, 0, st, v.Pg, v.g, nullptr, nullptr, ld, n, pr, part, s.active);
+            finish(1, dV, s.rb, s.active);
+        }
+        launch(s_p, sb, 128, 0, st, s, mb, icg == 1);
+        launch(k_cg_p<T>, vg, VT, 0, st, v, ld, n, s.bk, icg == 1, s.active);
+        RS_LAUNCH();
+        RS_CHECK(hpsi_device<T>(v.p, v.hp, ld, mb, spin, s.active));
+        // --- six dots: <x|x>, <p|x>, <p|p>, <x|Hx>, <p|Hx>, <p|Hp>
+        {
+            DotPairs<6> pr{{0, 1, 1, 0, 1, 1}, {0, 0, 1, 2, 2, 3}};
+            launch(k_multidot<T, 4, 6>, vg, VT, 0, st, x, v.p, v.hx, v.hp, ld, n, pr, part, s.active);
+            finish(6, dV, s.dots, s.active);
+        }
+        launch(s_eig, sb, 128, 0, st, s, mb);
+        launch(k_cg_upd1<T>, vg, VT, 0, st, v, ld, n, s, part, s.active);
+        finish(1, dV, s.rb, s.active);
+        launch(s_rej, sb, 128, 0, st, s, mb);
+        launch(k_cg_upd2<T>, vg, VT, 0, st, v, ld, n, s, s.active);
+        RS_LAUNCH();
+    }
+    RS_CUDA(cudaMemcpyAsync(esp, s.E, sizeof(double) * mb, cudaMemcpyDeviceToDevice, st));
+    RS_CUDA(cudaMemcpyAsync(res, s.res, sizeof(double) * mb, cudaMemcpyDeviceToDevice, st));
+    return RSDFT_OK;
+}
+
+int cg_device(double* unk, long ld, int mb, int spin, double* esp, double* res, int ncg, int mloop, int ipc,
+              int mode) {
+    if (mode == RSDFT_MODE_FP64) return cg_run<double>(unk, ld, mb, spin, esp, res, ncg, mloop, ipc);
+    Context& c = ctx();
+    float* x32 = nullptr;
+    const long n = ld * (long)mb;
+    RS_CHECK(workspace_t("cg_x32", (size_t)n, &x32));
+    launch(k_convert<float>, 4 * c.num_sms, 256, 0, c.stream, unk, x32, n);
+    RS_LAUNCH();
+    RS_CHECK(cg_run<float>(x32, ld, mb, spin, esp, res, ncg, mloop, ipc));
+    launch(k_convert_back<float>, 4 * c.num_sms, 256, 0, c.stream, x32, unk, n);
+    RS_LAUNCH();
+    return RSDFT_OK;
+}
+
+}  // namespace rsdft
+
+using namespace rsdft;
+
+extern "C" int rsdft_gpu_conjugate_gradient(int n1, int n2, int mb, int k, int s, double* unk, double* esp,
+                                            double* res, int ncg, int mloop, int ipc, int mode) {
+    RS_CHECK(require_grid());
+    Context& c = ctx();
+    if (k != 1) {
+        set_error("conjugate_gradient: only k=1 (Gamma) is supported");
+        return RSDFT_EUNSUP;
+    }
+    if (s < 1 || s > c.nspin) {
+        set_error("conjugate_gradient: s=%d outside 1..%d", s, c.nspin);
+        return RSDFT_EINVAL;
+    }
+    const long ld = (long)n2 - n1 + 1;
+    if (ld != c.ml || mb < 1 || mb > 65535 || ncg < 0 || !esp || !res) {
+        set_error("conjugate_gradient: bad sizes (ld=%ld ML=%ld MB=%d Ncg=%d)", ld, c.ml, mb, ncg);
+        return RSDFT_EINVAL;
+    }
+    if (ipc != 0 && ipc != 4) {
+        set_error("conjugate_gradient: ipc=%d unsupported (0 or 4)", ipc);
+        return RSDFT_EUNSUP;
+    }
+    if (mode < 0 || mode > 2) {
+        set_error("conjugate_gradient: mode=%d unknown", mode);
+        return RSDFT_EINVAL;
+    }
+    double *du, *desp, *dres;
+    bool su;
+    RS_CHECK(wf_acquire(unk, ld, mb, "cg_unk", &du, &su));
+    RS_CHECK(workspace_t("cg_out", (size_t)2 * mb, &desp));
+    dres = desp + mb;
+    RS_CHECK(cg_device(du, ld, mb, s, desp, dres, ncg, mloop, ipc, mode));
+    RS_CHECK(stage_out(esp, desp, sizeof(double) * mb));
+    RS_CHECK(stage_out(res, dres, sizeof(double) * mb));
+    RS_CHECK(wf_release(unk, du, ld, mb, su));
+    return RSDFT_OK;
+}

@@ -1,0 +1,185 @@
+// Shared state of the RSDFT B200 library: device context, workspace,
+// host-pointer registry and error reporting.  One context per process; the
+// library is not thread-safe (one CUDA stream per context).
+#pragma once
+
+#include <cuda_runtime.h>
+#include <cublas_v2.h>
+#include <cusolverDn.h>
+
+#include <cstdint>
+#include <cstdio>
+#include <map>
+#include <string>
+#include <utility>
+#include <vector>
+
+#include "../../include/rsdft_gpu.h"
+
+namespace rsdft {
+
+constexpr int MAXMD = 8;
+
+struct StencilCoef {
+    double c0;            // coef_lap0 + const_k2 (Gamma: const_k2 = 0)
+    double cx[MAXMD];     // coef_lap(1, m)
+    double cy[MAXMD];     // coef_lap(2, m)
+    double cz[MAXMD];     // coef_lap(3, m)
+};
+
+struct PrecondCoef {
+    double c, c1, c2, c3;  // precond_cg_mat2_omp operator
+};
+
+struct Buf {
+    void* p = nullptr;
+    size_t bytes = 0;
+};
+
+struct WfReg {
+    char* host = nullptr;
+    size_t bytes = 0;
+    char* dev = nullptr;
+};
+
+struct Context {
+    bool init = false;
+    int device = -1;
+    cudaStream_t stream = nullptr;
+    bool own_stream = false;
+    cublasHandle_t blas = nullptr;
+    cusolverDnHandle_t solver = nullptr;
+    int num_sms = 0;
+
+    // grid
+    bool grid_set = false;
+    int n1 = 0, n2 = 0, n3 = 0, md = 0;
+    long ml = 0;
+    double dV = 0.0;
+    double hgrid[3] = {0, 0, 0};
+    StencilCoef sc{};
+    PrecondCoef pc{};
+
+    // local potential (ml x nspin)
+    int nspin = 0;
+    double* vloc = nullptr;
+    float* vloc32 = nullptr;
+
+    // nonlocal tables
+    bool nl_set = false;
+    int nzlma = 0, natom = 0;
+    long nnz = 0;
+    int* lma_ptr = nullptr;     // nzlma+1
+    int* jjp = nullptr;         // nnz
+    double* uv = nullptr;       // nnz
+    float* uv32 = nullptr;
+    int* iuv = nullptr;         // nzlma
+    int* amap = nullptr;        // nzlma
+    double* duv = nullptr;      // nnz x 3 (row-major)
+    int ngroup = 0;             // sphere groups: consecutive lma sharing one point list
+    int* grp_lma0 = nullptr;    // ngroup
+    int* grp_cnt = nullptr;     // ngroup
+    int* pt_ptr = nullptr;      // ml+1: point-major CSR of the scatter
+    int* pt_lma = nullptr;      // nnz
+    double* pt_uv = nullptr;    // nnz
+    float* pt_uv32 = nullptr;
+    std::vector<int> h_amap;
+
+    // workspace
+    std::map<std::string, Buf> ws;
+    std::vector<WfReg> regs;
+};
+
+Context& ctx();
+
+// ---------------------------------------------------------------- errors
+void set_error(const char* fmt, ...);
+const char* get_error();
+
+#define RS_CUDA(call)                                                                 \
+    do {                                                                              \
+        cudaError_t _e = (call);                                                      \
+        if (_e != cudaSuccess) {                                                      \
+            ::rsdft::set_error("%s:%d %s: %s", __FILE__, __LINE__, #call,             \
+                               cudaGetErrorString(_e));                               \
+            return RSDFT_ECUDA;                                                       \
+        }                                                                             \
+    } while (0)
+
+#define RS_BLAS(call)                                                                 \
+    do {                                                                              \
+        cublasStatus_t _s = (call);                                                   \
+        if (_s != CUBLAS_STATUS_SUCCESS) {                                            \
+            ::rsdft::set_error("%s:%d %s: cublas status %d", __FILE__, __LINE__,     \
+                               #call, (int)_s);                                       \
+            return RSDFT_ECUDA;                                                       \
+        }                                                                             \
+    } while (0)
+
+#define RS_SOLVER(call)                                                               \
+    do {                                                                              \
+        cusolverStatus_t _s = (call);                                                 \
+        if (_s != CUSOLVER_STATUS_SUCCESS) {                                          \
+            ::rsdft::set_error("%s:%d %s: cusolver status %d", __FILE__, __LINE__,   \
+                               #call, (int)_s);                                       \
+            return RSDFT_ESOLVER;                                                     \
+        }                                                                             \
+    } while (0)
+
+#define RS_CHECK(expr)                                                                \
+    do {                                                                              \
+        int _r = (expr);                                                              \
+        if (_r != RSDFT_OK) return _r;                                                \
+    } while (0)
+
+#define RS_LAUNCH()                                                                   \
+    do {                                                                              \
+        cudaError_t _e = cudaGetLastError();                                          \
+        if (_e != cudaSuccess) {                                                      \
+            ::rsdft::set_error("%s:%d launch: %s", __FILE__, __LINE__,                \
+                               cudaGetErrorString(_e));                               \
+            return RSDFT_ECUDA;                                                       \
+        }                                                                             \
+    } while (0)
+
+// Number of this library's kernel launches since load (diagnostics).
+extern long long g_kernel_launches;
+
+// Launch one of this library's kernels and count it.
+template <typename... KArgs, typename... Args>
+inline void launch(void (*kernel)(KArgs...), dim3 grid, dim3 block, size_t smem, cudaStream_t st, Args&&... args) {
+    ++g_kernel_launches;
+    kernel<<<grid, block, smem, st>>>(std::forward<Args>(args)...);
+}
+
+int require_init();
+int require_grid();
+
+// ------------------------------------------------------------ workspace
+// Named device buffer, grown (never shrunk) on demand; contents undefined.
+int workspace(const char* name, size_t bytes, void** out);
+template <typename T>
+inline int workspace_t(const char* name, size_t count, T** out) {
+    return workspace(name, count * sizeof(T), reinterpret_cast<void**>(out));
+}
+
+// ------------------------------------------------- pointer resolution
+// Classify a caller pointer: device memory is used directly; a host pointer
+// inside a registered wavefunction range maps onto its device mirror.
+// Returns 1 if *dev was set (device-visible), 0 if p is plain host memory.
+int resolve(const void* p, void** dev);
+
+// Stage a small caller array onto the device (copy if host), and back.
+int stage_in(const void* host_or_dev, size_t bytes, const char* wsname, void** dev);
+int stage_out(void* host_or_dev, const void* dev, size_t bytes);
+
+// Wavefunction block (ld x nb doubles) as a device pointer; copies host data
+// in if the pointer is neither device memory nor registered.  *staged tells
+// the caller to copy results back with wf_release.
+int wf_acquire(const double* p, long ld, int nb, const char* wsname, double** dev, bool* staged,
+               bool copy_in = true);
+int wf_release(double* p, const double* dev, long ld, int nb, bool staged);
+
+inline int div_up(long a, long b) { return (int)((a + b - 1) / b); }
+
+}  // namespace rsdft

@@ -1,0 +1,247 @@
+// Dense tall-skinny steps of the eigensolver iteration.
+//
+// Gram-Schmidt (gram_schmidt_t_module.f90:84-316) is a recursive blocked
+// classical Gram-Schmidt in the dV metric.  Its output is the unique Q of
+// psi = Q R with dV Q^T Q = I and diag(R) > 0.  CholeskyQR2 computes the same
+// Q from one Gram matrix, one Cholesky factor and one triangular solve per
+// pass (two passes): all the work is in two tall-skinny BLAS-3 calls.
+//
+// Subspace diagonalisation follows subspace_diag_la (subspace_diag_la_module
+// .f90:18-232): Hsub = dV/2 (psi^T H psi + (H psi)^T psi) (dsyr2k), symmetric
+// eigen-decomposition (syevd) and the rotation psi V (dgemm).  The mate /
+// solv / rotv entries cover the ScaLAPACK route on a 1x1 process grid
+// (subspace_mate_sl, subspace_solv_sl, subspace_rotv_sl).
+//
+// FP64 form: cuBLAS DSYRK/DSYR2K/DGEMM/DTRSM and cuSOLVER DPOTRF/DSYEVD.
+// Mixed forms: the contractions go to the split-BF16 / FP32 tensor-core
+// kernels of mixed.cu, FP64 stays in Cholesky and the eigensolve.
+#include "common.cuh"
+#include "kernels.cuh"
+#include "mixed.cuh"
+
+namespace rsdft {
+
+__global__ void k_zero_upper(double* a, int n, int lda) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;  // row
+    int j = blockIdx.y;                              // column
+    if (i < n && i < j) a[(long)j * lda + i] = 0.0;
+}
+
+static int check_info(int* dinfo, const char* what) {
+    int h = 0;
+    RS_CUDA(cudaMemcpyAsync(&h, dinfo, sizeof(int), cudaMemcpyDeviceToHost, ctx().stream));
+    RS_CUDA(cudaStreamSynchronize(ctx().stream));
+    if (h != 0) {
+        set_error("%s: info=%d", what, h);
+        return RSDFT_ESOLVER;
+    }
+    return RSDFT_OK;
+}
+
+// one CholeskyQR pass in FP64: S = dV psi^T psi = R^T R, psi <- psi R^-1
+static int cholqr_fp64(double* psi, long ld, int nb, double* S, int* dinfo) {
+    Context& c = ctx();
+    const double zero = 0.0, one = 1.0, dv = c.dV;
+    RS_BLAS(cublasDsyrk(c.blas, CUBLAS_FILL_MODE_UPPER, CUBLAS_OP_T, nb, (int)c.ml, &dv, psi, (int)ld, &zero, S,
+                        nb));
+    int lwork = 0;
+    RS_SOLVER(cusolverDnDpotrf_bufferSize(c.solver, CUBLAS_FILL_MODE_UPPER, nb, S, nb, &lwork));
+    double* work = nullptr;
+    RS_CHECK(workspace_t("gs_potrf", (size_t)lwork + 1, &work));
+    RS_SOLVER(cusolverDnDpotrf(c.solver, CUBLAS_FILL_MODE_UPPER, nb, S, nb, work, lwork, dinfo));
+    RS_BLAS(cublasDtrsm(c.blas, CUBLAS_SIDE_RIGHT, CUBLAS_FILL_MODE_UPPER, CUBLAS_OP_N, CUBLAS_DIAG_NON_UNIT,
+                        (int)c.ml, nb, &one, S, nb, psi, (int)ld));
+    return RSDFT_OK;
+}
+
+int gram_schmidt_device(double* psi, long ld, int nb, int mode) {
+    Context& c = ctx();
+    double* S = nullptr;
+    int* dinfo = nullptr;
+    RS_CHECK(workspace_t("gs_S", (size_t)nb * nb, &S));
+    RS_CHECK(workspace_t("gs_info", 4, &dinfo));
+    if (mode == RSDFT_MODE_FP64) {
+        RS_CHECK(cholqr_fp64(psi, ld, nb, S, dinfo));
+        RS_CHECK(check_info(dinfo, "gram_schmidt: overlap Cholesky (pass 1)"));
+        RS_CHECK(cholqr_fp64(psi, ld, nb, S, dinfo));
+        RS_CHECK(check_info(dinfo, "gram_schmidt: overlap Cholesky (pass 2)"));
+        return RSDFT_OK;
+    }
+    RS_CHECK(cholqr_mixed(psi, ld, nb, mode, S, dinfo));
+    RS_CHECK(check_info(dinfo, "gram_schmidt: overlap Cholesky (mixed pass 1)"));
+    RS_CHECK(cholqr_mixed(psi, ld, nb, mode, S, dinfo));
+    RS_CHECK(check_info(dinfo, "gram_schmidt: overlap Cholesky (mixed pass 2)"));
+    (void)c;
+    return RSDFT_OK;
+}
+
+// symmetric eigensolve in place: A (n x n, lda n) -> eigenvectors, W ascending
+static int syevd(double* A, int n, double* W, cublasFillMode_t uplo, const char* what) {
+    Context& c = ctx();
+    int lwork = 0;
+    RS_SOLVER(cusolverDnDsyevd_bufferSize(c.solver, CUSOLVER_EIG_MODE_VECTOR, uplo, n, A, n, W, &lwork));
+    double* work = nullptr;
+    int* dinfo = nullptr;
+    RS_CHECK(workspace_t("syevd_work", (size_t)lwork + 1, &work));
+    RS_CHECK(workspace_t("syevd_info", 4, &dinfo));
+    RS_SOLVER(cusolverDnDsyevd(c.solver, CUSOLVER_EIG_MODE_VECTOR, uplo, n, A, n, W, work, lwork, dinfo));
+    return check_info(dinfo, what);
+}
+
+int subspace_diag_device(double* psi, long ld, int mb, int spin, double* esp, int mode) {
+    Context& c = ctx();
+    double *hpsi = nullptr, *H = nullptr;
+    RS_CHECK(workspace_t("sub_hpsi", (size_t)ld * mb, &hpsi));
+    RS_CHECK(workspace_t("sub_H", (size_t)mb * mb, &H));
+    const double zero = 0.0, one = 1.0, half_dv = 0.5 * c.dV;
+    if (mode == RSDFT_MODE_FP64) {
+        RS_CHECK(hpsi_device<double>(psi, hpsi, ld, mb, spin, nullptr));
+        RS_BLAS(cublasDsyr2k(c.blas, CUBLAS_FILL_MODE_UPPER, CUBLAS_OP_T, mb, (int)c.ml, &half_dv, psi, (int)ld,
+                             hpsi, (int)ld, &zero, H, mb));
+        RS_CHECK(syevd(H, mb, esp, CUBLAS_FILL_MODE_UPPER, "subspace_diag: syevd"));
+        RS_BLAS(cublasDgemm(c.blas, CUBLAS_OP_N, CUBLAS_OP_N, (int)c.ml, mb, mb, &one, psi, (int)ld, H, mb, &zero,
+                            hpsi, (int)ld));
+    } else {
+        RS_CHECK(subspace_matrix_mixed(psi, hpsi, ld, mb, spin, mode, H));
+        RS_CHECK(syevd(H, mb, esp, CUBLAS_FILL_MODE_UPPER, "subspace_diag: syevd"));
+        RS_CHECK(rotate_mixed(psi, hpsi, ld, mb, H, mode));
+    }
+    RS_CUDA(cudaMemcpy2DAsync(psi, ld * sizeof(double), hpsi, ld * sizeof(double), c.ml * sizeof(double), mb,
+                              cudaMemcpyDeviceToDevice, c.stream));
+    return RSDFT_OK;
+}
+
+}  // namespace rsdft
+
+using namespace rsdft;
+
+static int check_k_s(int k, int s, const char* who) {
+    if (k != 1) {
+        set_error("%s: only k=1 (Gamma) is supported", who);
+        return RSDFT_EUNSUP;
+    }
+    if (s < 1 || s > ctx().nspin) {
+        set_error("%s: s=%d outside 1..%d", who, s, ctx().nspin);
+        return RSDFT_EINVAL;
+    }
+    return RSDFT_OK;
+}
+
+extern "C" {
+
+int rsdft_gpu_gram_schmidt(int n0, int n1, int k, int s, double* unk, long ld, int nblk, int nblk1, int mode) {
+    RS_CHECK(require_grid());
+    (void)nblk;
+    (void)nblk1;
+    (void)s;
+    Context& c = ctx();
+    if (k != 1) {
+        set_error("gram_schmidt: only k=1 (Gamma) is supported");
+        return RSDFT_EUNSUP;
+    }
+    const int nb = n1 - n0 + 1;
+    if (n0 < 1 || nb < 1 || ld < c.ml || !unk || mode < 0 || mode > 2) {
+        set_error("gram_schmidt: bad arguments (n0=%d n1=%d ld=%ld)", n0, n1, ld);
+        return RSDFT_EINVAL;
+    }
+    if (nb > c.ml) {
+        set_error("gram_schmidt: %d bands exceed %ld grid points", nb, c.ml);
+        return RSDFT_EINVAL;
+    }
+    double* base = unk + (long)(n0 - 1) * ld;
+    double* d;
+    bool st;
+    RS_CHECK(wf_acquire(base, ld, nb, "gs_unk", &d, &st));
+    RS_CHECK(gram_schmidt_device(d, ld, nb, mode));
+    RS_CHECK(wf_release(base, d, ld, nb, st));
+    return RSDFT_OK;
+}
+
+int rsdft_gpu_subspace_mate(int k, int s, const double* unk, long ld, int mb, double* hsub, int ldh) {
+    RS_CHECK(require_grid());
+    RS_CHECK(check_k_s(k, s, "subspace_mate"));
+    Context& c = ctx();
+    if (ld < c.ml || mb < 1 || ldh < mb || !hsub) {
+        set_error("subspace_mate: bad arguments");
+        return RSDFT_EINVAL;
+    }
+    double *d, *hpsi, *H;
+    bool st;
+    RS_CHECK(wf_acquire(unk, ld, mb, "mate_unk", &d, &st));
+    RS_CHECK(workspace_t("sub_hpsi", (size_t)ld * mb, &hpsi));
+    RS_CHECK(workspace_t("sub_H", (size_t)mb * mb, &H));
+    RS_CHECK(hpsi_device<double>(d, hpsi, ld, mb, s, nullptr));
+    const double zero = 0.0, dv = c.dV;
+    RS_BLAS(cublasDgemm(c.blas, CUBLAS_OP_T, CUBLAS_OP_N, mb, mb, (int)c.ml, &dv, d, (int)ld, hpsi, (int)ld, &zero,
+                        H, mb));
+    launch(k_zero_upper, dim3(div_up(mb, 128), mb), 128, 0, c.stream, H, mb, mb);
+    RS_LAUNCH();
+    RS_CUDA(cudaMemcpy2DAsync(hsub, (size_t)ldh * sizeof(double), H, (size_t)mb * sizeof(double),
+                              (size_t)mb * sizeof(double), mb, cudaMemcpyDefault, c.stream));
+    RS_CUDA(cudaStreamSynchronize(c.stream));
+    return RSDFT_OK;
+}
+
+int rsdft_gpu_subspace_solv(int mb, const double* hsub, int ldh, double* esp, double* vsub, int ldv) {
+    RS_CHECK(require_init());
+    Context& c = ctx();
+    if (mb < 1 || ldh < mb || ldv < mb || !hsub || !esp || !vsub) {
+        set_error("subspace_solv: bad arguments");
+        return RSDFT_EINVAL;
+    }
+    double *H, *W;
+    RS_CHECK(workspace_t("solv_H", (size_t)mb * mb, &H));
+    RS_CHECK(workspace_t("solv_W", (size_t)mb, &W));
+    RS_CUDA(cudaMemcpy2DAsync(H, (size_t)mb * sizeof(double), hsub, (size_t)ldh * sizeof(double),
+                              (size_t)mb * sizeof(double), mb, cudaMemcpyDefault, c.stream));
+    RS_CHECK(syevd(H, mb, W, CUBLAS_FILL_MODE_LOWER, "subspace_solv: syevd"));
+    RS_CUDA(cudaMemcpy2DAsync(vsub, (size_t)ldv * sizeof(double), H, (size_t)mb * sizeof(double),
+                              (size_t)mb * sizeof(double), mb, cudaMemcpyDefault, c.stream));
+    RS_CUDA(cudaMemcpyAsync(esp, W, sizeof(double) * mb, cudaMemcpyDefault, c.stream));
+    RS_CUDA(cudaStreamSynchronize(c.stream));
+    return RSDFT_OK;
+}
+
+int rsdft_gpu_subspace_rotv(int k, int s, double* unk, long ld, int mb, const double* vsub, int ldv) {
+    RS_CHECK(require_grid());
+    RS_CHECK(check_k_s(k, s, "subspace_rotv"));
+    Context& c = ctx();
+    if (ld < c.ml || mb < 1 || ldv < mb || !vsub) {
+        set_error("subspace_rotv: bad arguments");
+        return RSDFT_EINVAL;
+    }
+    double *d, *V, *tmp;
+    bool st;
+    RS_CHECK(wf_acquire(unk, ld, mb, "rotv_unk", &d, &st));
+    RS_CHECK(workspace_t("rotv_V", (size_t)mb * mb, &V));
+    RS_CHECK(workspace_t("sub_hpsi", (size_t)ld * mb, &tmp));
+    RS_CUDA(cudaMemcpy2DAsync(V, (size_t)mb * sizeof(double), vsub, (size_t)ldv * sizeof(double),
+                              (size_t)mb * sizeof(double), mb, cudaMemcpyDefault, c.stream));
+    const double zero = 0.0, one = 1.0;
+    RS_BLAS(cublasDgemm(c.blas, CUBLAS_OP_N, CUBLAS_OP_N, (int)c.ml, mb, mb, &one, d, (int)ld, V, mb, &zero, tmp,
+                        (int)ld));
+    RS_CUDA(cudaMemcpy2DAsync(d, ld * sizeof(double), tmp, ld * sizeof(double), c.ml * sizeof(double), mb,
+                              cudaMemcpyDeviceToDevice, c.stream));
+    RS_CHECK(wf_release(unk, d, ld, mb, st));
+    return RSDFT_OK;
+}
+
+int rsdft_gpu_subspace_diag(int k, int s, double* unk, long ld, int mb, double* esp, int mode) {
+    RS_CHECK(require_grid());
+    RS_CHECK(check_k_s(k, s, "subspace_diag"));
+    Context& c = ctx();
+    if (ld < c.ml || mb < 1 || !esp || mode < 0 || mode > 2) {
+        set_error("subspace_diag: bad arguments");
+        return RSDFT_EINVAL;
+    }
+    double *d, *W;
+    bool st;
+    RS_CHECK(wf_acquire(unk, ld, mb, "sd_unk", &d, &st));
+    RS_CHECK(workspace_t("sd_W", (size_t)mb, &W));
+    RS_CHECK(subspace_diag_device(d, ld, mb, s, W, mode));
+    RS_CHECK(stage_out(esp, W, sizeof(double) * mb));
+    RS_CHECK(wf_release(unk, d, ld, mb, st));
+    return RSDFT_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,42 @@
+// Internal (C++) entry points shared between the library's translation units.
+#pragma once
+
+#include "common.cuh"
+
+namespace rsdft {
+
+// H psi for nb bands of leading dimension ld (device pointers).  Bands with
+// band_active[b] == 0 are skipped (output left untouched).
+template <typename T>
+int hpsi_device(const T* psi, T* hpsi, long ld, int nb, int spin, const int* band_active);
+
+// Deterministic block sum (fixed shuffle tree + fixed warp order).  All
+// threads of the block must call it; the result is valid in thread 0.
+template <int NT>
+__device__ __forceinline__ double block_sum(double v, double* sh /* >= NT/32 doubles */) {
+#pragma unroll
+    for (int s = 16; s > 0; s >>= 1) v += __shfl_xor_sync(0xffffffffu, v, s);
+    const int w = threadIdx.x >> 5, l = threadIdx.x & 31;
+    if (l == 0) sh[w] = v;
+    __syncthreads();
+    double r = 0.0;
+    if (threadIdx.x == 0) {
+#pragma unroll
+        for (int i = 0; i < NT / 32; ++i) r += sh[i];
+    }
+    __syncthreads();
+    return r;
+}
+
+// Symmetric-positive-definite orthonormalisation (CholeskyQR2 in the dV
+// metric) of nb columns, FP64 (cuBLAS/cuSOLVER) or mixed (tensor cores).
+int gram_schmidt_device(double* psi, long ld, int nb, int mode);
+
+// Rayleigh-Ritz (subspace_diag_la) on device data.
+int subspace_diag_device(double* psi, long ld, int mb, int spin, double* esp_dev, int mode);
+
+// CG over all bands (device data).
+int cg_device(double* unk, long ld, int mb, int spin, double* esp_dev, double* res_dev, int ncg, int mloop,
+              int ipc, int mode);
+
+}  // namespace rsdft

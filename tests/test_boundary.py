@@ -1,0 +1,60 @@
+"""The C-ABI boundary on the CPU: the library loads, exports every symbol the
+header declares, the binding table matches the header, and entries fail with a
+status (not a crash) when no device is bound."""
+import ctypes
+import os
+import re
+
+import pytest
+
+from rsdft_b200 import _lib, build
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+HEADER = os.path.join(ROOT, "include", "rsdft_gpu.h")
+
+
+def declared():
+    txt = open(HEADER).read()
+    txt = re.sub(r"/\*.*?\*/", "", txt, flags=re.S)
+    return sorted(set(re.findall(r"\b(rsdft_gpu_\w+)\s*\(", txt)))
+
+
+@pytest.fixture(scope="module")
+def lib():
+    build.build()
+    return ctypes.CDLL(build.LIB)
+
+
+def test_header_declares_entries():
+    names = declared()
+    assert "rsdft_gpu_hamiltonian" in names and "rsdft_gpu_conjugate_gradient" in names
+    assert len(names) >= 20
+
+
+def test_library_exports_all_declared(lib):
+    for n in declared():
+        assert hasattr(lib, n), f"{n} declared in rsdft_gpu.h but not exported"
+
+
+def test_binding_table_matches_header():
+    assert sorted(_lib.SIGNATURES) == declared()
+
+
+def test_calls_without_context_fail_cleanly(lib):
+    L = _lib.load()
+    rc = L.rsdft_gpu_hamiltonian(1, 1, None, None, 1, 10, 1, 1)
+    assert rc == -2  # ENOTINIT
+    assert b"rsdft_gpu_init" in L.rsdft_gpu_last_error()
+    rc = L.rsdft_gpu_conjugate_gradient(1, 10, 1, 1, 1, None, None, None, 4, 3, 4, 0)
+    assert rc == -2
+
+
+def test_init_reports_missing_device(lib):
+    import torch
+
+    if torch.cuda.is_available():
+        pytest.skip("a device is present")
+    L = _lib.load()
+    rc = L.rsdft_gpu_init(0)
+    assert rc in (-1, -3)
+    assert len(L.rsdft_gpu_last_error()) > 0
