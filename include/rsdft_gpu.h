@@ -36,6 +36,7 @@ extern "C" {
 #define RSDFT_ESOLVER (-4)   /* cuSOLVER failure or info != 0 (e.g. overlap not SPD) */
 #define RSDFT_ENOMEM (-5)    /* device allocation failed */
 #define RSDFT_EUNSUP (-6)    /* unsupported option (k != 1, Md > 8, ...) */
+#define RSDFT_ETIMEOUT (-7)  /* a kernel's bounded wait ran out (reported at the next sync) */
 
 /* precision modes of the eigensolver entries */
 #define RSDFT_MODE_FP64 0        /* plain all-FP64 form */
@@ -51,6 +52,8 @@ int rsdft_gpu_finalize(void);
 const char *rsdft_gpu_last_error(void);
 /* Launch on this cudaStream_t from now on (NULL: the library's own stream). */
 int rsdft_gpu_set_stream(void *stream);
+/* Wait for the stream; reports RSDFT_ETIMEOUT if a kernel aborted on a
+ * bounded wait since the last check. */
 int rsdft_gpu_synchronize(void);
 /* Number of this library's own kernels launched since it was loaded
  * (diagnostics; library calls such as cuBLAS are not counted).  (no

@@ -41,7 +41,7 @@ SIGNATURES = {
     "rsdft_gpu_hpsi_adjoint": (_c_int, [_vp, _vp, _c_long, _c_int, _vp, _vp, _vp]),
 }
 
-STATUS = {0: "OK", -1: "EINVAL", -2: "ENOTINIT", -3: "ECUDA", -4: "ESOLVER", -5: "ENOMEM", -6: "EUNSUP"}
+STATUS = {0: "OK", -1: "EINVAL", -2: "ENOTINIT", -3: "ECUDA", -4: "ESOLVER", -5: "ENOMEM", -6: "EUNSUP", -7: "ETIMEOUT"}
 
 _lib = None
 

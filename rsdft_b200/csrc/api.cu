@@ -177,6 +177,8 @@ int rsdft_gpu_init(int device) {
     RS_SOLVER(cusolverDnCreate(&c.solver));
     RS_SOLVER(cusolverDnSetStream(c.solver, c.stream));
     RS_CUDA(cudaDeviceGetAttribute(&c.num_sms, cudaDevAttrMultiProcessorCount, device));
+    RS_CUDA(cudaMalloc(&c.err_flag, 16));
+    RS_CUDA(cudaMemset(c.err_flag, 0, 16));
     c.device = device;
     c.init = true;
     return RSDFT_OK;
@@ -191,8 +193,9 @@ int rsdft_gpu_finalize(void) {
     c.ws.clear();
     for (auto& r : c.regs) cudaFree(r.dev);
     c.regs.clear();
-    void* ptrs[] = {c.vloc, c.vloc32, c.lma_ptr, c.jjp, c.uv, c.uv32, c.iuv, c.amap, c.duv,
-                    c.grp_lma0, c.grp_cnt, c.pt_ptr, c.pt_lma, c.pt_uv, c.pt_uv32};
+    void* ptrs[] = {c.err_flag, c.vloc, c.vloc32, c.lma_ptr, c.jjp, c.uv, c.uv32, c.iuv, c.amap, c.duv,
+                    c.grp_lma0, c.grp_cnt, c.pt_ptr, c.pt_lma, c.pt_uv, c.pt_uv32,
+                    c.gpt_ptr, c.gpt_grp, c.gpt_uv4, c.gpt_uv4_32};
     for (void* p : ptrs)
         if (p) cudaFree(p);
     if (c.blas) cublasDestroy(c.blas);
@@ -228,6 +231,13 @@ int rsdft_gpu_set_stream(void* stream) {
 int rsdft_gpu_synchronize(void) {
     RS_CHECK(require_init());
     RS_CUDA(cudaStreamSynchronize(g_ctx.stream));
+    int flag = 0;
+    RS_CUDA(cudaMemcpy(&flag, g_ctx.err_flag, sizeof(int), cudaMemcpyDeviceToHost));
+    if (flag) {
+        RS_CUDA(cudaMemset(g_ctx.err_flag, 0, sizeof(int)));
+        set_error("a kernel's bounded wait for a bulk copy ran out (code %d)", flag);
+        return RSDFT_ETIMEOUT;
+    }
     return RSDFT_OK;
 }
 
@@ -357,6 +367,29 @@ int rsdft_gpu_set_nonlocal(int nzlma, const int* lma_ptr, const int* jjp, const 
             plma[q] = l;
             puv[q] = huv[j];
         }
+    // the same scatter per sphere group: one entry per (point, group) holding
+    // the group's (up to 4) projector values at that point
+    std::vector<int> gcnt(c.ml + 1, 0);
+    for (size_t g = 0; g < g0.size(); ++g)
+        for (int j = hptr[g0[g]]; j < hptr[g0[g] + 1]; ++j) gcnt[hjjp[j] + 1]++;
+    std::partial_sum(gcnt.begin(), gcnt.end(), gcnt.begin());
+    const long ngnnz = gcnt[c.ml];
+    std::vector<int> gpos(gcnt.begin(), gcnt.end() - 1), ggrp(ngnnz);
+    std::vector<double> guv((size_t)ngnnz * 4, 0.0);
+    for (size_t g = 0; g < g0.size(); ++g) {
+        const int l0 = g0[g];
+        for (int j = hptr[l0]; j < hptr[l0 + 1]; ++j) {
+            const int q = gpos[hjjp[j]]++;
+            ggrp[q] = l0;
+            for (int k = 0; k < gc[g]; ++k) guv[(size_t)q * 4 + k] = huv[hptr[l0 + k] + (j - hptr[l0])];
+        }
+    }
+    gcnt.resize(c.ml + 8, gcnt[c.ml]);  // padding for vector reads past the end
+    std::vector<float> guv32(guv.begin(), guv.end());
+    RS_CHECK(upload(&c.gpt_ptr, gcnt.data(), gcnt.size()));
+    RS_CHECK(upload(&c.gpt_grp, ggrp.data(), ggrp.size()));
+    RS_CHECK(upload(&c.gpt_uv4, guv.data(), guv.size()));
+    RS_CHECK(upload(&c.gpt_uv4_32, guv32.data(), guv32.size()));
     std::vector<float> huv32(huv.begin(), huv.end()), puv32(puv.begin(), puv.end());
     RS_CHECK(upload(&c.lma_ptr, hptr.data(), hptr.size()));
     RS_CHECK(upload(&c.jjp, hjjp.data(), hjjp.size()));

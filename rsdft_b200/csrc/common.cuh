@@ -50,6 +50,7 @@ struct Context {
     cublasHandle_t blas = nullptr;
     cusolverDnHandle_t solver = nullptr;
     int num_sms = 0;
+    int* err_flag = nullptr;  // set by kernels whose bounded waits ran out
 
     // grid
     bool grid_set = false;
@@ -83,6 +84,10 @@ struct Context {
     int* pt_lma = nullptr;      // nnz
     double* pt_uv = nullptr;    // nnz
     float* pt_uv32 = nullptr;
+    int* gpt_ptr = nullptr;     // ml+1: point-major CSR over sphere groups
+    int* gpt_grp = nullptr;     // first projector of the group
+    double* gpt_uv4 = nullptr;  // 4 projector values of the group at the point
+    float* gpt_uv4_32 = nullptr;
     std::vector<int> h_amap;
 
     // workspace

@@ -15,6 +15,9 @@
 // FP64 form: cuBLAS DSYRK/DSYR2K/DGEMM/DTRSM and cuSOLVER DPOTRF/DSYEVD.
 // Mixed forms: the contractions go to the split-BF16 / FP32 tensor-core
 // kernels of mixed.cu, FP64 stays in Cholesky and the eigensolve.
+#include <algorithm>
+#include <vector>
+
 #include "common.cuh"
 #include "kernels.cuh"
 #include "mixed.cuh"
@@ -25,6 +28,56 @@ __global__ void k_zero_upper(double* a, int n, int lda) {
     int i = blockIdx.x * blockDim.x + threadIdx.x;  // row
     int j = blockIdx.y;                              // column
     if (i < n && i < j) a[(long)j * lda + i] = 0.0;
+}
+
+__global__ void k_zero_lower(double* a, int n, int lda) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;  // row
+    int j = blockIdx.y;                              // column
+    if (i < n && i > j) a[(long)j * lda + i] = 0.0;
+}
+
+// C = alpha * sum_c P[c] (sym: alpha/2 (G + G^T)), fixed summation order
+__global__ void k_reduce_partials(const double* __restrict__ P, int nch, int m, int n, double alpha, int sym,
+                                  double* __restrict__ C) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    const int j = blockIdx.y;
+    if (i >= m) return;
+    const long mn = (long)m * n;
+    double s = 0.0;
+    for (int c = 0; c < nch; ++c) s += P[c * mn + (long)j * m + i];
+    if (sym) {
+        double t = 0.0;
+        for (int c = 0; c < nch; ++c) t += P[c * mn + (long)i * m + j];
+        s = 0.5 * (s + t);
+    }
+    C[(long)j * m + i] = alpha * s;
+}
+
+// C (m x n) = alpha A^T B with A, B tall (ML rows, leading dimension ld):
+// split-K over the grid in equal chunks (strided-batched DGEMM), partial
+// products reduced in a fixed order.  sym = 1 returns the symmetric part.
+static int gemm_tn_splitk(const double* A, const double* B, long ld, int m, int n, double alpha, int sym,
+                          double* C) {
+    Context& c = ctx();
+    const long ml = c.ml;
+    const int nch = (int)std::max<long>(1, std::min<long>(64, (ml + 8191) / 8192));
+    long kc = (ml + nch - 1) / nch;
+    kc = (kc + 7) / 8 * 8;
+    const int full = (int)(ml / kc);
+    const long rem = ml - (long)full * kc;
+    const int parts = full + (rem > 0 ? 1 : 0);
+    double* P = nullptr;
+    RS_CHECK(workspace_t("splitk_partials", (size_t)parts * m * n, &P));
+    const double one = 1.0, zero = 0.0;
+    if (full > 0)
+        RS_BLAS(cublasDgemmStridedBatched(c.blas, CUBLAS_OP_T, CUBLAS_OP_N, m, n, (int)kc, &one, A, (int)ld, kc, B,
+                                          (int)ld, kc, &zero, P, m, (long long)m * n, full));
+    if (rem > 0)
+        RS_BLAS(cublasDgemm(c.blas, CUBLAS_OP_T, CUBLAS_OP_N, m, n, (int)rem, &one, A + (long)full * kc, (int)ld,
+                            B + (long)full * kc, (int)ld, &zero, P + (long)full * m * n, m));
+    launch(k_reduce_partials, dim3(div_up(m, 128), n), 128, 0, c.stream, P, parts, m, n, alpha, sym, C);
+    RS_LAUNCH();
+    return RSDFT_OK;
 }
 
 static int check_info(int* dinfo, const char* what) {
@@ -38,40 +91,53 @@ static int check_info(int* dinfo, const char* what) {
     return RSDFT_OK;
 }
 
-// one CholeskyQR pass in FP64: S = dV psi^T psi = R^T R, psi <- psi R^-1
-static int cholqr_fp64(double* psi, long ld, int nb, double* S, int* dinfo) {
+// One CholeskyQR pass in FP64: S = dV psi^T psi = R^T R, out = psi R^-1.
+// R^-1 comes from a triangular inverse of the small factor, so the tall
+// product is one DGEMM (in and out are different buffers).
+static int cholqr_fp64(const double* psi, double* out, long ld, int nb, double* S, int* dinfo) {
     Context& c = ctx();
-    const double zero = 0.0, one = 1.0, dv = c.dV;
-    RS_BLAS(cublasDsyrk(c.blas, CUBLAS_FILL_MODE_UPPER, CUBLAS_OP_T, nb, (int)c.ml, &dv, psi, (int)ld, &zero, S,
-                        nb));
+    const double zero = 0.0, one = 1.0;
+    RS_CHECK(gemm_tn_splitk(psi, psi, ld, nb, nb, c.dV, 0, S));
     int lwork = 0;
     RS_SOLVER(cusolverDnDpotrf_bufferSize(c.solver, CUBLAS_FILL_MODE_UPPER, nb, S, nb, &lwork));
     double* work = nullptr;
     RS_CHECK(workspace_t("gs_potrf", (size_t)lwork + 1, &work));
     RS_SOLVER(cusolverDnDpotrf(c.solver, CUBLAS_FILL_MODE_UPPER, nb, S, nb, work, lwork, dinfo));
-    RS_BLAS(cublasDtrsm(c.blas, CUBLAS_SIDE_RIGHT, CUBLAS_FILL_MODE_UPPER, CUBLAS_OP_N, CUBLAS_DIAG_NON_UNIT,
-                        (int)c.ml, nb, &one, S, nb, psi, (int)ld));
+    RS_CHECK(check_info(dinfo, "gram_schmidt: overlap Cholesky"));
+    size_t dws = 0, hws = 0;
+    RS_SOLVER(cusolverDnXtrtri_bufferSize(c.solver, CUBLAS_FILL_MODE_UPPER, CUBLAS_DIAG_NON_UNIT, nb, CUDA_R_64F, S,
+                                          nb, &dws, &hws));
+    void* dw = nullptr;
+    RS_CHECK(workspace("gs_trtri", dws + 16, &dw));
+    static std::vector<char> hw;
+    if (hw.size() < hws + 16) hw.resize(hws + 16);
+    RS_SOLVER(cusolverDnXtrtri(c.solver, CUBLAS_FILL_MODE_UPPER, CUBLAS_DIAG_NON_UNIT, nb, CUDA_R_64F, S, nb, dw,
+                               dws, hw.data(), hws, dinfo));
+    RS_CHECK(check_info(dinfo, "gram_schmidt: triangular inverse"));
+    launch(k_zero_lower, dim3(div_up(nb, 128), nb), 128, 0, c.stream, S, nb, nb);
+    RS_LAUNCH();
+    RS_BLAS(cublasDgemm(c.blas, CUBLAS_OP_N, CUBLAS_OP_N, (int)c.ml, nb, nb, &one, psi, (int)ld, S, nb, &zero, out,
+                        (int)ld));
     return RSDFT_OK;
 }
 
 int gram_schmidt_device(double* psi, long ld, int nb, int mode) {
-    Context& c = ctx();
     double* S = nullptr;
     int* dinfo = nullptr;
+    double* tmp = nullptr;
     RS_CHECK(workspace_t("gs_S", (size_t)nb * nb, &S));
     RS_CHECK(workspace_t("gs_info", 4, &dinfo));
     if (mode == RSDFT_MODE_FP64) {
-        RS_CHECK(cholqr_fp64(psi, ld, nb, S, dinfo));
-        RS_CHECK(check_info(dinfo, "gram_schmidt: overlap Cholesky (pass 1)"));
-        RS_CHECK(cholqr_fp64(psi, ld, nb, S, dinfo));
-        RS_CHECK(check_info(dinfo, "gram_schmidt: overlap Cholesky (pass 2)"));
+        // CholeskyQR2 as ping-pong: psi -> tmp -> psi
+        RS_CHECK(workspace_t("gs_tmp", (size_t)ld * nb, &tmp));
+        RS_CHECK(cholqr_fp64(psi, tmp, ld, nb, S, dinfo));
+        RS_CHECK(cholqr_fp64(tmp, psi, ld, nb, S, dinfo));
         return RSDFT_OK;
     }
     RS_CHECK(cholqr_mixed(psi, ld, nb, mode, S, dinfo));
     RS_CHECK(check_info(dinfo, "gram_schmidt: overlap Cholesky (mixed pass 1)"));
     RS_CHECK(cholqr_mixed(psi, ld, nb, mode, S, dinfo));
     RS_CHECK(check_info(dinfo, "gram_schmidt: overlap Cholesky (mixed pass 2)"));
-    (void)c;
     return RSDFT_OK;
 }
 
@@ -93,11 +159,11 @@ int subspace_diag_device(double* psi, long ld, int mb, int spin, double* esp, in
     double *hpsi = nullptr, *H = nullptr;
     RS_CHECK(workspace_t("sub_hpsi", (size_t)ld * mb, &hpsi));
     RS_CHECK(workspace_t("sub_H", (size_t)mb * mb, &H));
-    const double zero = 0.0, one = 1.0, half_dv = 0.5 * c.dV;
+    const double zero = 0.0, one = 1.0;
     if (mode == RSDFT_MODE_FP64) {
         RS_CHECK(hpsi_device<double>(psi, hpsi, ld, mb, spin, nullptr));
-        RS_BLAS(cublasDsyr2k(c.blas, CUBLAS_FILL_MODE_UPPER, CUBLAS_OP_T, mb, (int)c.ml, &half_dv, psi, (int)ld,
-                             hpsi, (int)ld, &zero, H, mb));
+        // Hsub = dV/2 (psi^T H psi + (H psi)^T psi): the symmetric part of dV psi^T (H psi)
+        RS_CHECK(gemm_tn_splitk(psi, hpsi, ld, mb, mb, c.dV, 1, H));
         RS_CHECK(syevd(H, mb, esp, CUBLAS_FILL_MODE_UPPER, "subspace_diag: syevd"));
         RS_BLAS(cublasDgemm(c.blas, CUBLAS_OP_N, CUBLAS_OP_N, (int)c.ml, mb, mb, &one, psi, (int)ld, H, mb, &zero,
                             hpsi, (int)ld));
@@ -171,9 +237,7 @@ int rsdft_gpu_subspace_mate(int k, int s, const double* unk, long ld, int mb, do
     RS_CHECK(workspace_t("sub_hpsi", (size_t)ld * mb, &hpsi));
     RS_CHECK(workspace_t("sub_H", (size_t)mb * mb, &H));
     RS_CHECK(hpsi_device<double>(d, hpsi, ld, mb, s, nullptr));
-    const double zero = 0.0, dv = c.dV;
-    RS_BLAS(cublasDgemm(c.blas, CUBLAS_OP_T, CUBLAS_OP_N, mb, mb, (int)c.ml, &dv, d, (int)ld, hpsi, (int)ld, &zero,
-                        H, mb));
+    RS_CHECK(gemm_tn_splitk(d, hpsi, ld, mb, mb, c.dV, 0, H));
     launch(k_zero_upper, dim3(div_up(mb, 128), mb), 128, 0, c.stream, H, mb, mb);
     RS_LAUNCH();
     RS_CUDA(cudaMemcpy2DAsync(hsub, (size_t)ldh * sizeof(double), H, (size_t)mb * sizeof(double),
