@@ -40,8 +40,8 @@ extern "C" {
 
 /* precision modes of the eigensolver entries */
 #define RSDFT_MODE_FP64 0        /* plain all-FP64 form */
-#define RSDFT_MODE_MIXED_BF16 1  /* split-BF16 tensor-core contractions, FP32 CG sweeps */
-#define RSDFT_MODE_MIXED_FP32 2  /* FP32 contractions, FP32 CG sweeps */
+#define RSDFT_MODE_MIXED_BF16 1    /* 3-term split-BF16 tensor-core contractions (6 products), FP32 CG */
+#define RSDFT_MODE_MIXED_BF16X3 2  /* 2-term split-BF16 tensor-core contractions (3 products), FP32 CG */
 
 /* ---------------------------------------------------------------- set-up */
 
@@ -131,6 +131,17 @@ int rsdft_gpu_subspace_rotv(int k, int s, double *unk, long ld, int mb, const do
  * -> subspace_diag_la, subspace_diag_module.f90:17-25,
  * subspace_diag_la_module.f90:18-232) */
 int rsdft_gpu_subspace_diag(int k, int s, double *unk, long ld, int mb, double *esp, int mode);
+
+/* e(ns:ne) = dV <wf_n|H wf_n>, FP64 (no normalisation, as the reference).
+ * (replaces esp_calc(k,s,wf,n1,n2,ns,ne,e), esp_calc_module.f90:15-49) */
+int rsdft_gpu_esp_calc(int k, int s, const double *wf, int n1, int n2, int ns, int ne, double *e);
+
+/* FP64 Rayleigh quotients and residual norms of nb bands: e(n) = dV <wf|H wf>,
+ * res(n) = dV |H wf - e(n) wf|^2 (the quantity cg_module.f90:213 reports as
+ * res, times 4 / c1^2 = 1).  The final FP64 pass of the mixed forms.  (no
+ * single reference routine: esp_calc_module.f90:15-49 plus the residual of
+ * cg_module.f90:186-213) */
+int rsdft_gpu_residual(int k, int s, const double *wf, long ld, int nb, double *e, double *res);
 
 /* Norm-conserving nonlocal force force2(3, MI) (column-major, i.e. xyz of
  * atom 1 first) for bands with occ(n) != 0.  (replaces

@@ -33,7 +33,7 @@ from ._lib import RsdftError  # noqa: F401  (re-export)
 
 MODE_FP64 = 0
 MODE_MIXED_BF16 = 1
-MODE_MIXED_FP32 = 2
+MODE_MIXED_BF16X3 = 2
 
 
 def _is_torch(a) -> bool:
@@ -158,6 +158,14 @@ class RsdftGpu:
         _lib.call("rsdft_gpu_subspace_rotv", k, s, _ptr(unk, name="unk"), _ld(unk), unk.shape[1],
                   _ptr(vsub, name="vsub"), _ld(vsub))
 
+    def esp_calc(self, k, s, wf, n1, n2, ns, ne, e) -> None:
+        _lib.call("rsdft_gpu_esp_calc", k, s, _ptr(wf, name="wf"), n1, n2, ns, ne, _ptr(e, name="e"))
+
+    def residual(self, k, s, wf, e, res) -> None:
+        """FP64 Rayleigh quotients e and residual norms res of all columns of wf."""
+        _lib.call("rsdft_gpu_residual", k, s, _ptr(wf, name="wf"), _ld(wf), wf.shape[1], _ptr(e, name="e"),
+                  _ptr(res, name="res"))
+
     def calc_force_ps_nloc2(self, MI, force2, unk, occ) -> None:
         """force2 is (3, MI) Fortran-ordered (xyz of atom 1 first)."""
         _lib.call("rsdft_gpu_force_nloc", MI, _ptr(unk, name="unk"), _ld(unk), unk.shape[1],
@@ -168,6 +176,13 @@ class RsdftGpu:
                   _ptr(occ, name="occ"), _ptr(dl_dv, name="dl_dv"), _ptr(dl_dr, name="dl_dr"))
 
     # --------------------------------------------------------- composite
+    def finalize_fp64(self, unk, esp, res) -> None:
+        """The FP64 closing pass of the mixed forms: CholeskyQR2 in FP64, then
+        FP64 Rayleigh quotients and residual norms."""
+        ml, mb = unk.shape
+        self.gram_schmidt(1, mb, 1, 1, unk, mode=MODE_FP64)
+        self.residual(1, 1, unk, esp, res)
+
     def eigensolver_iteration(self, unk, esp, res, *, ncg=4, mloop=3, mode=MODE_FP64) -> None:
         """One sweep iteration as calc_sweep runs it (sweep_module.f90:150-155):
         conjugate_gradient -> gram_schmidt -> subspace_diag."""

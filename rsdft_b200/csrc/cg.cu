@@ -403,6 +403,49 @@ __global__ void k_convert_back(const T* __restrict__ a, double* __restrict__ b, 
     for (; i < n; i += (long)gridDim.x * blockDim.x) b[i] = (double)a[i];
 }
 
+// sum_i (hx - e x)^2 per band (residual norms after the eigenvalues are known)
+__global__ void __launch_bounds__(VT) k_resid(const double* __restrict__ x, const double* __restrict__ hx, long ld,
+                                              long n, const double* __restrict__ e, double* __restrict__ part) {
+    __shared__ double sh[VT / 32];
+    const int b = blockIdx.y;
+    const long off = (long)b * ld, base = (long)blockIdx.x * VCHUNK;
+    const double eb = e[b];
+    double acc = 0.0;
+#pragma unroll
+    for (int it = 0; it < VITEMS; ++it) {
+        const long i = base + it * VT + threadIdx.x;
+        if (i < n) {
+            const double r = hx[off + i] - eb * x[off + i];
+            acc = fma(r, r, acc);
+        }
+    }
+    double s = block_sum<VT>(acc, sh);
+    if (threadIdx.x == 0) part[(long)b * gridDim.x + blockIdx.x] = s;
+}
+
+// e(n) = dV <x_n|H x_n> (esp_calc_module.f90:33-42) and, if res != NULL,
+// res(n) = dV |H x_n - e(n) x_n|^2, all FP64 (device pointers)
+int esp_device(const double* x, long ld, int nb, int spin, double* e, double* res) {
+    Context& c = ctx();
+    cudaStream_t st = c.stream;
+    const long n = c.ml;
+    const int nchunk = div_up(n, VCHUNK);
+    double *hx = nullptr, *part = nullptr;
+    RS_CHECK(workspace_t("esp_hx", (size_t)ld * nb, &hx));
+    RS_CHECK(workspace_t("esp_part", (size_t)nb * nchunk, &part));
+    RS_CHECK(hpsi_device<double>(x, hx, ld, nb, spin, nullptr));
+    const dim3 vg(nchunk, nb);
+    DotPairs<1> pr{{0}, {1}};
+    launch(k_multidot<double, 2, 1>, vg, VT, 0, st, x, hx, nullptr, nullptr, ld, n, pr, part, nullptr);
+    launch(k_finish, div_up(nb, 128), 128, 0, st, part, nchunk, 1, nb, c.dV, e, nullptr);
+    if (res) {
+        launch(k_resid, vg, VT, 0, st, x, hx, ld, n, e, part);
+        launch(k_finish, div_up(nb, 128), 128, 0, st, part, nchunk, 1, nb, c.dV, res, nullptr);
+    }
+    RS_LAUNCH();
+    return RSDFT_OK;
+}
+
 // ------------------------------------------------------------ driver
 template <typename T>
 static int cg_run(T* x, long ld, int mb, int spin, double* esp, double* res, int ncg, int mloop, int ipc) {
@@ -524,6 +567,49 @@ int cg_device(double* unk, long ld, int mb, int spin, double* esp, double* res, 
 }  // namespace rsdft
 
 using namespace rsdft;
+
+extern "C" int rsdft_gpu_esp_calc(int k, int s, const double* wf, int n1, int n2, int ns, int ne, double* e) {
+    RS_CHECK(require_grid());
+    Context& c = ctx();
+    if (k != 1) {
+        set_error("esp_calc: only k=1 (Gamma) is supported");
+        return RSDFT_EUNSUP;
+    }
+    if (s < 1 || s > c.nspin) {
+        set_error("esp_calc: s=%d outside 1..%d", s, c.nspin);
+        return RSDFT_EINVAL;
+    }
+    const long ld = (long)n2 - n1 + 1;
+    const int nb = ne - ns + 1;
+    if (ld != c.ml || nb < 1 || nb > 65535 || !e) {
+        set_error("esp_calc: bad sizes (n2-n1+1=%ld ML=%ld)", ld, c.ml);
+        return RSDFT_EINVAL;
+    }
+    double *d, *de;
+    bool sw;
+    RS_CHECK(wf_acquire(wf, ld, nb, "esp_wf", &d, &sw));
+    RS_CHECK(workspace_t("esp_out", (size_t)nb, &de));
+    RS_CHECK(esp_device(d, ld, nb, s, de, nullptr));
+    RS_CHECK(stage_out(e, de, sizeof(double) * nb));
+    return RSDFT_OK;
+}
+
+extern "C" int rsdft_gpu_residual(int k, int s, const double* wf, long ld, int nb, double* e, double* res) {
+    RS_CHECK(require_grid());
+    Context& c = ctx();
+    if (k != 1 || s < 1 || s > c.nspin || ld < c.ml || nb < 1 || nb > 65535 || !e || !res) {
+        set_error("residual: bad arguments");
+        return RSDFT_EINVAL;
+    }
+    double *d, *de;
+    bool sw;
+    RS_CHECK(wf_acquire(wf, ld, nb, "esp_wf", &d, &sw));
+    RS_CHECK(workspace_t("esp_out", (size_t)2 * nb, &de));
+    RS_CHECK(esp_device(d, ld, nb, s, de, de + nb));
+    RS_CHECK(stage_out(e, de, sizeof(double) * nb));
+    RS_CHECK(stage_out(res, de + nb, sizeof(double) * nb));
+    return RSDFT_OK;
+}
 
 extern "C" int rsdft_gpu_conjugate_gradient(int n1, int n2, int mb, int k, int s, double* unk, double* esp,
                                             double* res, int ncg, int mloop, int ipc, int mode) {

@@ -94,10 +94,13 @@ static int check_info(int* dinfo, const char* what) {
 // One CholeskyQR pass in FP64: S = dV psi^T psi = R^T R, out = psi R^-1.
 // R^-1 comes from a triangular inverse of the small factor, so the tall
 // product is one DGEMM (in and out are different buffers).
-static int cholqr_fp64(const double* psi, double* out, long ld, int nb, double* S, int* dinfo) {
+static int cholqr_pass(const double* psi, double* out, long ld, int nb, double* S, int* dinfo, int mode) {
     Context& c = ctx();
     const double zero = 0.0, one = 1.0;
-    RS_CHECK(gemm_tn_splitk(psi, psi, ld, nb, nb, c.dV, 0, S));
+    if (mode == RSDFT_MODE_FP64)
+        RS_CHECK(gemm_tn_splitk(psi, psi, ld, nb, nb, c.dV, 0, S));
+    else
+        RS_CHECK(gram_mixed(psi, psi, ld, nb, c.dV, 0, mode_terms(mode), S));
     int lwork = 0;
     RS_SOLVER(cusolverDnDpotrf_bufferSize(c.solver, CUBLAS_FILL_MODE_UPPER, nb, S, nb, &lwork));
     double* work = nullptr;
@@ -116,8 +119,11 @@ static int cholqr_fp64(const double* psi, double* out, long ld, int nb, double* 
     RS_CHECK(check_info(dinfo, "gram_schmidt: triangular inverse"));
     launch(k_zero_lower, dim3(div_up(nb, 128), nb), 128, 0, c.stream, S, nb, nb);
     RS_LAUNCH();
-    RS_BLAS(cublasDgemm(c.blas, CUBLAS_OP_N, CUBLAS_OP_N, (int)c.ml, nb, nb, &one, psi, (int)ld, S, nb, &zero, out,
-                        (int)ld));
+    if (mode == RSDFT_MODE_FP64)
+        RS_BLAS(cublasDgemm(c.blas, CUBLAS_OP_N, CUBLAS_OP_N, (int)c.ml, nb, nb, &one, psi, (int)ld, S, nb, &zero, out,
+                            (int)ld));
+    else
+        RS_CHECK(rotate_mixed(psi, out, ld, nb, S, nb, mode_terms(mode)));
     return RSDFT_OK;
 }
 
@@ -127,17 +133,12 @@ int gram_schmidt_device(double* psi, long ld, int nb, int mode) {
     double* tmp = nullptr;
     RS_CHECK(workspace_t("gs_S", (size_t)nb * nb, &S));
     RS_CHECK(workspace_t("gs_info", 4, &dinfo));
-    if (mode == RSDFT_MODE_FP64) {
-        // CholeskyQR2 as ping-pong: psi -> tmp -> psi
-        RS_CHECK(workspace_t("gs_tmp", (size_t)ld * nb, &tmp));
-        RS_CHECK(cholqr_fp64(psi, tmp, ld, nb, S, dinfo));
-        RS_CHECK(cholqr_fp64(tmp, psi, ld, nb, S, dinfo));
-        return RSDFT_OK;
-    }
-    RS_CHECK(cholqr_mixed(psi, ld, nb, mode, S, dinfo));
-    RS_CHECK(check_info(dinfo, "gram_schmidt: overlap Cholesky (mixed pass 1)"));
-    RS_CHECK(cholqr_mixed(psi, ld, nb, mode, S, dinfo));
-    RS_CHECK(check_info(dinfo, "gram_schmidt: overlap Cholesky (mixed pass 2)"));
+    // CholeskyQR2 as ping-pong: psi -> tmp -> psi.  Mixed forms: Gram matrix and
+    // the triangular update on the tensor cores, Cholesky and the triangular
+    // inverse in FP64.
+    RS_CHECK(workspace_t("gs_tmp", (size_t)ld * nb, &tmp));
+    RS_CHECK(cholqr_pass(psi, tmp, ld, nb, S, dinfo, mode));
+    RS_CHECK(cholqr_pass(tmp, psi, ld, nb, S, dinfo, mode));
     return RSDFT_OK;
 }
 
@@ -168,9 +169,10 @@ int subspace_diag_device(double* psi, long ld, int mb, int spin, double* esp, in
         RS_BLAS(cublasDgemm(c.blas, CUBLAS_OP_N, CUBLAS_OP_N, (int)c.ml, mb, mb, &one, psi, (int)ld, H, mb, &zero,
                             hpsi, (int)ld));
     } else {
-        RS_CHECK(subspace_matrix_mixed(psi, hpsi, ld, mb, spin, mode, H));
+        RS_CHECK(hpsi_device<double>(psi, hpsi, ld, mb, spin, nullptr));
+        RS_CHECK(gram_mixed(psi, hpsi, ld, mb, c.dV, 1, mode_terms(mode), H));
         RS_CHECK(syevd(H, mb, esp, CUBLAS_FILL_MODE_UPPER, "subspace_diag: syevd"));
-        RS_CHECK(rotate_mixed(psi, hpsi, ld, mb, H, mode));
+        RS_CHECK(rotate_mixed(psi, hpsi, ld, mb, H, mb, mode_terms(mode)));
     }
     RS_CUDA(cudaMemcpy2DAsync(psi, ld * sizeof(double), hpsi, ld * sizeof(double), c.ml * sizeof(double), mb,
                               cudaMemcpyDeviceToDevice, c.stream));

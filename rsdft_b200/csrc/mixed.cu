@@ -1,22 +1,436 @@
-// Mixed-precision contractions (tensor cores).  Not built yet: every entry
-// reports RSDFT_EUNSUP so callers see the gap instead of a silent fallback.
+// Mixed-precision contractions on the 5th-generation tensor cores (tcgen05).
+//
+// Operands are split into BF16 terms, x = x0 + x1 + x2 (x0 = bf16(x),
+// x1 = bf16(x - x0), x2 = bf16(x - x0 - x1): 24 significant bits), and a
+// product is the sum of the term pairs with s + t < NT (NT = 3: six
+// products, "split-BF16 x3 terms"; NT = 2: three products), every pair an
+// exact BF16 x BF16 product accumulated in FP32 in tensor memory.
+//
+// k_umma (one CTA = one 128 x BN output tile):
+//   warp 0    TMA producer: per K block of 32, the NT slices of the A tile
+//             (128 rows) and of the B tile (BN rows), 64-byte swizzle, into a
+//             ring of NS shared-memory stages (full/empty mbarriers);
+//   warp 1    allocates tensor memory; lane 0 issues the tcgen05.mma chain;
+//   warps 2-9 epilogue (two warps per TMEM lane quadrant, half the columns
+//             each).
+// Two epilogues:
+//   DRAIN (Gram matrices A^T B over the grid, K = ML): two TMEM accumulators;
+//     every SEG K blocks the epilogue adds the FP32 segment into FP64
+//     registers while the MMA fills the other accumulator, so FP32 rounding
+//     never spans more than SEG*32 terms.  Each CTA covers a K range
+//     (split-K) and writes an FP64 partial tile; k_reduce_tiles adds the
+//     partials in a fixed order.
+//   DIRECT (rotations psi V, K = MB): D(n, i) = sum_m V(m, n) psi(i, m) is
+//     written to out(i, n) in FP64.
+#include <cuda_bf16.h>
+
+#include <algorithm>
+
+#include "common.cuh"
+#include "kernels.cuh"
 #include "mixed.cuh"
+#include "tmap.cuh"
+#include "umma.cuh"
 
 namespace rsdft {
 
-int cholqr_mixed(double*, long, int, int, double*, int*) {
-    set_error("mixed-precision Gram-Schmidt is not available in this build");
-    return RSDFT_EUNSUP;
+constexpr int UB_M = 128;      // tile rows (TMEM lanes)
+constexpr int UB_K = 32;       // K block (64 bytes of BF16: one swizzle row)
+constexpr int U_EPI_WARPS = 8;
+constexpr int U_THREADS = 32 * (2 + U_EPI_WARPS);
+constexpr int U_SEG = 4;       // K blocks per FP32 accumulation segment (DRAIN)
+
+__device__ __forceinline__ void split_bf16(double x, __nv_bfloat16& h, __nv_bfloat16& m, __nv_bfloat16& l) {
+    h = __float2bfloat16_rn((float)x);
+    double r = x - (double)__bfloat162float(h);
+    m = __float2bfloat16_rn((float)r);
+    r -= (double)__bfloat162float(m);
+    l = __float2bfloat16_rn((float)r);
 }
 
-int subspace_matrix_mixed(const double*, double*, long, int, int, int, double*) {
-    set_error("mixed-precision subspace matrix is not available in this build");
-    return RSDFT_EUNSUP;
+// slices[s][b][k] = term s of psi(k, b): same layout as psi (K-major per band)
+__global__ void k_split_cols(const double* __restrict__ psi, long ld, int nb, long ml, __nv_bfloat16* __restrict__ out) {
+    const long n = ml * nb;
+    for (long e = (long)blockIdx.x * blockDim.x + threadIdx.x; e < n; e += (long)gridDim.x * blockDim.x) {
+        const long b = e / ml, k = e - b * ml;
+        __nv_bfloat16 h, m, l;
+        split_bf16(psi[b * ld + k], h, m, l);
+        out[e] = h;
+        out[n + e] = m;
+        out[2 * n + e] = l;
+    }
 }
 
-int rotate_mixed(const double*, double*, long, int, const double*, int) {
-    set_error("mixed-precision rotation is not available in this build");
-    return RSDFT_EUNSUP;
+// slices[s][i][m] = term s of psi(i, m), m fastest, padded to mbk (zeros):
+// the transpose that makes the band index the K dimension of a rotation
+__global__ void k_split_rows(const double* __restrict__ psi, long ld, int nb, long ml, int mbk,
+                             __nv_bfloat16* __restrict__ out) {
+    __shared__ double tile[32][33];
+    const long i0 = (long)blockIdx.x * 32;
+    const int m0 = blockIdx.y * 32;
+    const int tx = threadIdx.x, ty = threadIdx.y;  // 32 x 8
+    for (int r = ty; r < 32; r += 8) {
+        const long i = i0 + tx;
+        const int m = m0 + r;
+        tile[r][tx] = (i < ml && m < nb) ? psi[(long)m * ld + i] : 0.0;
+    }
+    __syncthreads();
+    const long n = ml * mbk;
+    for (int r = ty; r < 32; r += 8) {
+        const long i = i0 + r;
+        const int m = m0 + tx;
+        if (i < ml && m < mbk) {
+            __nv_bfloat16 h, mm, l;
+            split_bf16(tile[tx][r], h, mm, l);
+            const long e = i * mbk + m;
+            out[e] = h;
+            out[n + e] = mm;
+            out[2 * n + e] = l;
+        }
+    }
+}
+
+// slices[s][n][m] = term s of V(m, n) (V column-major mb x mb), padded to mbk
+__global__ void k_split_small(const double* __restrict__ V, int mb, int ldv, int mbk, __nv_bfloat16* __restrict__ out) {
+    const long n = (long)mb * mbk;
+    for (long e = (long)blockIdx.x * blockDim.x + threadIdx.x; e < n; e += (long)gridDim.x * blockDim.x) {
+        const int col = (int)(e / mbk), m = (int)(e - (long)col * mbk);
+        const double x = m < mb ? V[(long)col * ldv + m] : 0.0;
+        __nv_bfloat16 h, mm, l;
+        split_bf16(x, h, mm, l);
+        out[e] = h;
+        out[n + e] = mm;
+        out[2 * n + e] = l;
+    }
+}
+
+struct UmmaMaps {
+    CUtensorMap a, b;  // 3-D: {K, rows, slice}
+};
+
+struct UmmaArgs {
+    int kblocks;       // total K blocks of 32
+    int kb_per_split;  // K blocks per CTA (DRAIN)
+    int ntm, ntn;      // tiles along M (A rows) and N (B rows)
+    int sym;           // DRAIN: only tiles with tm <= tn
+    int npairs;
+    double* partial;   // DRAIN: [split][pair][BN][128]
+    double* out;       // DIRECT: out[(n) * ldo + i]
+    long ldo;
+    int mrows, nrows;  // valid rows of A and B
+    int* err;
+};
+
+__device__ __forceinline__ void pair_tiles(const UmmaArgs& g, int pair, int& tm, int& tn) {
+    if (!g.sym) {
+        tm = pair % g.ntm;
+        tn = pair / g.ntm;
+        return;
+    }
+    int r = pair;
+    tn = 0;
+    while (r >= tn + 1) {
+        r -= tn + 1;
+        ++tn;
+    }
+    tm = r;
+}
+
+template <int BN, int NT, int NS, bool DRAIN>
+__global__ void __launch_bounds__(U_THREADS, 1) k_umma(const __grid_constant__ UmmaMaps maps, UmmaArgs g) {
+    constexpr int ABYTES = UB_M * UB_K * 2;  // one A slice tile
+    constexpr int BBYTES = BN * UB_K * 2;
+    constexpr int STAGE = NT * (ABYTES + BBYTES);
+    constexpr int NACC = DRAIN ? 2 : 1;
+    constexpr int TCOLS = NACC * BN;  // 256 in both configurations
+    constexpr uint32_t IDESC = umma_idesc_bf16(UB_M, BN);
+    extern __shared__ __align__(1024) unsigned char smem[];
+    uint64_t* full = reinterpret_cast<uint64_t*>(smem + (size_t)NS * STAGE);
+    uint64_t* empty = full + NS;
+    uint64_t* accf = empty + NS;
+    uint64_t* acce = accf + 2;
+    uint32_t* tslot = reinterpret_cast<uint32_t*>(acce + 2);
+
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    int tm, tn, kb0, kb1;
+    if (DRAIN) {
+        pair_tiles(g, blockIdx.x, tm, tn);
+        kb0 = blockIdx.y * g.kb_per_split;
+        kb1 = min(kb0 + g.kb_per_split, g.kblocks);
+    } else {
+        tm = blockIdx.x;
+        tn = blockIdx.y;
+        kb0 = 0;
+        kb1 = g.kblocks;
+    }
+    const int nkb = max(kb1 - kb0, 0);
+    const int nseg = DRAIN ? (nkb + U_SEG - 1) / U_SEG : 1;
+
+    if (threadIdx.x == 0) {
+        for (int s = 0; s < NS; ++s) {
+            mbar_init(&full[s], 1);
+            mbar_init(&empty[s], 1);
+        }
+        for (int b = 0; b < 2; ++b) {
+            mbar_init(&accf[b], 1);
+            mbar_init(&acce[b], U_EPI_WARPS);
+        }
+        mbar_fence_init();
+    }
+    if (warp == 1) {
+        tmem_alloc(tslot, TCOLS);
+        tmem_relinquish();
+        tc_fence_before();
+    }
+    __syncthreads();
+    tc_fence_after();
+    const uint32_t tbase = *tslot;
+    bool ok = true;
+
+    if (warp == 0) {
+        // ------------------------------------------------------ TMA producer
+        if (lane == 0) {
+            for (int it = 0; it < nkb; ++it) {
+                const int s = it % NS;
+                if (it >= NS && !mbar_wait(&empty[s], ((it / NS) - 1) & 1)) ok = false;
+                unsigned char* st = smem + (size_t)s * STAGE;
+                mbar_arrive_expect_tx(&full[s], STAGE);
+                const int k = (kb0 + it) * UB_K;
+#pragma unroll
+                for (int t = 0; t < NT; ++t) {
+                    // the maps are rank 4 ({K, rows, slice, 1}): 4-D loads, w = 0
+                    tma_load_4d(st + t * ABYTES, &maps.a, k, tm * UB_M, t, 0, &full[s]);
+                    tma_load_4d(st + NT * ABYTES + t * BBYTES, &maps.b, k, tn * BN, t, 0, &full[s]);
+                }
+            }
+        }
+    } else if (warp == 1) {
+        // ------------------------------------------------------- MMA issuer
+        if (lane == 0) {
+            int it = 0;
+            for (int seg = 0; seg < nseg; ++seg) {
+                const int b = seg & 1;
+                if (DRAIN && seg >= 2 && !mbar_wait(&acce[b], ((seg >> 1) - 1) & 1)) ok = false;
+                tc_fence_after();
+                const uint32_t d = tbase + (uint32_t)(b * BN);
+                const int itend = DRAIN ? min(nkb, (seg + 1) * U_SEG) : nkb;
+                bool first = true;
+                for (; it < itend; ++it) {
+                    const int s = it % NS;
+                    if (!mbar_wait(&full[s], (it / NS) & 1)) ok = false;
+                    tc_fence_after();
+                    const uint32_t sa = smem_u32(smem + (size_t)s * STAGE);
+                    const uint32_t sb = sa + NT * ABYTES;
+#pragma unroll
+                    for (int p = 0; p < (NT == 3 ? 6 : 3); ++p) {
+                        const int ta = p == 0 ? 0 : p == 1 ? 0 : p == 2 ? 1 : p == 3 ? 0 : p == 4 ? 1 : 2;
+                        const int tb = p == 0 ? 0 : p == 1 ? 1 : p == 2 ? 0 : p == 3 ? 2 : p == 4 ? 1 : 0;
+#pragma unroll
+                        for (int kk = 0; kk < UB_K / 16; ++kk) {
+                            const uint64_t ad = umma_desc_sw64(sa + ta * ABYTES + kk * 32);
+                            const uint64_t bd = umma_desc_sw64(sb + tb * BBYTES + kk * 32);
+                            umma_bf16(d, ad, bd, IDESC, first ? 0u : 1u);
+                            first = false;
+                        }
+                    }
+                    umma_commit(&empty[s]);
+                }
+                umma_commit(&accf[b]);
+            }
+        }
+    } else {
+        // ---------------------------------------------------------- epilogue
+        const int q = warp & 3;                 // TMEM lane quadrant of this warp
+        const int h = (warp - 2) >> 2;          // column half
+        const int row = 32 * q + lane;          // tile row (TMEM lane)
+        constexpr int CW = BN / 2;              // columns per warp
+        if (DRAIN) {
+            double acc[CW];
+#pragma unroll
+            for (int c = 0; c < CW; ++c) acc[c] = 0.0;
+            for (int seg = 0; seg < nseg; ++seg) {
+                const int b = seg & 1;
+                if (!mbar_wait(&accf[b], (seg >> 1) & 1)) ok = false;
+                tc_fence_after();
+#pragma unroll
+                for (int c0 = 0; c0 < CW; c0 += 32) {
+                    uint32_t r[32];
+                    tmem_ld_x32(tbase + ((uint32_t)(32 * q) << 16) + (uint32_t)(b * BN + h * CW + c0), r);
+                    tmem_ld_wait();
+#pragma unroll
+                    for (int j = 0; j < 32; ++j) acc[c0 + j] += (double)__uint_as_float(r[j]);
+                }
+                tc_fence_before();
+                __syncwarp();
+                if (lane == 0) mbar_arrive(&acce[b]);
+            }
+            double* P = g.partial + ((size_t)blockIdx.y * g.npairs + blockIdx.x) * (size_t)(BN * UB_M);
+#pragma unroll
+            for (int c = 0; c < CW; ++c) P[(size_t)(h * CW + c) * UB_M + row] = acc[c];
+        } else {
+            if (!mbar_wait(&accf[0], 0)) ok = false;
+            tc_fence_after();
+            const int n = tm * UB_M + row;  // output column (A row)
+#pragma unroll
+            for (int c0 = 0; c0 < CW; c0 += 32) {
+                uint32_t r[32];
+                tmem_ld_x32(tbase + ((uint32_t)(32 * q) << 16) + (uint32_t)(h * CW + c0), r);
+                tmem_ld_wait();
+                if (n < g.mrows) {
+                    const int i0 = tn * BN + h * CW + c0;
+                    double* o = g.out + (size_t)n * g.ldo + i0;
+                    if (i0 + 32 <= g.nrows) {
+#pragma unroll
+                        for (int j = 0; j < 32; j += 2) {
+                            double2 v;
+                            v.x = (double)__uint_as_float(r[j]);
+                            v.y = (double)__uint_as_float(r[j + 1]);
+                            *reinterpret_cast<double2*>(o + j) = v;
+                        }
+                    } else {
+                        for (int j = 0; j < 32; ++j)
+                            if (i0 + j < g.nrows) o[j] = (double)__uint_as_float(r[j]);
+                    }
+                }
+            }
+        }
+    }
+    if (!ok) atomicExch(g.err, 2);
+    tc_fence_before();
+    __syncthreads();
+    if (warp == 1) {
+        tc_fence_after();
+        tmem_dealloc(tbase, TCOLS);
+    }
+}
+
+// C(i, j) = alpha * sum_split P (sym: symmetric part); tiles with tm > tn of a
+// symmetric product are read transposed from tile (tn, tm)
+__global__ void k_reduce_tiles(const double* __restrict__ P, int nsplit, int npairs, int ntm, int sym, int bn, int m,
+                               double alpha, int symmetrize, double* __restrict__ C) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    const int j = blockIdx.y;
+    if (i >= m) return;
+    auto fetch = [&](int r, int c) {  // full product element (r, c)
+        int tm = r / UB_M, tn = c / bn, rr = r % UB_M, cc = c % bn;
+        if (sym && tm > tn) {
+            const int t = r;
+            r = c;
+            c = t;
+            tm = r / UB_M;
+            tn = c / bn;
+            rr = r % UB_M;
+            cc = c % bn;
+        }
+        const int pair = sym ? tn * (tn + 1) / 2 + tm : tm + tn * ntm;
+        double s = 0.0;
+        for (int k = 0; k < nsplit; ++k) s += P[((size_t)k * npairs + pair) * (size_t)(bn * UB_M) + (size_t)cc * UB_M + rr];
+        return s;
+    };
+    double v = fetch(i, j);
+    if (symmetrize) v = 0.5 * (v + fetch(j, i));
+    C[(size_t)j * m + i] = alpha * v;
+}
+
+static int map3(CUtensorMap* mp, const __nv_bfloat16* base, long k, long rows, int box_rows) {
+    const unsigned long long dims[4] = {(unsigned long long)k, (unsigned long long)rows, 3ull, 1ull};
+    const unsigned long long strides[3] = {(unsigned long long)k * 2, (unsigned long long)k * rows * 2,
+                                           (unsigned long long)k * rows * 6};
+    const unsigned int box[4] = {(unsigned)UB_K, (unsigned)box_rows, 1u, 1u};
+    return encode_tmap_4d_swz64(mp, base, dims, strides, box);
+}
+
+template <int BN, int NT, int NS, bool DRAIN>
+static int launch_umma(const UmmaMaps& maps, const UmmaArgs& g, dim3 grid) {
+    constexpr int STAGE = NT * (UB_M * UB_K * 2 + BN * UB_K * 2);
+    const size_t smem = (size_t)NS * STAGE + 256;
+    static bool attr = false;
+    if (!attr) {
+        RS_CUDA(cudaFuncSetAttribute(k_umma<BN, NT, NS, DRAIN>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     (int)smem));
+        attr = true;
+    }
+    launch(k_umma<BN, NT, NS, DRAIN>, grid, U_THREADS, smem, ctx().stream, maps, g);
+    RS_LAUNCH();
+    return RSDFT_OK;
+}
+
+// C (nb x nb) = alpha * A^T B (symmetrize: alpha/2 (A^T B + B^T A)); A, B tall
+// (ML x nb, leading dimension ld); B == A computes only the upper tiles.
+int gram_mixed(const double* A, const double* B, long ld, int nb, double alpha, int symmetrize, int nterms,
+               double* C) {
+    Context& c = ctx();
+    const long ml = c.ml;
+    if (ml % 8 != 0) {
+        set_error("mixed contractions need ML to be a multiple of 8");
+        return RSDFT_EUNSUP;
+    }
+    const size_t nsl = (size_t)ml * nb;
+    __nv_bfloat16 *sa = nullptr, *sb = nullptr;
+    RS_CHECK(workspace_t("umma_sa", 3 * nsl, &sa));
+    launch(k_split_cols, 4 * c.num_sms, 256, 0, c.stream, A, ld, nb, ml, sa);
+    const bool same = (A == B);
+    if (!same) {
+        RS_CHECK(workspace_t("umma_sb", 3 * nsl, &sb));
+        launch(k_split_cols, 4 * c.num_sms, 256, 0, c.stream, B, ld, nb, ml, sb);
+    } else {
+        sb = sa;
+    }
+    RS_LAUNCH();
+    UmmaMaps maps;
+    RS_CHECK(map3(&maps.a, sa, ml, nb, UB_M));
+    RS_CHECK(map3(&maps.b, sb, ml, nb, 128));
+    UmmaArgs g{};
+    g.kblocks = (int)((ml + UB_K - 1) / UB_K);
+    g.ntm = g.ntn = (nb + UB_M - 1) / UB_M;
+    g.sym = same ? 1 : 0;
+    g.npairs = same ? g.ntm * (g.ntm + 1) / 2 : g.ntm * g.ntn;
+    const int sms = c.num_sms > 0 ? c.num_sms : 148;
+    int nsplit = std::max(1, sms / g.npairs);
+    nsplit = std::min(nsplit, g.kblocks);
+    g.kb_per_split = (g.kblocks + nsplit - 1) / nsplit;
+    nsplit = (g.kblocks + g.kb_per_split - 1) / g.kb_per_split;
+    RS_CHECK(workspace_t("umma_part", (size_t)nsplit * g.npairs * 128 * UB_M, &g.partial));
+    g.err = c.err_flag;
+    g.mrows = g.nrows = nb;
+    if (nterms == 3)
+        RS_CHECK((launch_umma<128, 3, 4, true>(maps, g, dim3(g.npairs, nsplit))));
+    else
+        RS_CHECK((launch_umma<128, 2, 4, true>(maps, g, dim3(g.npairs, nsplit))));
+    launch(k_reduce_tiles, dim3(div_up(nb, 128), nb), 128, 0, c.stream, g.partial, nsplit, g.npairs, g.ntm, g.sym, 128,
+           nb, alpha, symmetrize, C);
+    RS_LAUNCH();
+    return RSDFT_OK;
+}
+
+// out (ML x nb, leading dimension ldo) = psi V, V (nb x nb, leading dimension ldv)
+int rotate_mixed(const double* psi, double* out, long ld, int nb, const double* V, int ldv, int nterms) {
+    Context& c = ctx();
+    const long ml = c.ml;
+    const int mbk = (nb + 7) / 8 * 8;
+    __nv_bfloat16 *st = nullptr, *sv = nullptr;
+    RS_CHECK(workspace_t("umma_st", 3 * (size_t)ml * mbk, &st));
+    RS_CHECK(workspace_t("umma_sv", 3 * (size_t)nb * mbk, &sv));
+    launch(k_split_rows, dim3(div_up(ml, 32), div_up(mbk, 32)), dim3(32, 8), 0, c.stream, psi, ld, nb, ml, mbk, st);
+    launch(k_split_small, div_up((long)nb * mbk, 256), 256, 0, c.stream, V, nb, ldv, mbk, sv);
+    RS_LAUNCH();
+    UmmaMaps maps;
+    RS_CHECK(map3(&maps.a, sv, mbk, nb, UB_M));
+    RS_CHECK(map3(&maps.b, st, mbk, ml, 256));
+    UmmaArgs g{};
+    g.kblocks = (mbk + UB_K - 1) / UB_K;
+    g.ntm = (nb + UB_M - 1) / UB_M;
+    g.ntn = (int)((ml + 255) / 256);
+    g.out = out;
+    g.ldo = ld;
+    g.mrows = nb;
+    g.nrows = (int)ml;
+    g.err = c.err_flag;
+    if (nterms == 3)
+        RS_CHECK((launch_umma<256, 3, 3, false>(maps, g, dim3(g.ntm, g.ntn))));
+    else
+        RS_CHECK((launch_umma<256, 2, 3, false>(maps, g, dim3(g.ntm, g.ntn))));
+    return RSDFT_OK;
 }
 
 }  // namespace rsdft

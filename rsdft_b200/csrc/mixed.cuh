@@ -1,18 +1,20 @@
-// Mixed-precision contractions of the Gram-Schmidt and subspace steps.
+// Mixed-precision contractions of the Gram-Schmidt and subspace steps on the
+// tcgen05 tensor cores (split-BF16 operands, FP32 accumulation, FP64 result).
 #pragma once
 
 #include "common.cuh"
 
 namespace rsdft {
 
-// One CholeskyQR pass with the Gram matrix and the triangular update on the
-// tensor cores (split-BF16 or FP32), Cholesky in FP64.  S: nb x nb scratch.
-int cholqr_mixed(double* psi, long ld, int nb, int mode, double* S, int* dinfo);
+// C (nb x nb) = alpha A^T B (symmetrize: alpha/2 (A^T B + B^T A)) for tall A,
+// B (ML x nb, leading dimension ld).  nterms = 3 (six products) or 2 (three).
+int gram_mixed(const double* A, const double* B, long ld, int nb, double alpha, int symmetrize, int nterms,
+               double* C);
 
-// H = dV/2 (psi^T H psi + (H psi)^T psi) with H psi written to hpsi.
-int subspace_matrix_mixed(const double* psi, double* hpsi, long ld, int mb, int spin, int mode, double* H);
+// out (ML x nb, leading dimension ld) = psi V with V (nb x nb, leading
+// dimension ldv).  out must not alias psi.
+int rotate_mixed(const double* psi, double* out, long ld, int nb, const double* V, int ldv, int nterms);
 
-// out = psi V (ML x MB by MB x MB).
-int rotate_mixed(const double* psi, double* out, long ld, int mb, const double* V, int mode);
+inline int mode_terms(int mode) { return mode == RSDFT_MODE_MIXED_BF16 ? 3 : 2; }
 
 }  // namespace rsdft

@@ -25,7 +25,7 @@ static EncodeTiledFn encode_fn() {
 }
 
 int encode_tmap_4d(CUtensorMap* map, CUtensorMapDataType dtype, const void* base, const unsigned long long dims[4],
-                   const unsigned long long strides_bytes[3], const unsigned int box[4]) {
+                   const unsigned long long strides_bytes[3], const unsigned int box[4], CUtensorMapSwizzle swizzle) {
     EncodeTiledFn fn = encode_fn();
     if (!fn) {
         set_error("cuTensorMapEncodeTiled is not available from the driver");
@@ -35,8 +35,8 @@ int encode_tmap_4d(CUtensorMap* map, CUtensorMapDataType dtype, const void* base
     cuuint64_t s[3] = {strides_bytes[0], strides_bytes[1], strides_bytes[2]};
     cuuint32_t b[4] = {box[0], box[1], box[2], box[3]};
     cuuint32_t e[4] = {1, 1, 1, 1};
-    CUresult r = fn(map, dtype, 4, const_cast<void*>(base), d, s, b, e, CU_TENSOR_MAP_INTERLEAVE_NONE,
-                    CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    CUresult r = fn(map, dtype, 4, const_cast<void*>(base), d, s, b, e, CU_TENSOR_MAP_INTERLEAVE_NONE, swizzle,
+                    CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
     if (r != CUDA_SUCCESS) {
         set_error("cuTensorMapEncodeTiled failed (%d)", (int)r);
         return RSDFT_ECUDA;

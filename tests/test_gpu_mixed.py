@@ -1,0 +1,96 @@
+"""Mixed-precision forms (tcgen05 split-BF16 contractions, FP32 CG sweeps)
+against the FP64 oracle on seeded cells.
+
+Tolerances: the 3-term split keeps 24 significant bits per operand and the
+FP32 accumulation is drained to FP64 every 1024 terms, so contractions agree
+with FP64 to ~1e-7 relative; orthogonality after mixed CholeskyQR2 is ~1e-7,
+not the FP64 1e-12 (the FP64 finalisation restores that).
+"""
+import numpy as np
+import pytest
+import torch
+
+from oracle import oracle as O
+from rsdft_b200 import api
+
+from test_gpu_parity import dev, host, overlap_check, prepare, rel
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.mark.parametrize("mode,tol", [(api.MODE_MIXED_BF16, 3e-6), (api.MODE_MIXED_BF16X3, 2e-4)])
+@pytest.mark.parametrize("name,nb", [("si8", 32), ("si64", 160)])
+def test_mixed_gram_schmidt(gpu, cells, mode, tol, name, nb):
+    c, o = prepare(gpu, cells, name)
+    psi = np.asfortranarray(c.psi0()[:, :nb])
+    ref = o.gram_schmidt_t(psi)
+    u = dev(psi)
+    gpu.gram_schmidt(1, nb, 1, 1, u, mode=mode)
+    torch.cuda.synchronize()
+    g = host(u)
+    orth = np.abs(g.T @ g * c.dV - np.eye(nb)).max()
+    assert orth <= tol, f"orthogonality {orth:.2e}"
+    assert rel(g, ref) <= 50 * tol
+
+
+@pytest.mark.parametrize("mode,tol", [(api.MODE_MIXED_BF16, 3e-6), (api.MODE_MIXED_BF16X3, 1e-4)])
+def test_mixed_subspace_diag(gpu, cells, mode, tol):
+    c, o = prepare(gpu, cells, "si64")
+    nb = 160
+    psi = o.gram_schmidt_t(np.asfortranarray(c.psi0()[:, :nb]))
+    ref, w, _ = o.subspace_diag_la(psi)
+    u = dev(psi)
+    esp = torch.zeros(nb, dtype=torch.float64, device="cuda")
+    gpu.subspace_diag(1, 1, u, esp, mode=mode)
+    torch.cuda.synchronize()
+    e = host(esp)
+    assert np.abs(e - w).max() <= tol * max(1.0, np.abs(w).max())
+    assert overlap_check(host(u), ref, w, c.dV, gap_tol=1e-3) <= 1e3 * tol
+
+
+def test_mixed_cg_sweep_fp32(gpu, cells):
+    c, o = prepare(gpu, cells, "si8")
+    q = o.gram_schmidt_t(c.psi0())
+    ru, resp, rres, _ = o.conjugate_gradient(q, 4, 3)
+    u = dev(q)
+    esp = torch.zeros(c.nband, dtype=torch.float64, device="cuda")
+    res = torch.zeros_like(esp)
+    gpu.conjugate_gradient(1, c.ML, c.nband, 1, 1, u, esp, res, ncg=4, mloop=3, mode=api.MODE_MIXED_BF16)
+    torch.cuda.synchronize()
+    # FP32 storage and arithmetic in the sweeps: eigenvalue estimates to ~1e-6
+    assert np.abs(host(esp) - resp).max() <= 1e-5 * max(1.0, np.abs(resp).max())
+
+
+def test_mixed_iteration_tracks_fp64(gpu, cells):
+    """Three full iterations in the mixed form stay within 1e-5 Ha of FP64."""
+    c, o = prepare(gpu, cells, "si8")
+    q = o.gram_schmidt_t(c.psi0())
+    ua, ub = dev(q), dev(q)
+    ea = torch.zeros(c.nband, dtype=torch.float64, device="cuda")
+    eb = torch.zeros_like(ea)
+    res = torch.zeros_like(ea)
+    for _ in range(3):
+        gpu.eigensolver_iteration(ua, ea, res, ncg=4, mloop=3, mode=api.MODE_FP64)
+        gpu.eigensolver_iteration(ub, eb, res, ncg=4, mloop=3, mode=api.MODE_MIXED_BF16)
+    torch.cuda.synchronize()
+    assert np.abs(host(ea) - host(eb)).max() <= 1e-5
+
+
+def test_mixed_then_fp64_closing_pass(gpu, cells):
+    """Mixed iterations, then the FP64 closing pass: orthogonality at the FP64
+    level and Rayleigh quotients close to the all-FP64 run."""
+    c, o = prepare(gpu, cells, "si8")
+    q = o.gram_schmidt_t(c.psi0())
+    ua, ub = dev(q), dev(q)
+    ea = torch.zeros(c.nband, dtype=torch.float64, device="cuda")
+    eb = torch.zeros_like(ea)
+    res = torch.zeros_like(ea)
+    for _ in range(4):
+        gpu.eigensolver_iteration(ua, ea, res, ncg=4, mloop=3, mode=api.MODE_FP64)
+        gpu.eigensolver_iteration(ub, eb, res, ncg=4, mloop=3, mode=api.MODE_MIXED_BF16)
+    gpu.finalize_fp64(ua, ea, res)
+    gpu.finalize_fp64(ub, eb, res)
+    torch.cuda.synchronize()
+    g = host(ub)
+    assert np.abs(g.T @ g * c.dV - np.eye(c.nband)).max() <= 1e-12
+    assert np.abs(host(ea) - host(eb)).max() <= 1e-5

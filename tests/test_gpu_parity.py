@@ -293,3 +293,19 @@ def test_error_statuses(gpu, cells):
     # the context stays usable after the error
     gpu.hamiltonian(1, 1, psi, out, 1, c.ML, 1, psi.shape[1])
     assert rel(out, o.hamiltonian(psi)) <= TOL
+
+
+def test_esp_calc_and_residual(gpu, cells):
+    c, o = prepare(gpu, cells, "si8")
+    psi = np.asfortranarray(o.gram_schmidt_t(c.psi0()))
+    h = o.hamiltonian(psi)
+    e_ref = np.einsum("ij,ij->j", psi, h) * c.dV  # esp_calc_module.f90:41
+    r_ref = np.einsum("ij,ij->j", h - psi * e_ref, h - psi * e_ref) * c.dV
+    e = np.zeros(c.nband)
+    gpu.esp_calc(1, 1, psi, 1, c.ML, 1, c.nband, e)
+    assert rel(e, e_ref) <= TOL
+    e2 = np.zeros(c.nband)
+    r = np.zeros(c.nband)
+    gpu.residual(1, 1, dev(psi), e2, r)
+    assert rel(e2, e_ref) <= TOL
+    assert rel(r, r_ref) <= 1e-10
