@@ -1,0 +1,300 @@
+!-----------------------------------------------------------------------------
+! rsdft_gpu_mod: ISO_C_BINDING interface to librsdft_gpu.so (include/rsdft_gpu.h)
+! and thin shims with the call surfaces of RSDFT's eigensolver routines, so a
+! Fortran driver swaps the callee and keeps its own code.
+!
+! Shim                          replaces (RSDFT v1.3.0 src/)
+! gpu_hamiltonian               hamiltonian            hamiltonian_module.f90:20
+! gpu_conjugate_gradient        conjugate_gradient     cg_module.f90:54
+! gpu_gram_schmidt              gram_schmidt           gram_schmidt_module.f90:28
+! gpu_subspace_diag             subspace_diag          subspace_diag_module.f90:17
+! gpu_subspace_mate_sl          subspace_mate_sl       subspace_mate_sl_module.f90:27
+! gpu_subspace_solv_sl          subspace_solv_sl       subspace_solv_sl_module.f90:15
+! gpu_subspace_rotv_sl          subspace_rotv_sl       subspace_rotv_sl_module.f90:24
+! gpu_esp_calc                  esp_calc               esp_calc_module.f90:15
+! gpu_calc_force_ps_nloc2       calc_force_ps_nloc2    ps_nloc2_module.f90:1281
+!
+! Real Gamma-point build only (-D_DRSDFT_), one MPI rank per GPU.  Arrays are
+! passed by address (c_loc); a non-zero status stops the program with the
+! library's message, the reference's own convention for fatal errors.
+!-----------------------------------------------------------------------------
+MODULE rsdft_gpu_mod
+
+  use iso_c_binding
+
+  implicit none
+
+  PRIVATE
+  PUBLIC :: gpu_init, gpu_setup_grid, gpu_setup_vloc, gpu_setup_nonlocal, gpu_register_wf, gpu_sync_to_host, &
+            gpu_sync_to_device, gpu_hamiltonian, gpu_conjugate_gradient, gpu_gram_schmidt, gpu_subspace_diag, &
+            gpu_subspace_mate_sl, gpu_subspace_solv_sl, gpu_subspace_rotv_sl, gpu_esp_calc, gpu_calc_force_ps_nloc2
+
+  integer(c_int), parameter, PUBLIC :: RSDFT_MODE_FP64 = 0, RSDFT_MODE_MIXED_BF16 = 1, RSDFT_MODE_MIXED_BF16X3 = 2
+
+  interface
+     integer(c_int) function rsdft_gpu_init(device) bind(C, name="rsdft_gpu_init")
+       import :: c_int
+       integer(c_int), value :: device
+     end function rsdft_gpu_init
+     type(c_ptr) function rsdft_gpu_last_error() bind(C, name="rsdft_gpu_last_error")
+       import :: c_ptr
+     end function rsdft_gpu_last_error
+     integer(c_int) function rsdft_gpu_set_grid(ngrid, md, coef_lap0, coef_lap, hgrid, ggg, dv) &
+          bind(C, name="rsdft_gpu_set_grid")
+       import :: c_int, c_double, c_ptr
+       type(c_ptr), value :: ngrid, coef_lap, hgrid, ggg
+       integer(c_int), value :: md
+       real(c_double), value :: coef_lap0, dv
+     end function rsdft_gpu_set_grid
+     integer(c_int) function rsdft_gpu_set_vloc(vloc, ml, nspin) bind(C, name="rsdft_gpu_set_vloc")
+       import :: c_int, c_long, c_ptr
+       type(c_ptr), value :: vloc
+       integer(c_long), value :: ml
+       integer(c_int), value :: nspin
+     end function rsdft_gpu_set_vloc
+     integer(c_int) function rsdft_gpu_set_nonlocal(nzlma, lma_ptr, jjp, uv, iuv, amap, natom, duvdr) &
+          bind(C, name="rsdft_gpu_set_nonlocal")
+       import :: c_int, c_ptr
+       integer(c_int), value :: nzlma, natom
+       type(c_ptr), value :: lma_ptr, jjp, uv, iuv, amap, duvdr
+     end function rsdft_gpu_set_nonlocal
+     integer(c_int) function rsdft_gpu_register_wf(unk, ml, mb) bind(C, name="rsdft_gpu_register_wf")
+       import :: c_int, c_long, c_ptr
+       type(c_ptr), value :: unk
+       integer(c_long), value :: ml
+       integer(c_int), value :: mb
+     end function rsdft_gpu_register_wf
+     integer(c_int) function rsdft_gpu_sync_to_host(unk) bind(C, name="rsdft_gpu_sync_to_host")
+       import :: c_int, c_ptr
+       type(c_ptr), value :: unk
+     end function rsdft_gpu_sync_to_host
+     integer(c_int) function rsdft_gpu_sync_to_device(unk) bind(C, name="rsdft_gpu_sync_to_device")
+       import :: c_int, c_ptr
+       type(c_ptr), value :: unk
+     end function rsdft_gpu_sync_to_device
+     integer(c_int) function rsdft_gpu_hamiltonian(k, s, tpsi, htpsi, n1, n2, ib1, ib2) &
+          bind(C, name="rsdft_gpu_hamiltonian")
+       import :: c_int, c_ptr
+       integer(c_int), value :: k, s, n1, n2, ib1, ib2
+       type(c_ptr), value :: tpsi, htpsi
+     end function rsdft_gpu_hamiltonian
+     integer(c_int) function rsdft_gpu_conjugate_gradient(n1, n2, mb, k, s, unk, esp, res, ncg, mloop, ipc, mode) &
+          bind(C, name="rsdft_gpu_conjugate_gradient")
+       import :: c_int, c_ptr
+       integer(c_int), value :: n1, n2, mb, k, s, ncg, mloop, ipc, mode
+       type(c_ptr), value :: unk, esp, res
+     end function rsdft_gpu_conjugate_gradient
+     integer(c_int) function rsdft_gpu_gram_schmidt(n0, n1, k, s, unk, ld, nblk, nblk1, mode) &
+          bind(C, name="rsdft_gpu_gram_schmidt")
+       import :: c_int, c_long, c_ptr
+       integer(c_int), value :: n0, n1, k, s, nblk, nblk1, mode
+       type(c_ptr), value :: unk
+       integer(c_long), value :: ld
+     end function rsdft_gpu_gram_schmidt
+     integer(c_int) function rsdft_gpu_subspace_diag(k, s, unk, ld, mb, esp, mode) &
+          bind(C, name="rsdft_gpu_subspace_diag")
+       import :: c_int, c_long, c_ptr
+       integer(c_int), value :: k, s, mb, mode
+       type(c_ptr), value :: unk, esp
+       integer(c_long), value :: ld
+     end function rsdft_gpu_subspace_diag
+     integer(c_int) function rsdft_gpu_subspace_mate(k, s, unk, ld, mb, hsub, ldh) &
+          bind(C, name="rsdft_gpu_subspace_mate")
+       import :: c_int, c_long, c_ptr
+       integer(c_int), value :: k, s, mb, ldh
+       type(c_ptr), value :: unk, hsub
+       integer(c_long), value :: ld
+     end function rsdft_gpu_subspace_mate
+     integer(c_int) function rsdft_gpu_subspace_solv(mb, hsub, ldh, esp, vsub, ldv) &
+          bind(C, name="rsdft_gpu_subspace_solv")
+       import :: c_int, c_ptr
+       integer(c_int), value :: mb, ldh, ldv
+       type(c_ptr), value :: hsub, esp, vsub
+     end function rsdft_gpu_subspace_solv
+     integer(c_int) function rsdft_gpu_subspace_rotv(k, s, unk, ld, mb, vsub, ldv) &
+          bind(C, name="rsdft_gpu_subspace_rotv")
+       import :: c_int, c_long, c_ptr
+       integer(c_int), value :: k, s, mb, ldv
+       type(c_ptr), value :: unk, vsub
+       integer(c_long), value :: ld
+     end function rsdft_gpu_subspace_rotv
+     integer(c_int) function rsdft_gpu_esp_calc(k, s, wf, n1, n2, ns, ne, e) bind(C, name="rsdft_gpu_esp_calc")
+       import :: c_int, c_ptr
+       integer(c_int), value :: k, s, n1, n2, ns, ne
+       type(c_ptr), value :: wf, e
+     end function rsdft_gpu_esp_calc
+     integer(c_int) function rsdft_gpu_force_nloc(mi, unk, ld, mb, occ, force2) bind(C, name="rsdft_gpu_force_nloc")
+       import :: c_int, c_long, c_ptr
+       integer(c_int), value :: mi, mb
+       type(c_ptr), value :: unk, occ, force2
+       integer(c_long), value :: ld
+     end function rsdft_gpu_force_nloc
+  end interface
+
+CONTAINS
+
+  SUBROUTINE check(ierr, who)
+    integer(c_int), intent(IN) :: ierr
+    character(*), intent(IN) :: who
+    character(kind=c_char), pointer :: msg(:)
+    character(len=1024) :: text
+    integer :: i
+    if ( ierr == 0 ) return
+    call c_f_pointer(rsdft_gpu_last_error(), msg, [1024])
+    text = ""
+    do i = 1, 1024
+       if ( msg(i) == c_null_char ) exit
+       text(i:i) = msg(i)
+    end do
+    write(*,*) "rsdft_gpu: ", who, " status ", ierr, ": ", trim(text)
+    stop "rsdft_gpu"
+  END SUBROUTINE check
+
+  SUBROUTINE gpu_init(device)
+    integer, intent(IN) :: device
+    call check(rsdft_gpu_init(int(device, c_int)), "init")
+  END SUBROUTINE gpu_init
+
+  ! Ngrid(1:3), Md, coef_lap0, coef_lap(3,Md), Hgrid(1:3), ggg(1:3), dV
+  ! (kinetic_variables / rgrid_module after init_kinetic)
+  SUBROUTINE gpu_setup_grid(ngrid, md, coef_lap0, coef_lap, hgrid, ggg, dv)
+    integer, intent(IN) :: ngrid(3), md
+    real(8), intent(IN) :: coef_lap0, dv
+    real(8), intent(IN) :: coef_lap(3, md), hgrid(3), ggg(3)
+    integer(c_int), target :: ng(3)
+    real(c_double), target :: cl(md, 3), h(3), g(3)
+    ng = ngrid
+    cl = transpose(coef_lap)  ! axis-major: coef_lap[axis*Md + m-1]
+    h = hgrid
+    g = ggg
+    call check(rsdft_gpu_set_grid(c_loc(ng), int(md, c_int), coef_lap0, c_loc(cl), c_loc(h), c_loc(g), dv), &
+               "set_grid")
+  END SUBROUTINE gpu_setup_grid
+
+  SUBROUTINE gpu_setup_vloc(vloc, ml, nspin)
+    integer, intent(IN) :: ml, nspin
+    real(8), intent(IN), target :: vloc(ml, nspin)
+    call check(rsdft_gpu_set_vloc(c_loc(vloc), int(ml, c_long), int(nspin, c_int)), "set_vloc")
+  END SUBROUTINE gpu_setup_vloc
+
+  ! uVk(MAXMJJ,nzlma,1), JJP(MAXMJJ,nzlma), MJJ(nzlma), iuV(nzlma), amap(nzlma)
+  ! (ps_nloc2_variables after prep_ps_nloc2) converted to the CSR of the C side.
+  SUBROUTINE gpu_setup_nonlocal(nzlma, maxmjj, mjj, jjp, uvk, iuv, amap, natom, duvdr)
+    integer, intent(IN) :: nzlma, maxmjj, natom
+    integer, intent(IN) :: mjj(nzlma), jjp(maxmjj, nzlma), iuv(nzlma), amap(nzlma)
+    real(8), intent(IN) :: uvk(maxmjj, nzlma)
+    real(8), intent(IN), optional :: duvdr(3, maxmjj, nzlma)
+    integer(c_int), allocatable, target :: ptr(:), jj(:), iu(:), am(:)
+    real(c_double), allocatable, target :: uv(:), du(:)
+    integer :: lma, j, n, nnz
+    nnz = sum(mjj)
+    allocate( ptr(nzlma + 1), jj(max(nnz, 1)), uv(max(nnz, 1)), iu(max(nzlma, 1)), am(max(nzlma, 1)) )
+    allocate( du(max(3 * nnz, 1)) )
+    n = 0
+    ptr(1) = 0
+    do lma = 1, nzlma
+       do j = 1, mjj(lma)
+          n = n + 1
+          jj(n) = jjp(j, lma) - 1          ! 0-based grid index
+          uv(n) = uvk(j, lma)
+          if ( present(duvdr) ) du(3 * n - 2:3 * n) = duvdr(:, j, lma)
+       end do
+       ptr(lma + 1) = n
+       iu(lma) = iuv(lma)
+       am(lma) = amap(lma) - 1             ! 0-based atom
+    end do
+    if ( present(duvdr) ) then
+       call check(rsdft_gpu_set_nonlocal(int(nzlma, c_int), c_loc(ptr), c_loc(jj), c_loc(uv), c_loc(iu), &
+                  c_loc(am), int(natom, c_int), c_loc(du)), "set_nonlocal")
+    else
+       call check(rsdft_gpu_set_nonlocal(int(nzlma, c_int), c_loc(ptr), c_loc(jj), c_loc(uv), c_loc(iu), &
+                  c_loc(am), int(natom, c_int), c_null_ptr), "set_nonlocal")
+    end if
+    deallocate( du, am, iu, uv, jj, ptr )
+  END SUBROUTINE gpu_setup_nonlocal
+
+  SUBROUTINE gpu_register_wf(unk, ml, mb)
+    integer, intent(IN) :: ml, mb
+    real(8), intent(INOUT), target :: unk(ml, mb)
+    call check(rsdft_gpu_register_wf(c_loc(unk), int(ml, c_long), int(mb, c_int)), "register_wf")
+  END SUBROUTINE gpu_register_wf
+
+  SUBROUTINE gpu_sync_to_host(unk)
+    real(8), intent(INOUT), target :: unk(:, :)
+    call check(rsdft_gpu_sync_to_host(c_loc(unk)), "sync_to_host")
+  END SUBROUTINE gpu_sync_to_host
+
+  SUBROUTINE gpu_sync_to_device(unk)
+    real(8), intent(INOUT), target :: unk(:, :)
+    call check(rsdft_gpu_sync_to_device(c_loc(unk)), "sync_to_device")
+  END SUBROUTINE gpu_sync_to_device
+
+  SUBROUTINE gpu_hamiltonian(k, s, tpsi, htpsi, n1, n2, ib1, ib2)
+    integer, intent(IN) :: k, s, n1, n2, ib1, ib2
+    real(8), intent(IN), target :: tpsi(n1:n2, ib1:ib2)
+    real(8), intent(OUT), target :: htpsi(n1:n2, ib1:ib2)
+    call check(rsdft_gpu_hamiltonian(k, s, c_loc(tpsi), c_loc(htpsi), n1, n2, ib1, ib2), "hamiltonian")
+  END SUBROUTINE gpu_hamiltonian
+
+  SUBROUTINE gpu_conjugate_gradient(n1, n2, mb, k, s, unk, esp, res, ncg, mloop, ipc, mode)
+    integer, intent(IN) :: n1, n2, mb, k, s, ncg, mloop, ipc, mode
+    real(8), intent(INOUT), target :: unk(n1:n2, mb)
+    real(8), intent(INOUT), target :: esp(mb), res(mb)
+    call check(rsdft_gpu_conjugate_gradient(n1, n2, mb, k, s, c_loc(unk), c_loc(esp), c_loc(res), ncg, mloop, ipc, &
+               mode), "conjugate_gradient")
+  END SUBROUTINE gpu_conjugate_gradient
+
+  SUBROUTINE gpu_gram_schmidt(n0, n1, k, s, unk, mode)
+    integer, intent(IN) :: n0, n1, k, s, mode
+    real(8), intent(INOUT), target :: unk(:, :)
+    call check(rsdft_gpu_gram_schmidt(n0, n1, k, s, c_loc(unk), int(size(unk, 1), c_long), 0, 4, mode), &
+               "gram_schmidt")
+  END SUBROUTINE gpu_gram_schmidt
+
+  SUBROUTINE gpu_subspace_diag(k, s, unk, esp, mode)
+    integer, intent(IN) :: k, s, mode
+    real(8), intent(INOUT), target :: unk(:, :)
+    real(8), intent(OUT), target :: esp(:)
+    call check(rsdft_gpu_subspace_diag(k, s, c_loc(unk), int(size(unk, 1), c_long), int(size(unk, 2), c_int), &
+               c_loc(esp), mode), "subspace_diag")
+  END SUBROUTINE gpu_subspace_diag
+
+  SUBROUTINE gpu_subspace_mate_sl(k, s, unk, hsub)
+    integer, intent(IN) :: k, s
+    real(8), intent(IN), target :: unk(:, :)
+    real(8), intent(OUT), target :: hsub(:, :)
+    call check(rsdft_gpu_subspace_mate(k, s, c_loc(unk), int(size(unk, 1), c_long), int(size(unk, 2), c_int), &
+               c_loc(hsub), int(size(hsub, 1), c_int)), "subspace_mate_sl")
+  END SUBROUTINE gpu_subspace_mate_sl
+
+  SUBROUTINE gpu_subspace_solv_sl(hsub, esp, vsub)
+    real(8), intent(IN), target :: hsub(:, :)
+    real(8), intent(OUT), target :: esp(:), vsub(:, :)
+    call check(rsdft_gpu_subspace_solv(int(size(hsub, 2), c_int), c_loc(hsub), int(size(hsub, 1), c_int), &
+               c_loc(esp), c_loc(vsub), int(size(vsub, 1), c_int)), "subspace_solv_sl")
+  END SUBROUTINE gpu_subspace_solv_sl
+
+  SUBROUTINE gpu_subspace_rotv_sl(k, s, unk, vsub)
+    integer, intent(IN) :: k, s
+    real(8), intent(INOUT), target :: unk(:, :)
+    real(8), intent(IN), target :: vsub(:, :)
+    call check(rsdft_gpu_subspace_rotv(k, s, c_loc(unk), int(size(unk, 1), c_long), int(size(unk, 2), c_int), &
+               c_loc(vsub), int(size(vsub, 1), c_int)), "subspace_rotv_sl")
+  END SUBROUTINE gpu_subspace_rotv_sl
+
+  SUBROUTINE gpu_esp_calc(k, s, wf, n1, n2, ns, ne, e)
+    integer, intent(IN) :: k, s, n1, n2, ns, ne
+    real(8), intent(IN), target :: wf(n1:n2, ns:ne)
+    real(8), intent(OUT), target :: e(ns:ne)
+    call check(rsdft_gpu_esp_calc(k, s, c_loc(wf), n1, n2, ns, ne, c_loc(e)), "esp_calc")
+  END SUBROUTINE gpu_esp_calc
+
+  SUBROUTINE gpu_calc_force_ps_nloc2(mi, force2, unk, occ)
+    integer, intent(IN) :: mi
+    real(8), intent(OUT), target :: force2(3, mi)
+    real(8), intent(IN), target :: unk(:, :), occ(:)
+    call check(rsdft_gpu_force_nloc(int(mi, c_int), c_loc(unk), int(size(unk, 1), c_long), &
+               int(size(unk, 2), c_int), c_loc(occ), c_loc(force2)), "calc_force_ps_nloc2")
+  END SUBROUTINE gpu_calc_force_ps_nloc2
+
+END MODULE rsdft_gpu_mod
