@@ -95,6 +95,30 @@ int rsdft_gpu_sync_to_device(double *unk);
 int rsdft_gpu_hamiltonian(int k, int s, const double *tpsi, double *htpsi, int n1, int n2, int ib1,
                           int ib2);
 
+/* Capacity, in doubles (4 MiB), of the static scratch of
+ * rsdft_gpu_hamiltonian_noalloc. */
+#define RSDFT_NOALLOC_SCRATCH_VALUES 524288L
+
+/* The same H psi as rsdft_gpu_hamiltonian, for callers that cannot allocate
+ * device memory while they run: a host code that has handed all of its GPU
+ * memory to its own pool, or that must not wait on the allocator's implicit
+ * device synchronisation inside a latency-bound loop.  No counterpart in the
+ * reference.
+ *  - It calls no cudaMalloc/cudaFree and no allocating library routine.  Its
+ *    only scratch, the projection coefficients (nb x nzlma values), sits in a
+ *    static device array of RSDFT_NOALLOC_SCRATCH_VALUES doubles that every
+ *    GPU loading this library holds until exit.  A call with
+ *    (ib2-ib1+1) * nzlma above that returns RSDFT_EINVAL; split the bands.
+ *  - tpsi and htpsi must be device memory or lie in a registered
+ *    wavefunction: nothing is staged.
+ *  - The first call on a device looks up the array's device address; make
+ *    that first call before any stream capture.
+ *  - All calls share the one array: calls that overlap on the GPU (other
+ *    streams, other host threads) race.  Each call overwrites every value it
+ *    reads, so no clearing is needed between calls. */
+int rsdft_gpu_hamiltonian_noalloc(int k, int s, const double *tpsi, double *htpsi, int n1, int n2,
+                                  int ib1, int ib2);
+
 /* Band-by-band preconditioned CG, all bands advanced concurrently (exact:
  * SWGS = 0 keeps bands independent).  ncg line steps, mloop preconditioner
  * sweeps, ipc = 4 (hprsdft preconditioner) or 0 (none); mode per above.

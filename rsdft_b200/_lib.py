@@ -30,6 +30,7 @@ SIGNATURES = {
     "rsdft_gpu_sync_to_host": (_c_int, [_vp]),
     "rsdft_gpu_sync_to_device": (_c_int, [_vp]),
     "rsdft_gpu_hamiltonian": (_c_int, [_c_int, _c_int, _vp, _vp, _c_int, _c_int, _c_int, _c_int]),
+    "rsdft_gpu_hamiltonian_noalloc": (_c_int, [_c_int, _c_int, _vp, _vp, _c_int, _c_int, _c_int, _c_int]),
     "rsdft_gpu_conjugate_gradient": (_c_int, [_c_int, _c_int, _c_int, _c_int, _c_int, _vp, _vp, _vp, _c_int,
                                               _c_int, _c_int, _c_int]),
     "rsdft_gpu_gram_schmidt": (_c_int, [_c_int, _c_int, _c_int, _c_int, _vp, _c_long, _c_int, _c_int, _c_int]),

@@ -133,6 +133,12 @@ class RsdftGpu:
         _lib.call("rsdft_gpu_hamiltonian", k, s, _ptr(tpsi, name="tpsi"), _ptr(htpsi, name="htpsi"), n1, n2, ib1,
                   ib2)
 
+    def hamiltonian_noalloc(self, k, s, tpsi, htpsi, n1, n2, ib1, ib2) -> None:
+        """H psi without any device allocation (static 4 MiB scratch; see the
+        header).  tpsi/htpsi must be device tensors or registered arrays."""
+        _lib.call("rsdft_gpu_hamiltonian_noalloc", k, s, _ptr(tpsi, name="tpsi"), _ptr(htpsi, name="htpsi"), n1, n2,
+                  ib1, ib2)
+
     def conjugate_gradient(self, n1, n2, MB, k, s, unk, esp, res, *, ncg=3, mloop=3, ipc=4,
                            mode=MODE_FP64) -> None:
         """Reference defaults: Ncg = 3 (cg_module.f90:23), mloop = 3, IPC = 4."""

@@ -14,6 +14,7 @@
 //     2*Md+1 z values in a register queue, the x/y neighbours of the current
 //     plane come from a shared-memory tile with an Md-wide periodic halo.
 #include <algorithm>
+#include <mutex>
 
 #include "common.cuh"
 #include "kernels.cuh"
@@ -654,4 +655,121 @@ extern "C" int rsdft_gpu_hamiltonian(int k, int s, const double* tpsi, double* h
     RS_CHECK(hpsi_device<double>(dpsi, dh, ld, nb, s, nullptr));
     RS_CHECK(wf_release(htpsi, dh, ld, nb, sh));
     return RSDFT_OK;
+}
+
+// ------------------------------------------------- allocation-free hamiltonian
+// rsdft_gpu_hamiltonian_noalloc: the same H psi, for callers that must not
+// allocate device memory during the call.  Its only scratch, the projection
+// coefficients uVunk(nzlma, nb), lives in the file-scope array below, which
+// every GPU that loads this library holds until the process exits.  In host
+// code the array's name is a host-side stand-in, not a device address, so the
+// kernel is given the address cudaGetSymbolAddress returns for the current
+// device (looked up on the first call on each device).
+namespace rsdft {
+namespace {
+
+static __device__ __align__(256) double g_hpsi_noalloc_uvunk[RSDFT_NOALLOC_SCRATCH_VALUES];
+
+constexpr int kMaxDevices = 64;
+std::mutex g_noalloc_mutex;
+double* g_noalloc_addr[kMaxDevices] = {};
+
+int noalloc_scratch(double** out) {
+    int dev = -1;
+    RS_CUDA(cudaGetDevice(&dev));
+    if (dev < 0 || dev >= kMaxDevices) {
+        set_error("hamiltonian_noalloc: device ordinal %d outside 0..%d", dev, kMaxDevices - 1);
+        return RSDFT_EUNSUP;
+    }
+    if (dev != ctx().device) {
+        set_error("hamiltonian_noalloc: current device %d is not the device %d given to rsdft_gpu_init", dev,
+                  ctx().device);
+        return RSDFT_EINVAL;
+    }
+    std::lock_guard<std::mutex> lock(g_noalloc_mutex);
+    if (!g_noalloc_addr[dev]) {
+        void* p = nullptr;
+        const cudaError_t e = cudaGetSymbolAddress(&p, g_hpsi_noalloc_uvunk);
+        if (e != cudaSuccess || !p) {
+            set_error("hamiltonian_noalloc: cudaGetSymbolAddress of the static scratch failed on device %d: %s", dev,
+                      cudaGetErrorString(e));
+            return RSDFT_ECUDA;
+        }
+        g_noalloc_addr[dev] = static_cast<double*>(p);
+    }
+    *out = g_noalloc_addr[dev];
+    return RSDFT_OK;
+}
+
+// H psi on device-visible blocks with uVunk in the static scratch.  The
+// projection kernel writes every uVunk(lma, b) of the call before the stencil
+// reads it, so nothing left from an earlier call is ever read.
+int hpsi_static_scratch(const double* psi, double* hpsi, long ld, int nb, int spin) {
+    Context& c = ctx();
+    if (!c.vloc) {
+        set_error("hamiltonian_noalloc: rsdft_gpu_set_vloc has not been called");
+        return RSDFT_ENOTINIT;
+    }
+    const bool nl = c.nl_set && c.nzlma > 0;
+    double* uvunk = nullptr;
+    if (nl) {
+        RS_CHECK(noalloc_scratch(&uvunk));
+        launch(k_nl_project<double>, dim3(c.ngroup, div_up(nb, 8)), 256, 0, c.stream, psi, ld, nb, c.grp_lma0,
+               c.grp_cnt, c.lma_ptr, c.jjp, c.uv, c.iuv, c.dV, uvunk, c.nzlma, (const int*)nullptr);
+        RS_LAUNCH();
+    }
+    StencilArgs<double> a{};
+    a.psi = psi;
+    a.hpsi = hpsi;
+    a.ld = ld;
+    a.n1 = c.n1;
+    a.n2 = c.n2;
+    a.n3 = c.n3;
+    a.vloc = c.vloc + (long)(spin - 1) * c.ml;
+    a.pt_ptr = nl ? c.pt_ptr : nullptr;
+    a.pt_lma = c.pt_lma;
+    a.pt_uv = c.pt_uv;
+    a.uvunk = uvunk;
+    a.nzlma = c.nzlma;
+    a.gpt_ptr = nl ? c.gpt_ptr : nullptr;
+    a.gpt_grp = c.gpt_grp;
+    a.gpt_uv4 = c.gpt_uv4;
+    return launch_stencil<double>(a, c.sc, c.md, nb, c.stream);
+}
+
+}  // namespace
+}  // namespace rsdft
+
+extern "C" int rsdft_gpu_hamiltonian_noalloc(int k, int s, const double* tpsi, double* htpsi, int n1, int n2,
+                                             int ib1, int ib2) {
+    RS_CHECK(require_grid());
+    Context& c = ctx();
+    if (k != 1) {
+        set_error("hamiltonian_noalloc: k=%d, only the Gamma point (k=1) is supported", k);
+        return RSDFT_EUNSUP;
+    }
+    if (s < 1 || s > c.nspin) {
+        set_error("hamiltonian_noalloc: s=%d outside 1..%d", s, c.nspin);
+        return RSDFT_EINVAL;
+    }
+    const long ld = (long)n2 - n1 + 1;
+    const int nb = ib2 - ib1 + 1;
+    if (ld != c.ml || nb < 1 || nb > 65535) {
+        set_error("hamiltonian_noalloc: n2-n1+1=%ld must equal ML=%ld and 1 <= ib2-ib1+1 <= 65535", ld, c.ml);
+        return RSDFT_EINVAL;
+    }
+    if (c.nl_set && (long)nb * c.nzlma > RSDFT_NOALLOC_SCRATCH_VALUES) {
+        set_error("hamiltonian_noalloc: %d bands x %d projectors = %ld scratch values exceed the static maximum "
+                  "%ld (%ld MiB); call it on at most %ld bands at a time",
+                  nb, c.nzlma, (long)nb * c.nzlma, (long)RSDFT_NOALLOC_SCRATCH_VALUES,
+                  (long)RSDFT_NOALLOC_SCRATCH_VALUES * 8 / (1 << 20), (long)RSDFT_NOALLOC_SCRATCH_VALUES / c.nzlma);
+        return RSDFT_EINVAL;
+    }
+    void *dpsi = nullptr, *dh = nullptr;
+    if (!resolve(tpsi, &dpsi) || !resolve(htpsi, &dh)) {
+        set_error("hamiltonian_noalloc: tpsi and htpsi must be device memory or lie in a registered wavefunction "
+                  "(this entry point stages nothing)");
+        return RSDFT_EINVAL;
+    }
+    return hpsi_static_scratch(static_cast<const double*>(dpsi), static_cast<double*>(dh), ld, nb, s);
 }
