@@ -195,7 +195,7 @@ int rsdft_gpu_finalize(void) {
     c.regs.clear();
     void* ptrs[] = {c.err_flag, c.vloc, c.vloc32, c.lma_ptr, c.jjp, c.uv, c.uv32, c.iuv, c.amap, c.duv,
                     c.grp_lma0, c.grp_cnt, c.pt_ptr, c.pt_lma, c.pt_uv, c.pt_uv32,
-                    c.gpt_ptr, c.gpt_grp, c.gpt_uv4, c.gpt_uv4_32};
+                    c.gpt_ptr, c.gpt_grp, c.gpt_uv4, c.gpt_uv4_32, c.nl_pts, c.nl_ptr};
     for (void* p : ptrs)
         if (p) cudaFree(p);
     if (c.blas) cublasDestroy(c.blas);
@@ -384,12 +384,23 @@ int rsdft_gpu_set_nonlocal(int nzlma, const int* lma_ptr, const int* jjp, const 
             for (int k = 0; k < gc[g]; ++k) guv[(size_t)q * 4 + k] = huv[hptr[l0 + k] + (j - hptr[l0])];
         }
     }
+    // covered points and their entry ranges, for the scatter after the stencil
+    std::vector<int> npts, nptr;
+    for (long p = 0; p < c.ml; ++p)
+        if (gcnt[p + 1] > gcnt[p]) {
+            npts.push_back((int)p);
+            nptr.push_back(gcnt[p]);
+        }
+    nptr.push_back(gcnt[c.ml]);
     gcnt.resize(c.ml + 8, gcnt[c.ml]);  // padding for vector reads past the end
     std::vector<float> guv32(guv.begin(), guv.end());
     RS_CHECK(upload(&c.gpt_ptr, gcnt.data(), gcnt.size()));
     RS_CHECK(upload(&c.gpt_grp, ggrp.data(), ggrp.size()));
     RS_CHECK(upload(&c.gpt_uv4, guv.data(), guv.size()));
     RS_CHECK(upload(&c.gpt_uv4_32, guv32.data(), guv32.size()));
+    RS_CHECK(upload(&c.nl_pts, npts.data(), npts.size()));
+    RS_CHECK(upload(&c.nl_ptr, nptr.data(), nptr.size()));
+    c.nl_npt = (int)npts.size();
     std::vector<float> huv32(huv.begin(), huv.end()), puv32(puv.begin(), puv.end());
     RS_CHECK(upload(&c.lma_ptr, hptr.data(), hptr.size()));
     RS_CHECK(upload(&c.jjp, hjjp.data(), hjjp.size()));

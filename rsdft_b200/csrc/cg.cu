@@ -12,24 +12,11 @@
 // order: results are bit-reproducible run to run.
 #include <cmath>
 
+#include "cgvec.cuh"
 #include "common.cuh"
 #include "kernels.cuh"
 
 namespace rsdft {
-
-constexpr int VT = 256;           // threads per vector CTA
-constexpr int VITEMS = 8;         // elements per thread
-constexpr int VCHUNK = VT * VITEMS;
-
-struct CGScal {
-    double *E, *E1, *rb, *gkgk, *res, *u11, *u21, *W, *rr0, *rr1, *pa, *pb, *bk, *dots;
-    int *active, *pc_active, *reject;
-};
-
-template <typename T>
-struct CGVec {
-    T *x, *hx, *hp, *g, *Pg, *p, *r, *q;  // q = preconditioner search direction
-};
 
 // ----------------------------------------------------------- reductions
 __global__ void k_finish(const double* __restrict__ part, int nchunk, int K, int nb, double scale,
@@ -103,28 +90,6 @@ __global__ void __launch_bounds__(VT) k_cg_g(CGVec<T> v, long ld, long n, const 
     if (threadIdx.x == 0) part[(long)b * gridDim.x + blockIdx.x] = s;
 }
 
-// 7-point operator of precond_cg_mat2_omp at point i (E0 = 0)
-template <typename T>
-__device__ __forceinline__ T pc_apply(const T* __restrict__ f, long i, int n1, int n2, int n3, T d, T c1, T c2,
-                                      T c3) {
-    const long pl = (long)n1 * n2;
-    const int i1 = (int)(i % n1);
-    const int i2 = (int)((i / n1) % n2);
-    const int i3 = (int)(i / pl);
-    const long xm = i1 == 0 ? i + n1 - 1 : i - 1, xp = i1 == n1 - 1 ? i - n1 + 1 : i + 1;
-    const long ym = i2 == 0 ? i + pl - n1 : i - n1, yp = i2 == n2 - 1 ? i - pl + n1 : i + n1;
-    const long zm = i3 == 0 ? i + pl * (n3 - 1) : i - pl, zp = i3 == n3 - 1 ? i - pl * (n3 - 1) : i + pl;
-    T v = d * f[i];
-    v = v + c1 * (__ldg(f + xp) + __ldg(f + xm)) + c2 * (__ldg(f + yp) + __ldg(f + ym)) +
-        c3 * (__ldg(f + zp) + __ldg(f + zm));
-    return v;
-}
-
-struct PcArgs {
-    int n1, n2, n3;
-    double d, c1, c2, c3;
-};
-
 // P0: Pg = g; r = g - A g; q = r; partial |r|^2  (cgpc_hprsdft_module.f90:161-175)
 template <typename T>
 __global__ void __launch_bounds__(VT) k_pc0(CGVec<T> v, long ld, long n, PcArgs pa, double* __restrict__ part,
@@ -135,18 +100,21 @@ __global__ void __launch_bounds__(VT) k_pc0(CGVec<T> v, long ld, long n, PcArgs 
     const long off = (long)b * ld, base = (long)blockIdx.x * VCHUNK;
     const T* g = v.g + off;
     double acc = 0.0;
+    int i1, i2, i3;
+    pc_coords(base + threadIdx.x, pa, i1, i2, i3);
 #pragma unroll
     for (int it = 0; it < VITEMS; ++it) {
         const long i = base + it * VT + threadIdx.x;
         if (i < n) {
             const T gi = g[i];
-            const T f = pc_apply<T>(g, i, pa.n1, pa.n2, pa.n3, (T)pa.d, (T)pa.c1, (T)pa.c2, (T)pa.c3);
+            const T f = pc_apply<T>(g, i, i1, i2, i3, pa);
             const T r = gi - f;
             v.Pg[off + i] = gi;
             v.r[off + i] = r;
             v.q[off + i] = r;
             acc = fma((double)r, (double)r, acc);
         }
+        pc_step(pa, i1, i2, i3);
     }
     double s = block_sum<VT>(acc, sh);
     if (threadIdx.x == 0) part[(long)b * gridDim.x + blockIdx.x] = s;
@@ -162,14 +130,17 @@ __global__ void __launch_bounds__(VT) k_pc1(CGVec<T> v, long ld, long n, PcArgs 
     const long off = (long)b * ld, base = (long)blockIdx.x * VCHUNK;
     const T* q = v.q + off;
     double acc = 0.0;
+    int i1, i2, i3;
+    pc_coords(base + threadIdx.x, pa, i1, i2, i3);
 #pragma unroll
     for (int it = 0; it < VITEMS; ++it) {
         const long i = base + it * VT + threadIdx.x;
         if (i < n) {
-            const T f = pc_apply<T>(q, i, pa.n1, pa.n2, pa.n3, (T)pa.d, (T)pa.c1, (T)pa.c2, (T)pa.c3);
+            const T f = pc_apply<T>(q, i, i1, i2, i3, pa);
             v.hp[off + i] = f;
             acc = fma((double)q[i], (double)f, acc);
         }
+        pc_step(pa, i1, i2, i3);
     }
     double s = block_sum<VT>(acc, sh);
     if (threadIdx.x == 0) part[(long)b * gridDim.x + blockIdx.x] = s;
@@ -466,22 +437,25 @@ static int cg_run(T* x, long ld, int mb, int spin, double* esp, double* res, int
     v.r = base + 5 * vec;
     v.q = base + 6 * vec;
     double* scal = nullptr;
-    RS_CHECK(workspace_t("cg_scal", (size_t)mb * 20, &scal));
+    RS_CHECK(workspace_t("cg_scal", (size_t)mb * (20 + SS_STRIDE + SS_MAXM), &scal));
     CGScal s{};
     s.E = scal; s.E1 = scal + mb; s.rb = scal + 2 * mb; s.gkgk = scal + 3 * mb; s.res = scal + 4 * mb;
     s.u11 = scal + 5 * mb; s.u21 = scal + 6 * mb; s.W = scal + 7 * mb; s.rr0 = scal + 8 * mb;
     s.rr1 = scal + 9 * mb; s.pa = scal + 10 * mb; s.pb = scal + 11 * mb; s.bk = scal + 12 * mb;
     s.dots = scal + 13 * mb;  // 6 per band
+    double* ss = scal + 20 * mb;                 // s-step Gram / g-dot slots, SS_STRIDE per band
+    double* cz = ss + (size_t)SS_STRIDE * mb;    // s-step coefficients, SS_MAXM per band
     int* flags = nullptr;
     RS_CHECK(workspace_t("cg_flags", (size_t)mb * 3, &flags));
     s.active = flags; s.pc_active = flags + mb; s.reject = flags + 2 * mb;
     double* part = nullptr;
-    RS_CHECK(workspace_t("cg_part", (size_t)mb * nchunk * 6, &part));
+    RS_CHECK(workspace_t("cg_part", (size_t)mb * nchunk * 8, &part));
 
     const dim3 vg(nchunk, mb);
     const int sb = div_up(mb, 128);
     const double dV = c.dV;
-    PcArgs pa{c.n1, c.n2, c.n3, c.pc.c - 0.0, c.pc.c1, c.pc.c2, c.pc.c3};
+    PcArgs pa{c.n1, c.n2, c.n3, VT % c.n1, (VT / c.n1) % c.n2, VT / (c.n1 * c.n2),
+              c.pc.c - 0.0, c.pc.c1, c.pc.c2, c.pc.c3};
     auto finish = [&](int K, double scale, double* out, const int* act) {
         launch(k_finish, div_up((long)mb * K, 128), 128, 0, st, part, nchunk, K, mb, scale, out, act);
     };
@@ -501,35 +475,43 @@ static int cg_run(T* x, long ld, int mb, int spin, double* esp, double* res, int
         const int last = icg == ncg + 1;
         launch(s_top, sb, 128, 0, st, s, mb, last);
         if (last) break;
-        // --- preconditioning (Pgk = gk on entry)
-        if (ipc == 4 && mloop > 0) {
-            launch(k_pc0<T>, vg, VT, 0, st, v, ld, n, pa, part, s.active);
-            finish(1, 1.0, s.rr1, s.active);
-            launch(s_pc0, sb, 128, 0, st, s, mb);
-            for (int il = 1; il <= mloop; ++il) {
-                launch(k_pc1<T>, vg, VT, 0, st, v, ld, n, pa, part, s.pc_active);
-                finish(1, 1.0, s.dots, s.pc_active);
-                launch(s_pc1, sb, 128, 0, st, s, mb);
-                const int lastl = il == mloop;
-                launch(k_pc2<T>, vg, VT, 0, st, v, ld, n, s.pa, lastl, part, s.pc_active);
-                if (lastl) break;
-                finish(1, 1.0, s.rr1, s.pc_active);
-                launch(s_pc2, sb, 128, 0, st, s, mb);
-                launch(k_pc3<T>, vg, VT, 0, st, v, ld, n, s.pb, s.pc_active);
-            }
+        if (ipc == 4 && mloop >= 1 && mloop <= SS_MAXM) {
+            // --- preconditioner, rb = <Pg|g> dV and the search direction p
+            // in mloop + 2 passes (s-step form; w_j in r, q, Pg, hp, which
+            // are free until hpsi(p))
+            const SSVec<T> sv{{v.r, v.q, v.Pg, v.hp}};
+            RS_CHECK(sstep_precond<T>(v.g, sv, v.p, ld, mb, mloop, icg == 1, s, ss, cz, part, pa, dV));
         } else {
-            RS_CUDA(cudaMemcpyAsync(v.Pg, v.g, vec * sizeof(T), cudaMemcpyDeviceToDevice, st));
+            // --- preconditioning (Pgk = gk on entry)
+            if (ipc == 4 && mloop > 0) {
+                launch(k_pc0<T>, vg, VT, 0, st, v, ld, n, pa, part, s.active);
+                finish(1, 1.0, s.rr1, s.active);
+                launch(s_pc0, sb, 128, 0, st, s, mb);
+                for (int il = 1; il <= mloop; ++il) {
+                    launch(k_pc1<T>, vg, VT, 0, st, v, ld, n, pa, part, s.pc_active);
+                    finish(1, 1.0, s.dots, s.pc_active);
+                    launch(s_pc1, sb, 128, 0, st, s, mb);
+                    const int lastl = il == mloop;
+                    launch(k_pc2<T>, vg, VT, 0, st, v, ld, n, s.pa, lastl, part, s.pc_active);
+                    if (lastl) break;
+                    finish(1, 1.0, s.rr1, s.pc_active);
+                    launch(s_pc2, sb, 128, 0, st, s, mb);
+                    launch(k_pc3<T>, vg, VT, 0, st, v, ld, n, s.pb, s.pc_active);
+                }
+            } else {
+                RS_CUDA(cudaMemcpyAsync(v.Pg, v.g, vec * sizeof(T), cudaMemcpyDeviceToDevice, st));
+            }
+            RS_LAUNCH();
+            // --- rb = <Pg|g> dV; search direction
+            {
+                DotPairs<1> pr{{0}, {1}};
+                launch(k_multidot<T, 2, 1>, vg, VT, 0, st, v.Pg, v.g, nullptr, nullptr, ld, n, pr, part, s.active);
+                finish(1, dV, s.rb, s.active);
+            }
+            launch(s_p, sb, 128, 0, st, s, mb, icg == 1);
+            launch(k_cg_p<T>, vg, VT, 0, st, v, ld, n, s.bk, icg == 1, s.active);
+            RS_LAUNCH();
         }
-        RS_LAUNCH();
-        // --- rb = <Pg|g> dV; search direction
-        {
-            DotPairs<1> pr{{0}, {1}};
-            launch(k_multidot<T, 2, 1>, vg, VT, 0, st, v.Pg, v.g, nullptr, nullptr, ld, n, pr, part, s.active);
-            finish(1, dV, s.rb, s.active);
-        }
-        launch(s_p, sb, 128, 0, st, s, mb, icg == 1);
-        launch(k_cg_p<T>, vg, VT, 0, st, v, ld, n, s.bk, icg == 1, s.active);
-        RS_LAUNCH();
         RS_CHECK(hpsi_device<T>(v.p, v.hp, ld, mb, spin, s.active));
         // --- six dots: <x|x>, <p|x>, <p|p>, <x|Hx>, <p|Hx>, <p|Hp>
         {

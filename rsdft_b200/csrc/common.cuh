@@ -88,6 +88,9 @@ struct Context {
     int* gpt_grp = nullptr;     // first projector of the group
     double* gpt_uv4 = nullptr;  // 4 projector values of the group at the point
     float* gpt_uv4_32 = nullptr;
+    int nl_npt = 0;             // grid points covered by at least one sphere
+    int* nl_pts = nullptr;      // nl_npt: those points, ascending
+    int* nl_ptr = nullptr;      // nl_npt+1: their first entry in the group CSR
     std::vector<int> h_amap;
 
     // workspace

@@ -1,18 +1,16 @@
 // hpsi on sm_100a: H psi = T psi + Vloc psi + V_nl psi for a batch of bands.
 //
-// Two kernels per call:
 //  1. k_nl_project: uVunk(lma, b) = iuV dV sum_j uV(j) psi(JJP(j), b)
-//     (ps_nloc2_op_module.f90:161-175).  One warp per band, lanes stride the
-//     sphere's point list, the projectors of one sphere (same point list)
-//     share each gathered psi value; fixed-order shuffle-tree reduction.
-//  2. k_stencil: the Md-order periodic FD Laplacian (kinetic_sol_module.f90:
-//     72-77, 129-149) fused with the Vloc multiply (localpot_module.f90:73)
-//     and the nonlocal scatter-add (ps_nloc2_op_module.f90:255-263), the
-//     scatter turned into a per-point gather over a point-major CSR so the
-//     sum is deterministic.  2.5-D blocking: a CTA owns a TX x 16 column tile
-//     of one band and marches along z; each thread keeps its column's
-//     2*Md+1 z values in a register queue, the x/y neighbours of the current
-//     plane come from a shared-memory tile with an Md-wide periodic halo.
+//     (ps_nloc2_op_module.f90:161-175), one sphere group x 32 bands per CTA.
+//  2. k_stencil_tma: the Md-order periodic FD Laplacian (kinetic_sol_module.
+//     f90:72-77, 129-149) fused with the Vloc multiply (localpot_module.f90:
+//     73): TMA-fed plane ring, z "push" march with register accumulators.
+//  3. k_nl_scatter: the nonlocal scatter-add (ps_nloc2_op_module.f90:
+//     255-263) turned into a per-point gather over a point-major CSR, so every
+//     sum is deterministic.
+//  Shapes the TMA kernel does not take (odd row widths, rows wider than 256
+//  elements) run k_stencil, a register-queue kernel with per-plane halo
+//  loads and the scatter fused in its epilogue.
 #include <algorithm>
 #include <mutex>
 
@@ -29,6 +27,15 @@ __device__ __forceinline__ int pwrap(int i, int n) {
 }
 
 // ------------------------------------------------------------ projection
+// A CTA takes one sphere group (up to 4 projectors sharing a point list) and
+// 32 bands, 4 per warp.  The group's point indices and projector values are
+// staged in shared memory a chunk at a time; each lane strides the points
+// and issues the 4 bands' gathers together.  Per (band, projector) the lanes
+// sum points lane, lane+32, ... in order, then a fixed xor-shuffle tree.
+constexpr int PJ_BW = 4;    // bands per warp
+constexpr int PJ_WARPS = 8;
+constexpr int PJ_CH = 512;  // sphere points staged per pass (multiple of 32)
+
 template <typename T>
 __global__ void __launch_bounds__(256) k_nl_project(const T* __restrict__ psi, long ld, int nb,
                                                     const int* __restrict__ grp_lma0,
@@ -39,34 +46,79 @@ __global__ void __launch_bounds__(256) k_nl_project(const T* __restrict__ psi, l
                                                     const int* __restrict__ iuv, double dV,
                                                     double* __restrict__ uvunk, int nzlma,
                                                     const int* __restrict__ band_active) {
+    __shared__ int s_j[PJ_CH];
+    __shared__ double s_u[4][PJ_CH];
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const int b = blockIdx.y * 8 + warp;
-    if (b >= nb) return;
-    if (band_active && !band_active[b]) return;
     const int g = blockIdx.x;
     const int l0 = grp_lma0[g], cnt = grp_cnt[g];
     const int js = lma_ptr[l0], n = lma_ptr[l0 + 1] - js;
-    const T* p = psi + (long)b * ld;
-    double acc[4] = {0.0, 0.0, 0.0, 0.0};
     int off[4];
 #pragma unroll
     for (int q = 0; q < 4; ++q) off[q] = q < cnt ? lma_ptr[l0 + q] : js;
-    for (int j = lane; j < n; j += 32) {
-        const double v = (double)__ldg(p + jjp[js + j]);
+    const int bw0 = (blockIdx.y * PJ_WARPS + warp) * PJ_BW;
+    bool act[PJ_BW];
+    const T* p[PJ_BW];
+#pragma unroll
+    for (int w = 0; w < PJ_BW; ++w) {
+        const int b = bw0 + w;
+        act[w] = b < nb && (!band_active || band_active[b]);
+        p[w] = psi + (long)(act[w] ? b : 0) * ld;
+    }
+    double acc[PJ_BW][4];
+#pragma unroll
+    for (int w = 0; w < PJ_BW; ++w)
+#pragma unroll
+        for (int q = 0; q < 4; ++q) acc[w][q] = 0.0;
+    for (int c0 = 0; c0 < n; c0 += PJ_CH) {
+        const int m = min(PJ_CH, n - c0);
+        __syncthreads();
+        for (int i = threadIdx.x; i < m; i += blockDim.x) {
+            s_j[i] = jjp[js + c0 + i];
+#pragma unroll
+            for (int q = 0; q < 4; ++q) s_u[q][i] = q < cnt ? uv[off[q] + c0 + i] : 0.0;
+        }
+        __syncthreads();
+#pragma unroll 2
+        for (int j = lane; j < m; j += 32) {
+            const int jj = s_j[j];
+            double v[PJ_BW];
+#pragma unroll
+            for (int w = 0; w < PJ_BW; ++w) v[w] = act[w] ? (double)__ldg(p[w] + jj) : 0.0;
+#pragma unroll
+            for (int q = 0; q < 4; ++q) {
+                if (q < cnt) {
+                    const double u = s_u[q][j];
+#pragma unroll
+                    for (int w = 0; w < PJ_BW; ++w) acc[w][q] = fma(u, v[w], acc[w][q]);
+                }
+            }
+        }
+    }
+#pragma unroll
+    for (int w = 0; w < PJ_BW; ++w)
 #pragma unroll
         for (int q = 0; q < 4; ++q)
-            if (q < cnt) acc[q] = fma(__ldg(uv + off[q] + j), v, acc[q]);
-    }
 #pragma unroll
-    for (int q = 0; q < 4; ++q) {
-#pragma unroll
-        for (int s = 16; s > 0; s >>= 1) acc[q] += __shfl_xor_sync(0xffffffffu, acc[q], s);
-    }
+            for (int s = 16; s > 0; s >>= 1) acc[w][q] += __shfl_xor_sync(0xffffffffu, acc[w][q], s);
     if (lane == 0) {
 #pragma unroll
-        for (int q = 0; q < 4; ++q)
-            if (q < cnt) uvunk[(long)b * nzlma + l0 + q] = iuv[l0 + q] * dV * acc[q];
+        for (int w = 0; w < PJ_BW; ++w) {
+            if (!act[w]) continue;
+#pragma unroll
+            for (int q = 0; q < 4; ++q)
+                if (q < cnt) uvunk[(long)(bw0 + w) * nzlma + l0 + q] = iuv[l0 + q] * dV * acc[w][q];
+        }
     }
+}
+
+template <typename T>
+static int launch_project(const T* psi, long ld, int nb, double* uvunk, const int* band_active, cudaStream_t st) {
+    const Context& c = ctx();
+    dim3 grid(c.ngroup, div_up(nb, PJ_WARPS * PJ_BW));
+    launch(k_nl_project<T>, grid, 256, 0, st, psi, ld, nb, c.grp_lma0, c.grp_cnt, c.lma_ptr, c.jjp, c.uv, c.iuv,
+           c.dV, uvunk, c.nzlma, band_active);
+    RS_LAUNCH();
+    return RSDFT_OK;
 }
 
 // -------------------------------------------------------------- stencil
@@ -163,61 +215,109 @@ __global__ void __launch_bounds__(TX * 16) k_stencil(StencilArgs<T> a, StencilCo
 }
 
 template <typename T>
-struct Vec2;
+struct Vec16;
 template <>
-struct Vec2<double> {
+struct Vec16<double> {
     using t = double2;
+    __device__ static __forceinline__ void get(const t& v, double* o) {
+        o[0] = v.x;
+        o[1] = v.y;
+    }
+    __device__ static __forceinline__ t make(const double* o) { return make_double2(o[0], o[1]); }
 };
 template <>
-struct Vec2<float> {
-    using t = float2;
+struct Vec16<float> {
+    using t = float4;
+    __device__ static __forceinline__ void get(const t& v, float* o) {
+        o[0] = v.x;
+        o[1] = v.y;
+        o[2] = v.z;
+        o[3] = v.w;
+    }
+    __device__ static __forceinline__ t make(const float* o) { return make_float4(o[0], o[1], o[2], o[3]); }
 };
 
-// Shared-memory padding (elements) on each side of a row: >= the even
-// rounding of Md, and a multiple of 16 bytes so bulk copies land aligned.
-template <typename T, int MD>
-__host__ __device__ constexpr int ring_pad() {
-    return sizeof(T) == 8 ? ((MD + 1) / 2) * 2 : ((MD + 3) / 4) * 4;
+struct TmaMaps {
+    CUtensorMap full, edge, mid, wrap;  // psi boxes of height TY + 2 Md, TY + Md, TY, Md
+    CUtensorMap vloc;                   // Vloc box of height TY
+};
+
+// One arrival's z pushes for accumulator slot U (compile time): outputs
+// U + m (first touch at m = Md) and U - m get cz_m c, slot U gets the in-plane
+// part when the plane is one of the tile's own, and slot U + Md + 1 (the
+// output completed by this arrival) is written when hp is set.
+template <typename T, int MD, int NP, int BY, int VX, int U>
+__device__ __forceinline__ void push_body(T (&acc)[2 * MD + 1][NP], const T* c, const T* in, bool inner,
+                                          const StencilCoef& cf, T* hp, int n1) {
+    using VT = Vec16<T>;
+    using V = typename VT::t;
+    constexpr int Q = 2 * MD + 1;
+#pragma unroll
+    for (int i = 0; i < NP; ++i) {
+        acc[(U + MD) % Q][i] = (T)cf.cz[MD - 1] * c[i];
+#pragma unroll
+        for (int m = 1; m < MD; ++m) acc[(U + m) % Q][i] += (T)cf.cz[m - 1] * c[i];
+#pragma unroll
+        for (int m = 1; m <= MD; ++m) acc[(U + Q - m) % Q][i] += (T)cf.cz[m - 1] * c[i];
+        if (inner) acc[U][i] += in[i];
+    }
+    if (hp) {
+#pragma unroll
+        for (int r = 0; r < BY; ++r)
+            *reinterpret_cast<V*>(hp + (long)r * n1) = VT::make(&acc[(U + MD + 1) % Q][r * VX]);
+    }
 }
 
-struct WsMaps {
-    CUtensorMap full, edge, mid, wrap;  // box heights ROWS, ROWS - Md, TY, Md
-};
+// Runtime slot -> compile-time slot: only the short push runs per case, so
+// the loop body is not replicated 2 Md + 1 times.
+template <typename T, int MD, int NP, int BY, int VX>
+__device__ __forceinline__ void push_slot(int u, T (&acc)[2 * MD + 1][NP], const T* c, const T* in, bool inner,
+                                          const StencilCoef& cf, T* hp, int n1) {
+    constexpr int Q = 2 * MD + 1;
+#define RS_PUSH_CASE(K)                                                                  \
+    case K:                                                                              \
+        if constexpr (K < Q) push_body<T, MD, NP, BY, VX, K>(acc, c, in, inner, cf, hp, n1); \
+        break;
+    switch (u) {
+        RS_PUSH_CASE(0) RS_PUSH_CASE(1) RS_PUSH_CASE(2) RS_PUSH_CASE(3) RS_PUSH_CASE(4) RS_PUSH_CASE(5)
+        RS_PUSH_CASE(6) RS_PUSH_CASE(7) RS_PUSH_CASE(8) RS_PUSH_CASE(9) RS_PUSH_CASE(10) RS_PUSH_CASE(11)
+        RS_PUSH_CASE(12) RS_PUSH_CASE(13) RS_PUSH_CASE(14) RS_PUSH_CASE(15) RS_PUSH_CASE(16)
+        default: break;
+    }
+#undef RS_PUSH_CASE
+}
 
-// hpsi stencil, warp-specialized TMA pipeline.  A CTA owns TY full-width
-// rows (all n1 x) of one band and marches along z.
-//  * TMA warp: one 4-D tensor-map TMA per plane tile (TY + 2 Md rows, x from
-//    -PAD to n1 + PAD, the out-of-range pad columns arrive as zeros; periodic
-//    wrap in y by splitting the box at the boundary) into a ring of S
-//    shared-memory stages (full[] barriers); it reuses a stage once every
-//    consumer warp has released it (empty[]).
-//  * Pad warp: fills the periodic x pads of each landed tile and publishes
-//    it (ready[] barriers).
-//  * Consumer warps: each thread owns 2 (x) x BY (y) points; x neighbours from
-//    a register window of its rows, y neighbours from one 2-wide load per row
-//    of the y window, z neighbours from a register queue of 2 Md + 1 planes
-//    whose head is read from the stage Md planes ahead.  Epilogue: Vloc,
-//    nonlocal scatter (sphere-group CSR, uVunk column in shared memory).
-//  No CTA-wide barrier inside the z loop: warps drift, so one warp's memory
-//  latency overlaps other warps' arithmetic.
-template <typename T, int MD, int BY, int UNR>
-__global__ void __launch_bounds__(384, 1) k_stencil_ws(const __grid_constant__ WsMaps maps, StencilArgs<T> a,
-                                                      StencilCoef cf, int TY, int S, int ncw, int* __restrict__ err) {
-    using T2 = typename Vec2<T>::t;
-    constexpr int PAD = ring_pad<T, MD>();
-    constexpr int MD2 = ((MD + 1) / 2) * 2;  // even window half-width
-    constexpr int NW = 2 * MD2 + 2;           // x window per row (elements)
+// hpsi stencil + Vloc, TMA pipeline with a z "push" march.  A CTA owns TY
+// full-width rows of one band and marches along z over planes zs-Md ..
+// ze+Md-1.  One producer warp streams each plane (TY + 2 Md rows with the
+// periodic y wrap split into boxes, plus the Vloc rows of the tile) into a
+// ring of S shared-memory stages.  Each consumer thread owns VX (16 bytes)
+// x BY points.  When plane P lands the thread
+//  * forms the in-plane part of H psi at P (centre, Md x and y neighbours,
+//    the x window read with periodic offsets, Vloc),
+//  * adds cz_m psi(P) to the accumulators of the outputs P -+ m (m = 1..Md),
+//  * and writes output P - Md, which is then complete.
+// The 2 Md + 1 accumulators rotate through registers with compile-time
+// indices (a switch on the slot selects the push), so a stage is read only
+// while its own plane is current and the ring can stay shallow.
+template <typename T, int MD, int BY>
+__global__ void __launch_bounds__(384, 1) k_stencil_tma(const __grid_constant__ TmaMaps maps, StencilArgs<T> a,
+                                                       StencilCoef cf, int TY, int RS, int S, int ncw,
+                                                       int* __restrict__ err) {
+    using VT = Vec16<T>;
+    using V = typename VT::t;
+    constexpr int VX = 16 / (int)sizeof(T);
+    constexpr int MDX = (MD + VX - 1) / VX * VX;  // x window half-width, whole vectors
+    constexpr int NV = 1 + 2 * MDX / VX;           // vectors in the x window
+    constexpr int Q = 2 * MD + 1;                  // accumulator ring
+    constexpr int NP = VX * BY;                    // points per thread
     extern __shared__ __align__(128) unsigned char smem[];
     const int n1 = a.n1, n2 = a.n2, n3 = a.n3;
-    constexpr int RQ = 128 / (int)sizeof(T);      // row stride quantum: rows start on 128-byte boundaries
-    const int RS = (n1 + 2 * PAD + RQ - 1) / RQ * RQ;
     const int ROWS = TY + 2 * MD;
-    const int SE = ROWS * RS;
+    const int SE = (ROWS + TY) * RS;  // elements per stage: psi rows, then Vloc rows
     T* stages = reinterpret_cast<T*>(smem);
     uint64_t* full = reinterpret_cast<uint64_t*>(smem + (size_t)S * SE * sizeof(T));
-    uint64_t* ready = full + S;
-    uint64_t* empty = ready + S;
-    double* s_un = reinterpret_cast<double*>(empty + S);
+    uint64_t* empty = full + S;
 
     const int t = threadIdx.x;
     const int warp = t >> 5, lane = t & 31;
@@ -227,216 +327,202 @@ __global__ void __launch_bounds__(384, 1) k_stencil_ws(const __grid_constant__ W
     if (a.band_active && !a.band_active[band]) return;  // uniform per CTA
     const int y0 = blockIdx.x * TY;
     const int zs = zc * a.zlen;
-    const int ze = min(zs + a.zlen, n3);
-    const int zlen = ze - zs;
+    const int zlen = min(zs + a.zlen, n3) - zs;
+    const int nk = zlen + 2 * MD;  // arrival k <-> plane zs - Md + k
     const long plane = (long)n1 * n2;
-    const int nload = zlen + MD;  // ring index k <-> plane zs + k
 
     if (t == 0) {
         for (int s = 0; s < S; ++s) {
             mbar_init(&full[s], 1);
-            mbar_init(&ready[s], 1);
             mbar_init(&empty[s], ncw);
         }
         mbar_fence_init();
     }
-    if (a.gpt_ptr)
-        for (int i = t; i < a.nzlma; i += blockDim.x) s_un[i] = a.uvunk[(long)band * a.nzlma + i];
     __syncthreads();
 
     if (warp == ncw) {
-        // ------------------------------------------------- producer: TMA
-        const uint32_t bytes = (uint32_t)(SE * sizeof(T));
+        // ------------------------------------------------------ producer
         bool ok = true;
-        for (int k = 0; k < nload; ++k) {
-            const int slot = k % S;
-            if (k >= S && !mbar_wait(&empty[slot], ((k / S) - 1) & 1)) ok = false;
-            fence_proxy_async_smem();
-            __syncwarp();
-            if (lane == 0) {
-                T* dst = stages + (size_t)slot * SE;
-                const int zp = pwrap(zs + k, n3);
-                mbar_arrive_expect_tx(&full[slot], bytes);
-                if (y0 - MD >= 0 && y0 + TY + MD <= n2) {
-                    tma_load_4d(dst, &maps.full, -PAD, y0 - MD, zp, band, &full[slot]);
-                } else if (TY == n2) {
-                    tma_load_4d(dst, &maps.wrap, -PAD, n2 - MD, zp, band, &full[slot]);
-                    tma_load_4d(dst + MD * RS, &maps.mid, -PAD, 0, zp, band, &full[slot]);
-                    tma_load_4d(dst + (MD + TY) * RS, &maps.wrap, -PAD, 0, zp, band, &full[slot]);
-                } else if (y0 - MD < 0) {
-                    tma_load_4d(dst, &maps.wrap, -PAD, n2 - MD, zp, band, &full[slot]);
-                    tma_load_4d(dst + MD * RS, &maps.edge, -PAD, 0, zp, band, &full[slot]);
-                } else {
-                    tma_load_4d(dst, &maps.edge, -PAD, y0 - MD, zp, band, &full[slot]);
-                    tma_load_4d(dst + (TY + MD) * RS, &maps.wrap, -PAD, 0, zp, band, &full[slot]);
+        if (lane == 0) {
+            const uint32_t b_in = (uint32_t)((size_t)(ROWS + TY) * RS * sizeof(T));
+            const uint32_t b_out = (uint32_t)((size_t)TY * RS * sizeof(T));
+            for (int k = 0; k < nk; ++k) {
+                const int s = k % S;
+                if (k >= S && !mbar_wait(&empty[s], ((k / S) - 1) & 1)) ok = false;
+                T* dst = stages + (size_t)s * SE;
+                const int zp = pwrap(zs - MD + k, n3);
+                const bool inner = k >= MD && k < MD + zlen;
+                fence_proxy_async_smem();
+                mbar_arrive_expect_tx(&full[s], inner ? b_in : b_out);
+                if (!inner) {
+                    // halo planes only feed the z accumulators: the TY own rows
+                    tma_load_4d(dst + MD * RS, &maps.mid, 0, y0, zp, band, &full[s]);
+                    continue;
                 }
+                if (y0 - MD >= 0 && y0 + TY + MD <= n2) {
+                    tma_load_4d(dst, &maps.full, 0, y0 - MD, zp, band, &full[s]);
+                } else if (TY == n2) {
+                    tma_load_4d(dst, &maps.wrap, 0, n2 - MD, zp, band, &full[s]);
+                    tma_load_4d(dst + MD * RS, &maps.mid, 0, 0, zp, band, &full[s]);
+                    tma_load_4d(dst + (MD + TY) * RS, &maps.wrap, 0, 0, zp, band, &full[s]);
+                } else if (y0 - MD < 0) {
+                    tma_load_4d(dst, &maps.wrap, 0, n2 - MD, zp, band, &full[s]);
+                    tma_load_4d(dst + MD * RS, &maps.edge, 0, 0, zp, band, &full[s]);
+                } else {
+                    tma_load_4d(dst, &maps.edge, 0, y0 - MD, zp, band, &full[s]);
+                    tma_load_4d(dst + (TY + MD) * RS, &maps.wrap, 0, 0, zp, band, &full[s]);
+                }
+                tma_load_4d(dst + ROWS * RS, &maps.vloc, 0, y0, zp, 0, &full[s]);
             }
         }
-        if (!ok && lane == 0) atomicExch(err, 1);
-        return;
-    }
-    if (warp == ncw + 1) {
-        // ------------------------------------------ producer: periodic pads
-        // left pad x = -PAD..-1 <- x = n1-PAD..n1-1, right pad x = n1..n1+PAD-1
-        // <- x = 0..PAD-1; both are PAD contiguous elements, copied as pairs
-        bool ok = true;
-        constexpr int H = PAD / 2;  // pairs per pad
-        for (int kp = 0; kp < nload; ++kp) {
-            const int slot = kp % S;
-            if (!mbar_wait(&full[slot], (kp / S) & 1)) ok = false;
-            T* st = stages + (size_t)slot * SE;
-            for (int c = lane; c < ROWS * 2 * H; c += 32) {
-                const int r = c / (2 * H), i = c - r * (2 * H);
-                T* row = st + r * RS;
-                if (i < H)
-                    *reinterpret_cast<T2*>(row + 2 * i) = *reinterpret_cast<const T2*>(row + n1 + 2 * i);
-                else
-                    *reinterpret_cast<T2*>(row + n1 + PAD + 2 * (i - H)) =
-                        *reinterpret_cast<const T2*>(row + PAD + 2 * (i - H));
-            }
-            fence_proxy_async_smem();
-            __syncwarp();
-            if (lane == 0) mbar_arrive(&ready[slot]);
-        }
-        if (!ok && lane == 0) atomicExch(err, 1);
+        __syncwarp();
+        if (!ok) atomicExch(err, 1);
         return;
     }
 
     // ---------------------------------------------------------- consumers
-    const int nxp = n1 >> 1;
-    const int ncons = nxp * (TY / BY);
+    const int nxv = n1 / VX;
+    const int ncons = nxv * (TY / BY);
     const bool thr = t < ncons;
-    const int px = thr ? t % nxp : 0, py = thr ? t / nxp : 0;
-    const int x = 2 * px, yl = BY * py;
-    const T* __restrict__ p = a.psi + (long)band * a.ld;
-    T* __restrict__ h = a.hpsi + (long)band * a.ld;
-    bool rowok[BY];
-#pragma unroll
-    for (int r = 0; r < BY; ++r) rowok[r] = thr && (y0 + yl + r < n2);
+    const int px = thr ? t % nxv : 0, py = thr ? t / nxv : 0;
+    const int x = VX * px, yl = BY * py;
+    const int xw = x - MDX;  // first x of the periodic window
+    T* __restrict__ hb = a.hpsi + (long)band * a.ld + (long)n1 * (y0 + yl) + x;
+    const T c0 = (T)cf.c0;
 
-    // z queue: q[k][2r + c] = psi(x + c, y0 + yl + r, z - MD + k); UNR - 1
-    // extra slots so the loop can run UNR planes before shifting
-    T q[2 * MD + UNR][2 * BY];
+    T acc[Q][NP];
 #pragma unroll
-    for (int k = 0; k < 2 * MD; ++k) {
-        const T* pz = p + plane * pwrap(zs - MD + k, n3);
+    for (int q = 0; q < Q; ++q)
 #pragma unroll
-        for (int r = 0; r < BY; ++r) {
-            T2 v = {0, 0};
-            if (rowok[r]) v = __ldg(reinterpret_cast<const T2*>(pz + (long)n1 * (y0 + yl + r) + x));
-            q[k][2 * r] = v.x;
-            q[k][2 * r + 1] = v.y;
-        }
-    }
+        for (int i = 0; i < NP; ++i) acc[q][i] = (T)0;
+
     bool ok = true;
-    for (int kz0 = 0; kz0 < zlen; kz0 += UNR) {
+    int s = 0, u = 0;
+    uint32_t ph = 0;
+    for (int k = 0; k < nk; ++k) {
+        if (!mbar_wait(&full[s], ph)) ok = false;
+        const T* st = stages + (size_t)s * SE;
+        const bool inner = k >= MD && k < MD + zlen;  // uniform
+        T c[NP], in[NP];
+        if (inner) {
+            const T* sp = st + yl * RS + x;
 #pragma unroll
-        for (int u = 0; u < UNR; ++u) {
-            const int kz = kz0 + u;
-            if (kz >= zlen) break;  // uniform
-            const int z = zs + kz;
-            const int kh = kz + MD;
-            // epilogue operands, issued early so their latency overlaps the stencil
-            T2 vl[BY];
-            int sp[BY][3];
-#pragma unroll
-            for (int r = 0; r < BY; ++r) {
-                const long j = (long)x + (long)n1 * (y0 + yl + r) + plane * z;
-                vl[r].x = 0;
-                vl[r].y = 0;
-                sp[r][0] = sp[r][1] = sp[r][2] = 0;
-                if (rowok[r]) {
-                    vl[r] = __ldg(reinterpret_cast<const T2*>(a.vloc + j));
-                    if (a.gpt_ptr) {
-                        sp[r][0] = __ldg(a.gpt_ptr + j);
-                        sp[r][1] = __ldg(a.gpt_ptr + j + 1);
-                        sp[r][2] = __ldg(a.gpt_ptr + j + 2);
-                    }
-                }
-            }
-            if (!mbar_wait(&ready[kh % S], (kh / S) & 1)) ok = false;
-            {
-                const T* sh = stages + (size_t)(kh % S) * SE + PAD + x;
-#pragma unroll
-                for (int r = 0; r < BY; ++r) {
-                    const T2 v = *reinterpret_cast<const T2*>(sh + (MD + yl + r) * RS);
-                    q[2 * MD + u][2 * r] = v.x;
-                    q[2 * MD + u][2 * r + 1] = v.y;
-                }
-            }
-            if (kz < MD && !mbar_wait(&ready[kz % S], (kz / S) & 1)) ok = false;
-            const T* st = stages + (size_t)(kz % S) * SE + PAD + x;
-            T acc[2 * BY];
-#pragma unroll
-            for (int i = 0; i < 2 * BY; ++i) acc[i] = (T)cf.c0 * q[MD + u][i];
-#pragma unroll
-            for (int r = 0; r < BY; ++r) {
-                T w[NW];
-                const T* rp = st + (MD + yl + r) * RS - MD2;
-#pragma unroll
-                for (int k = 0; k < NW / 2; ++k) {
-                    const T2 v = *reinterpret_cast<const T2*>(rp + 2 * k);
-                    w[2 * k] = v.x;
-                    w[2 * k + 1] = v.y;
-                }
-#pragma unroll
-                for (int m = 1; m <= MD; ++m) {
-                    acc[2 * r] += (T)cf.cx[m - 1] * (w[MD2 - m] + w[MD2 + m]);
-                    acc[2 * r + 1] += (T)cf.cx[m - 1] * (w[MD2 + 1 - m] + w[MD2 + 1 + m]);
-                }
-            }
+            for (int i = 0; i < NP; ++i) in[i] = (T)0;
+            // y neighbours (the window also holds the thread's own rows)
 #pragma unroll
             for (int j = 0; j < BY + 2 * MD; ++j) {
-                const T2 v = *reinterpret_cast<const T2*>(st + (yl + j) * RS);
+                T v[VX];
+                VT::get(*reinterpret_cast<const V*>(sp + j * RS), v);
 #pragma unroll
                 for (int r = 0; r < BY; ++r) {
                     const int m = j - MD - r;
-                    if (m != 0 && m >= -MD && m <= MD) {
-                        const T c = (T)cf.cy[(m > 0 ? m : -m) - 1];
-                        acc[2 * r] += c * v.x;
-                        acc[2 * r + 1] += c * v.y;
+                    if (m == 0) {
+#pragma unroll
+                        for (int e = 0; e < VX; ++e) c[r * VX + e] = v[e];
+                    } else if (m >= -MD && m <= MD) {
+                        const T cy = (T)cf.cy[(m > 0 ? m : -m) - 1];
+#pragma unroll
+                        for (int e = 0; e < VX; ++e) in[r * VX + e] += cy * v[e];
                     }
                 }
             }
-            __syncwarp();
-            if (lane == 0) mbar_arrive(&empty[kz % S]);  // this warp is done with the stage
-#pragma unroll
-            for (int m = 1; m <= MD; ++m) {
-#pragma unroll
-                for (int i = 0; i < 2 * BY; ++i)
-                    acc[i] += (T)cf.cz[m - 1] * (q[MD + u - m][i] + q[MD + u + m][i]);
-            }
+            // x neighbours from the periodic window of each own row
 #pragma unroll
             for (int r = 0; r < BY; ++r) {
-                if (!rowok[r]) continue;
-                const long j = (long)x + (long)n1 * (y0 + yl + r) + plane * z;
-                T o0 = acc[2 * r] + vl[r].x * q[MD + u][2 * r];
-                T o1 = acc[2 * r + 1] + vl[r].y * q[MD + u][2 * r + 1];
-                if (a.gpt_ptr) {
-                    for (int e = sp[r][0]; e < sp[r][2]; ++e) {
-                        const int g = __ldg(a.gpt_grp + e);
-                        const T2 u01 = __ldg(reinterpret_cast<const T2*>(a.gpt_uv4 + 4L * e));
-                        const T2 u23 = __ldg(reinterpret_cast<const T2*>(a.gpt_uv4 + 4L * e + 2));
-                        const T c = u01.x * (T)s_un[g] + u01.y * (T)s_un[g + 1] + u23.x * (T)s_un[g + 2] +
-                                    u23.y * (T)s_un[g + 3];
-                        if (e < sp[r][1])
-                            o0 += c;
-                        else
-                            o1 += c;
-                    }
+                const T* rp = st + (MD + yl + r) * RS;
+                T w[NV * VX];
+#pragma unroll
+                for (int j = 0; j < NV; ++j) {
+                    int xx = xw + VX * j;
+                    xx += xx < 0 ? n1 : (xx >= n1 ? -n1 : 0);
+                    VT::get(*reinterpret_cast<const V*>(rp + xx), w + j * VX);
                 }
-                T2 o;
-                o.x = o0;
-                o.y = o1;
-                *reinterpret_cast<T2*>(h + j) = o;
+#pragma unroll
+                for (int e = 0; e < VX; ++e)
+#pragma unroll
+                    for (int m = 1; m <= MD; ++m)
+                        in[r * VX + e] += (T)cf.cx[m - 1] * (w[MDX + e - m] + w[MDX + e + m]);
+            }
+            // centre and local potential
+#pragma unroll
+            for (int r = 0; r < BY; ++r) {
+                T vl[VX];
+                VT::get(*reinterpret_cast<const V*>(sp + (ROWS + r) * RS), vl);
+#pragma unroll
+                for (int e = 0; e < VX; ++e) {
+                    const int i = r * VX + e;
+                    in[i] += (c0 + vl[e]) * c[i];
+                }
+            }
+        } else {
+#pragma unroll
+            for (int r = 0; r < BY; ++r)
+                VT::get(*reinterpret_cast<const V*>(st + (MD + yl + r) * RS + x), c + r * VX);
+        }
+        __syncwarp();
+        if (lane == 0) mbar_arrive(&empty[s]);  // this warp is done with the stage
+        // z pushes into the accumulator ring (slot = output arrival mod Q)
+        // and, from arrival 2 Md on, the write of the completed output k - Md
+        T* hp = (k >= 2 * MD && thr) ? hb + plane * (zs + k - 2 * MD) : nullptr;
+        push_slot<T, MD, NP, BY, VX>(u, acc, c, in, inner, cf, hp, n1);
+        if (++s == S) {
+            s = 0;
+            ph ^= 1u;
+        }
+        if (++u == Q) u = 0;
+    }
+    if (!ok) atomicExch(err, 1);
+}
+
+// Nonlocal scatter after the stencil: hpsi(p, b) += sum over the sphere
+// groups g covering p of sum_q uV(p, g, q) uVunk(g + q, b)
+// (ps_nloc2_op_module.f90:255-263), one thread per covered point and a chunk
+// of bands, SC_BU bands in flight at once.  A point's entries are taken in
+// projector order, so every sum has a fixed order.
+constexpr int SC_BU = 8;
+
+template <typename T>
+__global__ void __launch_bounds__(128) k_nl_scatter(T* __restrict__ hpsi, long ld, int nb, int bchunk,
+                                                   const int* __restrict__ nl_pts, const int* __restrict__ nl_ptr,
+                                                   int npt, const int* __restrict__ gpt_grp,
+                                                   const T* __restrict__ gpt_uv4, const double* __restrict__ uvunk,
+                                                   int nzlma, const int* __restrict__ band_active) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= npt) return;
+    const int p = nl_pts[i];
+    const int e0 = nl_ptr[i], e1 = nl_ptr[i + 1];
+    const int b0 = blockIdx.y * bchunk, b1 = min(nb, b0 + bchunk);
+    for (int b = b0; b < b1; b += SC_BU) {
+        bool act[SC_BU];
+        T o[SC_BU];
+#pragma unroll
+        for (int u = 0; u < SC_BU; ++u) {
+            const int bb = b + u;
+            act[u] = bb < b1 && (!band_active || band_active[bb]);
+            o[u] = act[u] ? hpsi[(long)bb * ld + p] : (T)0;
+        }
+        for (int e = e0; e < e1; ++e) {
+            // a group holds 1..4 projectors; missing ones have zero values
+            // and must not be read past the end of uVunk
+            const int g = __ldg(gpt_grp + e);
+            T uq[4];
+#pragma unroll
+            for (int q = 0; q < 4; ++q) uq[q] = __ldg(gpt_uv4 + 4L * e + q);
+#pragma unroll
+            for (int u = 0; u < SC_BU; ++u) {
+                if (!act[u]) continue;
+                const double* un = uvunk + (long)(b + u) * nzlma;
+                T c = uq[0] * (T)__ldg(un + g);
+#pragma unroll
+                for (int q = 1; q < 4; ++q)
+                    if (g + q < nzlma) c += uq[q] * (T)__ldg(un + g + q);
+                o[u] += c;
             }
         }
 #pragma unroll
-        for (int k = 0; k < 2 * MD; ++k)
-#pragma unroll
-            for (int i = 0; i < 2 * BY; ++i) q[k][i] = q[k + UNR][i];
+        for (int u = 0; u < SC_BU; ++u)
+            if (act[u]) hpsi[(long)(b + u) * ld + p] = o[u];
     }
-    if (!ok) atomicExch(err, 1);
 }
 
 template <typename T, int MD, int TX>
@@ -455,86 +541,89 @@ static void launch_stencil_md(const StencilArgs<T>& a, const StencilCoef& cf, in
         launch_stencil_tx<T, MD, 16>(a, cf, nb, st);
 }
 
-// Warp-specialized kernel geometry: tile height TY (multiple of BY, divides
-// n2, >= Md, and n2 == TY or n2 >= TY + Md), ring depth S >= Md + 3,
-// consumer threads (n1/2)(TY/BY) rounded up to warps, plus two producer warps
-// (TMA, pads), at most 384 threads.
-struct RingGeom {
-    int TY = 0, S = 0, threads = 0, ncw = 0;
+// Geometry of k_stencil_tma: tile height TY (multiple of BY, divides n2,
+// >= Md, and n2 == TY or n2 >= TY + Md), shared-memory row pitch RS (n1
+// rounded up to 128 bytes; the columns past n1 arrive as zeros and are never
+// read), ring depth S >= 3, consumer warps ncw, one producer warp, at most
+// 384 threads (the register budget of the 2 Md + 1 accumulators).
+struct TmaGeom {
+    int TY = 0, RS = 0, S = 0, ncw = 0, threads = 0;
     size_t smem = 0;
 };
 
 template <typename T, int MD, int BY>
-static RingGeom ring_geometry(int n1, int n2, int zlen, int nzlma) {
-    RingGeom best;
-    constexpr int PAD = ring_pad<T, MD>();
-    constexpr int RQ = 128 / (int)sizeof(T);
-    const int RS = (n1 + 2 * PAD + RQ - 1) / RQ * RQ;
-    if (n1 % (16 / (int)sizeof(T)) != 0 || n1 < PAD || RS > 256 || n2 < MD) return best;
-    const size_t budget = 220 * 1024 - (size_t)nzlma * 8;
-    int best_score = -1;
-    for (int TY = BY; TY <= std::min(n2, 96); TY += BY) {
-        if (n2 % TY != 0 || TY < MD || !(TY == n2 || n2 >= TY + MD) || TY + 2 * MD > 256) continue;
-        const int ncons = (n1 / 2) * (TY / BY);
-        const int ncw = (ncons + 31) / 32;
-        const int threads = 32 * (ncw + 2);
+static TmaGeom tma_geometry(int n1, int n2) {
+    TmaGeom best;
+    constexpr int VX = 16 / (int)sizeof(T);
+    constexpr int MDX = (MD + VX - 1) / VX * VX;
+    const int RS = (int)((((size_t)n1 * sizeof(T) + 127) / 128) * 128 / sizeof(T));
+    if (n1 % VX != 0 || n1 < MDX || RS > 256 || n2 < MD) return best;
+    const size_t budget = 220 * 1024;
+    double best_score = -1.0;
+    for (int TY = BY; TY <= std::min(n2, 256 - 2 * MD); TY += BY) {
+        if (n2 % TY != 0 || TY < MD || !(TY == n2 || n2 >= TY + MD)) continue;
+        const int ncw = ((n1 / VX) * (TY / BY) + 31) / 32;
+        const int threads = 32 * (ncw + 1);
         if (threads > 384) continue;
-        const size_t stage = (size_t)(TY + 2 * MD) * RS * sizeof(T);
-        int S = (int)std::min<size_t>(budget / (stage + 24), 16);
-        S = std::min(S, std::max(zlen + MD, MD + 3));
-        if (S < MD + 3) continue;
-        const int score = (int)(1000.0 * TY / (TY + 2 * MD)) * 100 + S;
+        const size_t stage = (size_t)(2 * TY + 2 * MD) * RS * sizeof(T);
+        const int S = (int)std::min<size_t>(budget / (stage + 16), 8);
+        if (S < 3) continue;
+        // halo overhead first, then busy threads, then ring depth
+        const double used = (double)((n1 / VX) * (TY / BY)) / threads;
+        const double score = 100.0 * TY / (TY + 2 * MD) + 10.0 * used + 0.1 * S;
         if (score > best_score) {
             best_score = score;
             best.TY = TY;
+            best.RS = RS;
             best.S = S;
-            best.threads = threads;
             best.ncw = ncw;
-            best.smem = (size_t)S * stage + (size_t)S * 24 + (size_t)nzlma * 8;
+            best.threads = threads;
+            best.smem = (size_t)S * stage + (size_t)S * 16;
         }
     }
     return best;
 }
 
 template <typename T, int MD, int BY>
-static int launch_ring(StencilArgs<T> a, const StencilCoef& cf, int nb, cudaStream_t st, bool* used) {
+static int launch_tma(StencilArgs<T> a, const StencilCoef& cf, int nb, cudaStream_t st, bool* used) {
     Context& c = ctx();
     *used = false;
+    const TmaGeom g = tma_geometry<T, MD, BY>(a.n1, a.n2);
+    if (g.TY == 0) return RSDFT_OK;
+    if (reinterpret_cast<uintptr_t>(a.hpsi) % 16 != 0 || (a.ld * sizeof(T)) % 16 != 0) return RSDFT_OK;
     const int sms = c.num_sms > 0 ? c.num_sms : 148;
-    RingGeom g0 = ring_geometry<T, MD, BY>(a.n1, a.n2, a.n3, a.nzlma);
-    if (g0.TY == 0) return RSDFT_OK;
-    const long base = (long)(a.n2 / g0.TY) * nb;
-    int nzc = (int)std::min<long>(std::max<long>(1, (2L * sms + base - 1) / base), std::max(1, a.n3 / 8));
+    const long base = (long)(a.n2 / g.TY) * nb;
+    int nzc = (int)std::min<long>(std::max<long>(1, (sms + base - 1) / base), std::max(1, a.n3 / (4 * MD)));
     while ((long)nb * nzc > 65535 && nzc > 1) --nzc;
     a.zlen = div_up(a.n3, nzc);
     a.nzc = div_up(a.n3, a.zlen);
-    RingGeom g = ring_geometry<T, MD, BY>(a.n1, a.n2, a.zlen, a.nzlma);
-    if (g.TY == 0) return RSDFT_OK;
-    constexpr int PAD = ring_pad<T, MD>();
-    constexpr int RQ = 128 / (int)sizeof(T);
-    WsMaps maps;
+    TmaMaps maps;
     const CUtensorMapDataType dt = sizeof(T) == 8 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT64 : CU_TENSOR_MAP_DATA_TYPE_FLOAT32;
     const unsigned long long dims[4] = {(unsigned long long)a.n1, (unsigned long long)a.n2,
                                         (unsigned long long)a.n3, (unsigned long long)nb};
     const unsigned long long strides[3] = {(unsigned long long)a.n1 * sizeof(T),
                                            (unsigned long long)a.n1 * a.n2 * sizeof(T),
                                            (unsigned long long)a.ld * sizeof(T)};
-    const unsigned int RS = (a.n1 + 2 * PAD + RQ - 1) / RQ * RQ, ROWS = g.TY + 2 * MD;
-    const unsigned int bf[4] = {RS, ROWS, 1, 1}, be[4] = {RS, ROWS - MD, 1, 1}, bm[4] = {RS, (unsigned)g.TY, 1, 1},
+    const unsigned long long vdims[4] = {(unsigned long long)a.n1, (unsigned long long)a.n2,
+                                         (unsigned long long)a.n3, 1ull};
+    const unsigned long long vstrides[3] = {strides[0], strides[1], (unsigned long long)a.n1 * a.n2 * a.n3 * sizeof(T)};
+    const unsigned int RS = (unsigned)g.RS, TY = (unsigned)g.TY;
+    const unsigned int bf[4] = {RS, TY + 2 * MD, 1, 1}, be[4] = {RS, TY + MD, 1, 1}, bm[4] = {RS, TY, 1, 1},
                        bw[4] = {RS, (unsigned)MD, 1, 1};
     if (encode_tmap_4d(&maps.full, dt, a.psi, dims, strides, bf) != RSDFT_OK ||
         encode_tmap_4d(&maps.edge, dt, a.psi, dims, strides, be) != RSDFT_OK ||
         encode_tmap_4d(&maps.mid, dt, a.psi, dims, strides, bm) != RSDFT_OK ||
-        encode_tmap_4d(&maps.wrap, dt, a.psi, dims, strides, bw) != RSDFT_OK)
+        encode_tmap_4d(&maps.wrap, dt, a.psi, dims, strides, bw) != RSDFT_OK ||
+        encode_tmap_4d(&maps.vloc, dt, a.vloc, vdims, vstrides, bm) != RSDFT_OK)
         return RSDFT_OK;  // not usable for this shape: the caller takes the general kernel
     static bool attr_set = false;
     if (!attr_set) {
-        RS_CUDA(cudaFuncSetAttribute(k_stencil_ws<T, MD, BY, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                     220 * 1024 + 16 * 24));
+        RS_CUDA(cudaFuncSetAttribute(k_stencil_tma<T, MD, BY>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     220 * 1024 + 8 * 16));
         attr_set = true;
     }
     dim3 grid(a.n2 / g.TY, (unsigned)(nb * a.nzc));
-    launch(k_stencil_ws<T, MD, BY, 1>, grid, g.threads, g.smem, st, maps, a, cf, g.TY, g.S, g.ncw, c.err_flag);
+    launch(k_stencil_tma<T, MD, BY>, grid, g.threads, g.smem, st, maps, a, cf, g.TY, g.RS, g.S, g.ncw, c.err_flag);
     RS_LAUNCH();
     *used = true;
     return RSDFT_OK;
@@ -542,17 +631,23 @@ static int launch_ring(StencilArgs<T> a, const StencilCoef& cf, int nb, cudaStre
 
 template <typename T, int MD>
 static int launch_stencil_md2(StencilArgs<T> a, const StencilCoef& cf, int nb, cudaStream_t st) {
-    bool used = false;
-    if ((long)nb * 2 <= 65535) {
-        if constexpr (sizeof(T) == 8)
-            RS_CHECK((launch_ring<T, MD, 2>(a, cf, nb, st, &used)));
-        else
-            RS_CHECK((launch_ring<T, MD, 4>(a, cf, nb, st, &used)));
-    }
-    if (used) return RSDFT_OK;
-    // general shapes (odd widths, very wide rows): register-queue kernel with
-    // per-plane halo loads
     const Context& c = ctx();
+    bool used = false;
+    // two rows per thread up to Md = 6; one above, where the 2 Md + 1
+    // accumulators of two rows no longer fit the register budget
+    RS_CHECK((launch_tma<T, MD, (MD <= 6 ? 2 : 1)>(a, cf, nb, st, &used)));
+    if (used) {
+        if (a.gpt_ptr && c.nl_npt > 0) {
+            constexpr int BCH = 32;
+            dim3 grid(div_up(c.nl_npt, 128), div_up(nb, BCH));
+            launch(k_nl_scatter<T>, grid, 128, 0, st, a.hpsi, a.ld, nb, BCH, (const int*)c.nl_pts,
+                   (const int*)c.nl_ptr, c.nl_npt, a.gpt_grp, a.gpt_uv4, a.uvunk, a.nzlma, a.band_active);
+            RS_LAUNCH();
+        }
+        return RSDFT_OK;
+    }
+    // general shapes (odd widths, very wide rows): register-queue kernel with
+    // per-plane halo loads and the nonlocal scatter fused
     const int tx = (a.n1 % 32 == 0 || a.n1 > 24) ? 32 : (a.n1 % 24 == 0 ? 24 : 16);
     const long base = (long)div_up(a.n1, tx) * div_up(a.n2, 16) * nb;
     const long want = 8L * (c.num_sms > 0 ? c.num_sms : 148);
@@ -596,10 +691,7 @@ int hpsi_device(const T* psi, T* hpsi, long ld, int nb, int spin, const int* ban
     double* uvunk = nullptr;
     if (nl) {
         RS_CHECK(workspace_t("hpsi_uvunk", (size_t)nb * c.nzlma, &uvunk));
-        dim3 grid(c.ngroup, div_up(nb, 8));
-        launch(k_nl_project<T>, grid, 256, 0, c.stream, psi, ld, nb, c.grp_lma0, c.grp_cnt, c.lma_ptr, c.jjp, c.uv,
-                                                    c.iuv, c.dV, uvunk, c.nzlma, band_active);
-        RS_LAUNCH();
+        RS_CHECK(launch_project<T>(psi, ld, nb, uvunk, band_active, c.stream));
     }
     StencilArgs<T> a{};
     a.psi = psi;
@@ -714,9 +806,7 @@ int hpsi_static_scratch(const double* psi, double* hpsi, long ld, int nb, int sp
     double* uvunk = nullptr;
     if (nl) {
         RS_CHECK(noalloc_scratch(&uvunk));
-        launch(k_nl_project<double>, dim3(c.ngroup, div_up(nb, 8)), 256, 0, c.stream, psi, ld, nb, c.grp_lma0,
-               c.grp_cnt, c.lma_ptr, c.jjp, c.uv, c.iuv, c.dV, uvunk, c.nzlma, (const int*)nullptr);
-        RS_LAUNCH();
+        RS_CHECK(launch_project<double>(psi, ld, nb, uvunk, nullptr, c.stream));
     }
     StencilArgs<double> a{};
     a.psi = psi;

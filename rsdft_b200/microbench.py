@@ -1,0 +1,112 @@
+"""Small timing drivers for single pieces of the eigensolver, for profiling.
+
+``python -m rsdft_b200.microbench hpsi --workload si216 --bands 64``
+    H psi through ``rsdft_gpu_hamiltonian`` on device arrays (warm-up calls,
+    then ``--reps`` timed calls); prints ms per call and the algorithmic
+    bytes rate.  ``--no-nonlocal`` uploads an empty projector table first, so
+    the stencil and Vloc part is timed alone.
+``python -m rsdft_b200.microbench iteration --workload si216 --mode fp64``
+    eigensolver iterations (CG -> Gram-Schmidt -> subspace) from the seeded
+    start, ``--warmup`` untimed and ``--steps`` timed.
+
+Both run on cuda:0 with the library on a dedicated torch stream; timings are
+CUDA events on that stream.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import sys
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+if ROOT not in sys.path:
+    sys.path.insert(0, ROOT)
+
+MODES = {"fp64": 0, "mixed-bf16": 1, "mixed-bf16x3": 2}
+
+
+def _setup(workload: str):
+    import torch
+
+    from rsdft_b200 import api
+    from rsdft_b200.cell import build_cell
+
+    st = torch.cuda.Stream()
+    torch.cuda.set_stream(st)
+    g = api.RsdftGpu(0)
+    g.set_stream(st.cuda_stream)
+    cell = build_cell(workload)
+    g.setup(cell)
+    psi = torch.from_numpy(np.ascontiguousarray(cell.psi0().T)).cuda().t()
+    return torch, api, g, cell, st, psi
+
+
+def _timed(torch, st, fn, warmup: int, reps: int) -> float:
+    for _ in range(warmup):
+        fn()
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(st)
+    for _ in range(reps):
+        fn()
+    e1.record(st)
+    torch.cuda.synchronize()
+    return e0.elapsed_time(e1) / reps
+
+
+def run_hpsi(args) -> dict:
+    torch, api, g, cell, st, psi = _setup(args.workload)
+    from rsdft_b200 import _lib
+
+    if args.no_nonlocal:
+        lp = np.zeros(1, np.int32)
+        _lib.call("rsdft_gpu_set_nonlocal", 0, lp.ctypes.data, None, None, None, None, cell.natom, None)
+    nb = min(args.bands, cell.nband)
+    p = psi[:, :nb]
+    h = api.fortran_empty(cell.ML, nb)
+    ms = _timed(torch, st, lambda: g.hamiltonian(1, 1, p, h, 1, cell.ML, 1, nb), args.warmup, args.reps)
+    nnz = 0 if args.no_nonlocal else int(cell.lma_ptr[-1])
+    nbytes = nb * cell.ML * 16 + cell.ML * 8 + nnz * 12
+    return {"what": "hpsi", "workload": args.workload, "bands": nb, "nonlocal": not args.no_nonlocal,
+            "ms": ms, "bytes": nbytes, "gbs": nbytes / (ms * 1e-3) / 1e9}
+
+
+def run_iteration(args) -> dict:
+    torch, api, g, cell, st, psi = _setup(args.workload)
+    MB = cell.nband
+    u = psi.t().contiguous().t()
+    g.gram_schmidt(1, MB, 1, 1, u)
+    esp = torch.zeros(MB, dtype=torch.float64, device="cuda")
+    res = torch.zeros_like(esp)
+    mode = MODES[args.mode]
+    ms = _timed(torch, st, lambda: g.eigensolver_iteration(u, esp, res, ncg=args.ncg, mloop=args.mloop, mode=mode),
+                args.warmup, args.steps)
+    return {"what": "iteration", "workload": args.workload, "mode": args.mode, "ms_per_iter": ms}
+
+
+def main(argv=None) -> None:
+    p = argparse.ArgumentParser(description=__doc__, formatter_class=argparse.RawDescriptionHelpFormatter)
+    sub = p.add_subparsers(dest="what", required=True)
+    h = sub.add_parser("hpsi")
+    h.add_argument("--workload", default="si216")
+    h.add_argument("--bands", type=int, default=64)
+    h.add_argument("--warmup", type=int, default=3)
+    h.add_argument("--reps", type=int, default=10)
+    h.add_argument("--no-nonlocal", action="store_true")
+    it = sub.add_parser("iteration")
+    it.add_argument("--workload", default="si216")
+    it.add_argument("--mode", default="fp64", choices=sorted(MODES))
+    it.add_argument("--ncg", type=int, default=4)
+    it.add_argument("--mloop", type=int, default=3)
+    it.add_argument("--warmup", type=int, default=3)
+    it.add_argument("--steps", type=int, default=2)
+    args = p.parse_args(argv)
+    out = run_hpsi(args) if args.what == "hpsi" else run_iteration(args)
+    print(json.dumps(out), flush=True)
+
+
+if __name__ == "__main__":
+    main()
