@@ -18,6 +18,7 @@
 #include "kernels.cuh"
 #include "tma.cuh"
 #include "tmap.cuh"
+#include "vec16.cuh"
 
 namespace rsdft {
 
@@ -213,29 +214,6 @@ __global__ void __launch_bounds__(TX * 16) k_stencil(StencilArgs<T> a, StencilCo
         for (int k = 0; k < 2 * MD; ++k) q[k] = q[k + 1];
     }
 }
-
-template <typename T>
-struct Vec16;
-template <>
-struct Vec16<double> {
-    using t = double2;
-    __device__ static __forceinline__ void get(const t& v, double* o) {
-        o[0] = v.x;
-        o[1] = v.y;
-    }
-    __device__ static __forceinline__ t make(const double* o) { return make_double2(o[0], o[1]); }
-};
-template <>
-struct Vec16<float> {
-    using t = float4;
-    __device__ static __forceinline__ void get(const t& v, float* o) {
-        o[0] = v.x;
-        o[1] = v.y;
-        o[2] = v.z;
-        o[3] = v.w;
-    }
-    __device__ static __forceinline__ t make(const float* o) { return make_float4(o[0], o[1], o[2], o[3]); }
-};
 
 struct TmaMaps {
     CUtensorMap full, edge, mid, wrap;  // psi boxes of height TY + 2 Md, TY + Md, TY, Md
