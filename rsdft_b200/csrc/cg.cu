@@ -41,7 +41,7 @@ template <typename T, int NV, int K>
 __global__ void __launch_bounds__(VT) k_multidot(const T* v0, const T* v1, const T* v2, const T* v3, long ld,
                                                  long n, DotPairs<K> pr, double* __restrict__ part,
                                                  const int* __restrict__ active) {
-    __shared__ double sh[VT / 32];
+    __shared__ double sh[K * (VT / 32)];
     const int b = blockIdx.y;
     if (active && !active[b]) return;
     const T* vs[4] = {v0, v1, v2, v3};
@@ -49,7 +49,7 @@ __global__ void __launch_bounds__(VT) k_multidot(const T* v0, const T* v1, const
 #pragma unroll
     for (int k = 0; k < K; ++k) acc[k] = 0.0;
     const long base = (long)blockIdx.x * VCHUNK;
-#pragma unroll
+#pragma unroll 8
     for (int it = 0; it < VITEMS; ++it) {
         const long i = base + it * VT + threadIdx.x;
         if (i < n) {
@@ -60,10 +60,10 @@ __global__ void __launch_bounds__(VT) k_multidot(const T* v0, const T* v1, const
             for (int k = 0; k < K; ++k) acc[k] = fma(v[pr.a[k]], v[pr.b[k]], acc[k]);
         }
     }
+    block_sum_n<VT, K>(acc, sh);
+    if (threadIdx.x == 0) {
 #pragma unroll
-    for (int k = 0; k < K; ++k) {
-        double s = block_sum<VT>(acc[k], sh);
-        if (threadIdx.x == 0) part[((long)b * gridDim.x + blockIdx.x) * K + k] = s;
+        for (int k = 0; k < K; ++k) part[((long)b * gridDim.x + blockIdx.x) * K + k] = acc[k];
     }
 }
 
@@ -77,7 +77,7 @@ __global__ void __launch_bounds__(VT) k_cg_g(CGVec<T> v, long ld, long n, const 
     const double e = E[b];
     double acc = 0.0;
     const long base = (long)blockIdx.x * VCHUNK, off = (long)b * ld;
-#pragma unroll
+#pragma unroll 8
     for (int it = 0; it < VITEMS; ++it) {
         const long i = base + it * VT + threadIdx.x;
         if (i < n) {
@@ -102,7 +102,7 @@ __global__ void __launch_bounds__(VT) k_pc0(CGVec<T> v, long ld, long n, PcArgs 
     double acc = 0.0;
     int i1, i2, i3;
     pc_coords(base + threadIdx.x, pa, i1, i2, i3);
-#pragma unroll
+#pragma unroll 8
     for (int it = 0; it < VITEMS; ++it) {
         const long i = base + it * VT + threadIdx.x;
         if (i < n) {
@@ -132,7 +132,7 @@ __global__ void __launch_bounds__(VT) k_pc1(CGVec<T> v, long ld, long n, PcArgs 
     double acc = 0.0;
     int i1, i2, i3;
     pc_coords(base + threadIdx.x, pa, i1, i2, i3);
-#pragma unroll
+#pragma unroll 8
     for (int it = 0; it < VITEMS; ++it) {
         const long i = base + it * VT + threadIdx.x;
         if (i < n) {
@@ -156,7 +156,7 @@ __global__ void __launch_bounds__(VT) k_pc2(CGVec<T> v, long ld, long n, const d
     const long off = (long)b * ld, base = (long)blockIdx.x * VCHUNK;
     const T a = (T)pa_[b];
     double acc = 0.0;
-#pragma unroll
+#pragma unroll 8
     for (int it = 0; it < VITEMS; ++it) {
         const long i = base + it * VT + threadIdx.x;
         if (i < n) {
@@ -183,7 +183,7 @@ __global__ void __launch_bounds__(VT) k_pc3(CGVec<T> v, long ld, long n, const d
     if (active && !active[b]) return;
     const long off = (long)b * ld, base = (long)blockIdx.x * VCHUNK;
     const T bb = (T)pb_[b];
-#pragma unroll
+#pragma unroll 8
     for (int it = 0; it < VITEMS; ++it) {
         const long i = base + it * VT + threadIdx.x;
         if (i < n) v.q[off + i] = v.r[off + i] + bb * v.q[off + i];
@@ -198,7 +198,7 @@ __global__ void __launch_bounds__(VT) k_cg_p(CGVec<T> v, long ld, long n, const 
     if (active && !active[b]) return;
     const long off = (long)b * ld, base = (long)blockIdx.x * VCHUNK;
     const T bk = (T)bk_[b];
-#pragma unroll
+#pragma unroll 8
     for (int it = 0; it < VITEMS; ++it) {
         const long i = base + it * VT + threadIdx.x;
         if (i < n) v.p[off + i] = first ? v.Pg[off + i] : v.Pg[off + i] + bk * v.p[off + i];
@@ -215,7 +215,7 @@ __global__ void __launch_bounds__(VT) k_cg_upd1(CGVec<T> v, long ld, long n, CGS
     const long off = (long)b * ld, base = (long)blockIdx.x * VCHUNK;
     const T u11 = (T)s.u11[b], u21 = (T)s.u21[b], w = (T)s.W[b];
     double acc = 0.0;
-#pragma unroll
+#pragma unroll 8
     for (int it = 0; it < VITEMS; ++it) {
         const long i = base + it * VT + threadIdx.x;
         if (i < n) {
@@ -239,7 +239,7 @@ __global__ void __launch_bounds__(VT) k_cg_upd2(CGVec<T> v, long ld, long n, CGS
     if (s.reject[b]) return;
     const long off = (long)b * ld, base = (long)blockIdx.x * VCHUNK;
     const T u11 = (T)s.u11[b], u21 = (T)s.u21[b];
-#pragma unroll
+#pragma unroll 8
     for (int it = 0; it < VITEMS; ++it) {
         const long i = base + it * VT + threadIdx.x;
         if (i < n) v.x[off + i] = u11 * v.x[off + i] + u21 * v.p[off + i];
@@ -382,7 +382,7 @@ __global__ void __launch_bounds__(VT) k_resid(const double* __restrict__ x, cons
     const long off = (long)b * ld, base = (long)blockIdx.x * VCHUNK;
     const double eb = e[b];
     double acc = 0.0;
-#pragma unroll
+#pragma unroll 8
     for (int it = 0; it < VITEMS; ++it) {
         const long i = base + it * VT + threadIdx.x;
         if (i < n) {

@@ -8,7 +8,7 @@
 namespace rsdft {
 
 constexpr int VT = 256;           // threads per vector CTA
-constexpr int VITEMS = 8;         // elements per thread
+constexpr int VITEMS = 32;        // elements per thread
 constexpr int VCHUNK = VT * VITEMS;
 
 struct CGScal {

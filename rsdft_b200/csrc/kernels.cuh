@@ -28,6 +28,30 @@ __device__ __forceinline__ double block_sum(double v, double* sh /* >= NT/32 dou
     return r;
 }
 
+// K deterministic block sums with one pair of barriers; results valid in
+// thread 0.  sh holds K * NT / 32 doubles.
+template <int NT, int K>
+__device__ __forceinline__ void block_sum_n(double (&v)[K], double* sh) {
+    const int w = threadIdx.x >> 5, l = threadIdx.x & 31;
+#pragma unroll
+    for (int k = 0; k < K; ++k) {
+#pragma unroll
+        for (int s = 16; s > 0; s >>= 1) v[k] += __shfl_xor_sync(0xffffffffu, v[k], s);
+        if (l == 0) sh[k * (NT / 32) + w] = v[k];
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+#pragma unroll
+        for (int k = 0; k < K; ++k) {
+            double r = 0.0;
+#pragma unroll
+            for (int i = 0; i < NT / 32; ++i) r += sh[k * (NT / 32) + i];
+            v[k] = r;
+        }
+    }
+    __syncthreads();
+}
+
 // Symmetric-positive-definite orthonormalisation (CholeskyQR2 in the dV
 // metric) of nb columns, FP64 (cuBLAS/cuSOLVER) or mixed (tensor cores).
 int gram_schmidt_device(double* psi, long ld, int nb, int mode);

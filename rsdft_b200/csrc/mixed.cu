@@ -48,16 +48,37 @@ __device__ __forceinline__ void split_bf16(double x, __nv_bfloat16& h, __nv_bflo
     l = __float2bfloat16_rn((float)r);
 }
 
-// slices[s][b][k] = term s of psi(k, b): same layout as psi (K-major per band)
-__global__ void k_split_cols(const double* __restrict__ psi, long ld, int nb, long ml, __nv_bfloat16* __restrict__ out) {
+// slices[s][b][k] = term s of psi(k, b): same layout as psi (K-major per
+// band).  grid (ceil(ml / 2048), nb): 8 consecutive k per thread, read as
+// 16-byte pairs and written as one 16-byte group per slice when vec is set
+// (ml % 8 == 0, ld even, 16-byte aligned bases).
+__global__ void __launch_bounds__(256) k_split_cols(const double* __restrict__ psi, long ld, int nb, long ml,
+                                                    __nv_bfloat16* __restrict__ out, int vec) {
     const long n = ml * nb;
-    for (long e = (long)blockIdx.x * blockDim.x + threadIdx.x; e < n; e += (long)gridDim.x * blockDim.x) {
-        const long b = e / ml, k = e - b * ml;
+    const int b = blockIdx.y;
+    const long k0 = ((long)blockIdx.x * blockDim.x + threadIdx.x) * 8;
+    if (k0 >= ml) return;
+    const double* src = psi + (long)b * ld + k0;
+    __nv_bfloat16* o = out + (long)b * ml + k0;
+    if (vec && k0 + 8 <= ml) {
+        __nv_bfloat16 h[8], m[8], l[8];
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+            const double2 v = *reinterpret_cast<const double2*>(src + 2 * q);
+            split_bf16(v.x, h[2 * q], m[2 * q], l[2 * q]);
+            split_bf16(v.y, h[2 * q + 1], m[2 * q + 1], l[2 * q + 1]);
+        }
+        *reinterpret_cast<uint4*>(o) = *reinterpret_cast<const uint4*>(h);
+        *reinterpret_cast<uint4*>(o + n) = *reinterpret_cast<const uint4*>(m);
+        *reinterpret_cast<uint4*>(o + 2 * n) = *reinterpret_cast<const uint4*>(l);
+        return;
+    }
+    for (long k = 0; k < 8 && k0 + k < ml; ++k) {
         __nv_bfloat16 h, m, l;
-        split_bf16(psi[b * ld + k], h, m, l);
-        out[e] = h;
-        out[n + e] = m;
-        out[2 * n + e] = l;
+        split_bf16(src[k], h, m, l);
+        o[k] = h;
+        o[n + k] = m;
+        o[2 * n + k] = l;
     }
 }
 
@@ -368,11 +389,16 @@ int gram_mixed(const double* A, const double* B, long ld, int nb, double alpha, 
     const size_t nsl = (size_t)ml * nb;
     __nv_bfloat16 *sa = nullptr, *sb = nullptr;
     RS_CHECK(workspace_t("umma_sa", 3 * nsl, &sa));
-    launch(k_split_cols, 4 * c.num_sms, 256, 0, c.stream, A, ld, nb, ml, sa);
+    const int vec = (ml % 8 == 0 && ld % 2 == 0 && reinterpret_cast<uintptr_t>(A) % 16 == 0 &&
+                     reinterpret_cast<uintptr_t>(B) % 16 == 0)
+                        ? 1
+                        : 0;
+    const dim3 sg(div_up(ml, 2048), nb);
+    launch(k_split_cols, sg, 256, 0, c.stream, A, ld, nb, ml, sa, vec);
     const bool same = (A == B);
     if (!same) {
         RS_CHECK(workspace_t("umma_sb", 3 * nsl, &sb));
-        launch(k_split_cols, 4 * c.num_sms, 256, 0, c.stream, B, ld, nb, ml, sb);
+        launch(k_split_cols, sg, 256, 0, c.stream, B, ld, nb, ml, sb, vec);
     } else {
         sb = sa;
     }

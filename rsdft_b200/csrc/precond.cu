@@ -19,7 +19,7 @@ template <typename T, int K, bool STORE>
 __global__ void __launch_bounds__(VT) k_ss_basis(const T* __restrict__ g, SSVec<T> sv, long ld, long n, PcArgs pa,
                                                  double* __restrict__ part, const int* __restrict__ active) {
     constexpr int D = K == 0 ? 1 : (STORE ? K + 1 : 2 * K);
-    __shared__ double sh[VT / 32];
+    __shared__ double sh[D * (VT / 32)];
     const int b = blockIdx.y;
     if (active && !active[b]) return;
     const long off = (long)b * ld, base = (long)blockIdx.x * VCHUNK;
@@ -30,7 +30,7 @@ __global__ void __launch_bounds__(VT) k_ss_basis(const T* __restrict__ g, SSVec<
     for (int k = 0; k < D; ++k) acc[k] = 0.0;
     int i1, i2, i3;
     pc_coords(base + threadIdx.x, pa, i1, i2, i3);
-#pragma unroll
+#pragma unroll 8
     for (int it = 0; it < VITEMS; ++it) {
         const long i = base + it * VT + threadIdx.x;
         if (i < n) {
@@ -62,10 +62,10 @@ __global__ void __launch_bounds__(VT) k_ss_basis(const T* __restrict__ g, SSVec<
         }
         pc_step(pa, i1, i2, i3);
     }
+    block_sum_n<VT, D>(acc, sh);
+    if (threadIdx.x == 0) {
 #pragma unroll
-    for (int k = 0; k < D; ++k) {
-        const double r = block_sum<VT>(acc[k], sh);
-        if (threadIdx.x == 0) part[((long)b * gridDim.x + blockIdx.x) * D + k] = r;
+        for (int k = 0; k < D; ++k) part[((long)b * gridDim.x + blockIdx.x) * D + k] = acc[k];
     }
 }
 
@@ -150,7 +150,7 @@ __global__ void __launch_bounds__(VT) k_ss_p(const T* __restrict__ g, SSVec<T> s
 #pragma unroll
     for (int j = 0; j < SS_MAXM; ++j) c[j] = (T)cz[(long)b * SS_MAXM + j];
     const T bk = (T)bk_[b];
-#pragma unroll
+#pragma unroll 8
     for (int it = 0; it < VITEMS; ++it) {
         const long i = base + it * VT + threadIdx.x;
         if (i < n) {
