@@ -40,22 +40,36 @@ struct DotPairs {
 template <typename T, int NV, int K>
 __global__ void __launch_bounds__(VT) k_multidot(const T* v0, const T* v1, const T* v2, const T* v3, long ld,
                                                  long n, DotPairs<K> pr, double* __restrict__ part,
-                                                 const int* __restrict__ active) {
+                                                 const int* __restrict__ active, int vec) {
+    using G = Grp16<T>;
+    constexpr int W = G::W;
     __shared__ double sh[K * (VT / 32)];
     const int b = blockIdx.y;
     if (active && !active[b]) return;
     const T* vs[4] = {v0, v1, v2, v3};
+    const long off = (long)b * ld;
     double acc[K];
 #pragma unroll
     for (int k = 0; k < K; ++k) acc[k] = 0.0;
     const long base = (long)blockIdx.x * VCHUNK;
-#pragma unroll 8
-    for (int it = 0; it < VITEMS; ++it) {
-        const long i = base + it * VT + threadIdx.x;
-        if (i < n) {
+#pragma unroll 4
+    for (int j = 0; j < VITEMS / W; ++j) {
+        const long i = base + ((long)j * VT + threadIdx.x) * W;
+        T vv[NV][W];
+        if (vec && i + W <= n) {
+#pragma unroll
+            for (int q = 0; q < NV; ++q) G::load(vs[q] + off + i, vv[q]);
+        } else {
+#pragma unroll
+            for (int q = 0; q < NV; ++q)
+#pragma unroll
+                for (int e = 0; e < W; ++e) vv[q][e] = i + e < n ? vs[q][off + i + e] : (T)0;
+        }
+#pragma unroll
+        for (int e = 0; e < W; ++e) {
             double v[NV];
 #pragma unroll
-            for (int q = 0; q < NV; ++q) v[q] = (double)vs[q][(long)b * ld + i];
+            for (int q = 0; q < NV; ++q) v[q] = (double)vv[q][e];
 #pragma unroll
             for (int k = 0; k < K; ++k) acc[k] = fma(v[pr.a[k]], v[pr.b[k]], acc[k]);
         }
@@ -70,24 +84,38 @@ __global__ void __launch_bounds__(VT) k_multidot(const T* v0, const T* v1, const
 // g = -c1 (hx - E x); partial |g|^2 (cg_module.f90:186-190)
 template <typename T>
 __global__ void __launch_bounds__(VT) k_cg_g(CGVec<T> v, long ld, long n, const double* __restrict__ E,
-                                             double* __restrict__ part, const int* __restrict__ active) {
+                                             double* __restrict__ part, const int* __restrict__ active, int vec) {
+    using G = Grp16<T>;
+    constexpr int W = G::W;
     __shared__ double sh[VT / 32];
     const int b = blockIdx.y;
     if (active && !active[b]) return;
-    const double e = E[b];
+    const T e = (T)E[b];
     double acc = 0.0;
     const long base = (long)blockIdx.x * VCHUNK, off = (long)b * ld;
-#pragma unroll 8
-    for (int it = 0; it < VITEMS; ++it) {
-        const long i = base + it * VT + threadIdx.x;
-        if (i < n) {
-            const T g = (T)(-2.0) * (v.hx[off + i] - (T)e * v.x[off + i]);
-            v.g[off + i] = g;
-            acc = fma((double)g, (double)g, acc);
+#pragma unroll 4
+    for (int j = 0; j < VITEMS / W; ++j) {
+        const long i = base + ((long)j * VT + threadIdx.x) * W;
+        if (vec && i + W <= n) {
+            T hx[W], x[W], g[W];
+            G::load(v.hx + off + i, hx);
+            G::load(v.x + off + i, x);
+#pragma unroll
+            for (int q = 0; q < W; ++q) {
+                g[q] = (T)(-2.0) * (hx[q] - e * x[q]);
+                acc = fma((double)g[q], (double)g[q], acc);
+            }
+            G::store(v.g + off + i, g);
+        } else {
+            for (int q = 0; q < W && i + q < n; ++q) {
+                const T g = (T)(-2.0) * (v.hx[off + i + q] - e * v.x[off + i + q]);
+                v.g[off + i + q] = g;
+                acc = fma((double)g, (double)g, acc);
+            }
         }
     }
-    double s = block_sum<VT>(acc, sh);
-    if (threadIdx.x == 0) part[(long)b * gridDim.x + blockIdx.x] = s;
+    double r = block_sum<VT>(acc, sh);
+    if (threadIdx.x == 0) part[(long)b * gridDim.x + blockIdx.x] = r;
 }
 
 // P0: Pg = g; r = g - A g; q = r; partial |r|^2  (cgpc_hprsdft_module.f90:161-175)
@@ -207,23 +235,47 @@ __global__ void __launch_bounds__(VT) k_cg_p(CGVec<T> v, long ld, long n, const 
 
 // hx = u11 hx + u21 hp; g = -c1 (hx - W (u11 x + u21 p)); partial |g|^2 (:337-347)
 template <typename T>
+__device__ __forceinline__ T cg_upd1_elem(T& hx, T hp, T x, T p, T u11, T u21, T w) {
+    hx = u11 * hx + u21 * hp;
+    return (T)(-2.0) * (hx - w * (u11 * x + u21 * p));
+}
+
+template <typename T>
 __global__ void __launch_bounds__(VT) k_cg_upd1(CGVec<T> v, long ld, long n, CGScal s, double* __restrict__ part,
-                                                const int* __restrict__ active) {
+                                                const int* __restrict__ active, int vec) {
+    using G = Grp16<T>;
+    constexpr int W = G::W;
     __shared__ double sh[VT / 32];
     const int b = blockIdx.y;
     if (active && !active[b]) return;
     const long off = (long)b * ld, base = (long)blockIdx.x * VCHUNK;
     const T u11 = (T)s.u11[b], u21 = (T)s.u21[b], w = (T)s.W[b];
     double acc = 0.0;
-#pragma unroll 8
-    for (int it = 0; it < VITEMS; ++it) {
-        const long i = base + it * VT + threadIdx.x;
-        if (i < n) {
-            const T hx = u11 * v.hx[off + i] + u21 * v.hp[off + i];
-            v.hx[off + i] = hx;
-            const T g = (T)(-2.0) * (hx - w * (u11 * v.x[off + i] + u21 * v.p[off + i]));
-            v.g[off + i] = g;
-            acc = fma((double)g, (double)g, acc);
+#pragma unroll 4
+    for (int j = 0; j < VITEMS / W; ++j) {
+        const long i = base + ((long)j * VT + threadIdx.x) * W;
+        if (vec && i + W <= n) {
+            T hx[W], hp[W], x[W], p[W], g[W];
+            G::load(v.hx + off + i, hx);
+            G::load(v.hp + off + i, hp);
+            G::load(v.x + off + i, x);
+            G::load(v.p + off + i, p);
+#pragma unroll
+            for (int q = 0; q < W; ++q) {
+                g[q] = cg_upd1_elem(hx[q], hp[q], x[q], p[q], u11, u21, w);
+                acc = fma((double)g[q], (double)g[q], acc);
+            }
+            G::store(v.hx + off + i, hx);
+            G::store(v.g + off + i, g);
+        } else {
+            for (int q = 0; q < W && i + q < n; ++q) {
+                const long k = off + i + q;
+                T hx = v.hx[k];
+                const T g = cg_upd1_elem(hx, v.hp[k], v.x[k], v.p[k], u11, u21, w);
+                v.hx[k] = hx;
+                v.g[k] = g;
+                acc = fma((double)g, (double)g, acc);
+            }
         }
     }
     double r = block_sum<VT>(acc, sh);
@@ -233,16 +285,27 @@ __global__ void __launch_bounds__(VT) k_cg_upd1(CGVec<T> v, long ld, long n, CGS
 // x = u11 x + u21 p unless rejected (:366-369)
 template <typename T>
 __global__ void __launch_bounds__(VT) k_cg_upd2(CGVec<T> v, long ld, long n, CGScal s,
-                                                const int* __restrict__ active) {
+                                                const int* __restrict__ active, int vec) {
+    using G = Grp16<T>;
+    constexpr int W = G::W;
     const int b = blockIdx.y;
     if (active && !active[b]) return;
     if (s.reject[b]) return;
     const long off = (long)b * ld, base = (long)blockIdx.x * VCHUNK;
     const T u11 = (T)s.u11[b], u21 = (T)s.u21[b];
-#pragma unroll 8
-    for (int it = 0; it < VITEMS; ++it) {
-        const long i = base + it * VT + threadIdx.x;
-        if (i < n) v.x[off + i] = u11 * v.x[off + i] + u21 * v.p[off + i];
+#pragma unroll 4
+    for (int j = 0; j < VITEMS / W; ++j) {
+        const long i = base + ((long)j * VT + threadIdx.x) * W;
+        if (vec && i + W <= n) {
+            T x[W], p[W];
+            G::load(v.x + off + i, x);
+            G::load(v.p + off + i, p);
+#pragma unroll
+            for (int q = 0; q < W; ++q) x[q] = u11 * x[q] + u21 * p[q];
+            G::store(v.x + off + i, x);
+        } else {
+            for (int q = 0; q < W && i + q < n; ++q) v.x[off + i + q] = u11 * v.x[off + i + q] + u21 * v.p[off + i + q];
+        }
     }
 }
 
@@ -407,7 +470,8 @@ int esp_device(const double* x, long ld, int nb, int spin, double* e, double* re
     RS_CHECK(hpsi_device<double>(x, hx, ld, nb, spin, nullptr));
     const dim3 vg(nchunk, nb);
     DotPairs<1> pr{{0}, {1}};
-    launch(k_multidot<double, 2, 1>, vg, VT, 0, st, x, hx, nullptr, nullptr, ld, n, pr, part, nullptr);
+    const int gv = grp16_ok<double>(ld, {x, hx}) ? 1 : 0;
+    launch(k_multidot<double, 2, 1>, vg, VT, 0, st, x, hx, nullptr, nullptr, ld, n, pr, part, nullptr, gv);
     launch(k_finish, div_up(nb, 128), 128, 0, st, part, nchunk, 1, nb, c.dV, e, nullptr);
     if (res) {
         launch(k_resid, vg, VT, 0, st, x, hx, ld, n, e, part);
@@ -454,6 +518,7 @@ static int cg_run(T* x, long ld, int mb, int spin, double* esp, double* res, int
     const dim3 vg(nchunk, mb);
     const int sb = div_up(mb, 128);
     const double dV = c.dV;
+    const int gv = grp16_ok<T>(ld, {x, base}) ? 1 : 0;  // 16-byte element groups
     PcArgs pa{c.n1, c.n2, c.n3, VT % c.n1, (VT / c.n1) % c.n2, VT / (c.n1 * c.n2),
               c.pc.c - 0.0, c.pc.c1, c.pc.c2, c.pc.c3};
     auto finish = [&](int K, double scale, double* out, const int* act) {
@@ -464,10 +529,10 @@ static int cg_run(T* x, long ld, int mb, int spin, double* esp, double* res, int
     RS_CHECK(hpsi_device<T>(x, v.hx, ld, mb, spin, nullptr));
     {
         DotPairs<1> pr{{0}, {1}};
-        launch(k_multidot<T, 2, 1>, vg, VT, 0, st, x, v.hx, nullptr, nullptr, ld, n, pr, part, nullptr);
+        launch(k_multidot<T, 2, 1>, vg, VT, 0, st, x, v.hx, nullptr, nullptr, ld, n, pr, part, nullptr, gv);
         finish(1, dV, s.E, nullptr);
     }
-    launch(k_cg_g<T>, vg, VT, 0, st, v, ld, n, s.E, part, nullptr);
+    launch(k_cg_g<T>, vg, VT, 0, st, v, ld, n, s.E, part, nullptr, gv);
     finish(1, dV, s.rb, nullptr);
     RS_LAUNCH();
 
@@ -505,7 +570,8 @@ static int cg_run(T* x, long ld, int mb, int spin, double* esp, double* res, int
             // --- rb = <Pg|g> dV; search direction
             {
                 DotPairs<1> pr{{0}, {1}};
-                launch(k_multidot<T, 2, 1>, vg, VT, 0, st, v.Pg, v.g, nullptr, nullptr, ld, n, pr, part, s.active);
+                launch(k_multidot<T, 2, 1>, vg, VT, 0, st, v.Pg, v.g, nullptr, nullptr, ld, n, pr, part, s.active,
+                       gv);
                 finish(1, dV, s.rb, s.active);
             }
             launch(s_p, sb, 128, 0, st, s, mb, icg == 1);
@@ -516,14 +582,14 @@ static int cg_run(T* x, long ld, int mb, int spin, double* esp, double* res, int
         // --- six dots: <x|x>, <p|x>, <p|p>, <x|Hx>, <p|Hx>, <p|Hp>
         {
             DotPairs<6> pr{{0, 1, 1, 0, 1, 1}, {0, 0, 1, 2, 2, 3}};
-            launch(k_multidot<T, 4, 6>, vg, VT, 0, st, x, v.p, v.hx, v.hp, ld, n, pr, part, s.active);
+            launch(k_multidot<T, 4, 6>, vg, VT, 0, st, x, v.p, v.hx, v.hp, ld, n, pr, part, s.active, gv);
             finish(6, dV, s.dots, s.active);
         }
         launch(s_eig, sb, 128, 0, st, s, mb);
-        launch(k_cg_upd1<T>, vg, VT, 0, st, v, ld, n, s, part, s.active);
+        launch(k_cg_upd1<T>, vg, VT, 0, st, v, ld, n, s, part, s.active, gv);
         finish(1, dV, s.rb, s.active);
         launch(s_rej, sb, 128, 0, st, s, mb);
-        launch(k_cg_upd2<T>, vg, VT, 0, st, v, ld, n, s, s.active);
+        launch(k_cg_upd2<T>, vg, VT, 0, st, v, ld, n, s, s.active, gv);
         RS_LAUNCH();
     }
     RS_CUDA(cudaMemcpyAsync(esp, s.E, sizeof(double) * mb, cudaMemcpyDeviceToDevice, st));

@@ -3,13 +3,42 @@
 // 7-point preconditioner operator and the s-step basis vectors.
 #pragma once
 
+#include <cstdint>
+#include <initializer_list>
+
 #include "common.cuh"
+#include "vec16.cuh"
 
 namespace rsdft {
 
 constexpr int VT = 256;           // threads per vector CTA
 constexpr int VITEMS = 32;        // elements per thread
 constexpr int VCHUNK = VT * VITEMS;
+
+// 16-byte element groups of the vector kernels: a thread takes W = 16 /
+// sizeof(T) consecutive elements per step (one vector access per stream);
+// the scalar form serves misaligned shapes and the tail.
+template <typename T>
+struct Grp16 {
+    static constexpr int W = 16 / (int)sizeof(T);
+    using V = typename Vec16<T>::t;
+    __device__ static __forceinline__ void load(const T* p, T (&v)[W]) {
+        Vec16<T>::get(*reinterpret_cast<const V*>(p), v);
+    }
+    __device__ static __forceinline__ void store(T* p, const T (&v)[W]) {
+        *reinterpret_cast<V*>(p) = Vec16<T>::make(v);
+    }
+};
+
+// Whether 16-byte accesses suit vectors of leading dimension ld at these
+// bases (host side).
+template <typename T>
+inline bool grp16_ok(long ld, std::initializer_list<const void*> ptrs) {
+    if ((ld * (long)sizeof(T)) % 16 != 0) return false;
+    for (const void* p : ptrs)
+        if (p && reinterpret_cast<uintptr_t>(p) % 16 != 0) return false;
+    return true;
+}
 
 struct CGScal {
     double *E, *E1, *rb, *gkgk, *res, *u11, *u21, *W, *rr0, *rr1, *pa, *pb, *bk, *dots;

@@ -142,7 +142,9 @@ __global__ void s_sstep(CGScal s, const double* __restrict__ ss, double* __restr
 template <typename T>
 __global__ void __launch_bounds__(VT) k_ss_p(const T* __restrict__ g, SSVec<T> sv, T* __restrict__ p, long ld,
                                              long n, const double* __restrict__ cz, const double* __restrict__ bk_,
-                                             int m, int first, const int* __restrict__ active) {
+                                             int m, int first, const int* __restrict__ active, int vec) {
+    using G = Grp16<T>;
+    constexpr int W = G::W;
     const int b = blockIdx.y;
     if (active && !active[b]) return;
     const long off = (long)b * ld, base = (long)blockIdx.x * VCHUNK;
@@ -150,15 +152,34 @@ __global__ void __launch_bounds__(VT) k_ss_p(const T* __restrict__ g, SSVec<T> s
 #pragma unroll
     for (int j = 0; j < SS_MAXM; ++j) c[j] = (T)cz[(long)b * SS_MAXM + j];
     const T bk = (T)bk_[b];
-#pragma unroll 8
-    for (int it = 0; it < VITEMS; ++it) {
-        const long i = base + it * VT + threadIdx.x;
-        if (i < n) {
-            T pg = g[off + i];
+#pragma unroll 2
+    for (int it = 0; it < VITEMS / W; ++it) {
+        const long i = base + ((long)it * VT + threadIdx.x) * W;
+        if (vec && i + W <= n) {
+            T pg[W], t[W];
+            G::load(g + off + i, pg);
 #pragma unroll
-            for (int j = 0; j < SS_MAXM; ++j)
-                if (j < m) pg += c[j] * sv.w[j][off + i];
-            p[off + i] = first ? pg : pg + bk * p[off + i];
+            for (int j = 0; j < SS_MAXM; ++j) {
+                if (j < m) {
+                    G::load(sv.w[j] + off + i, t);
+#pragma unroll
+                    for (int q = 0; q < W; ++q) pg[q] += c[j] * t[q];
+                }
+            }
+            if (!first) {
+                G::load(p + off + i, t);
+#pragma unroll
+                for (int q = 0; q < W; ++q) pg[q] += bk * t[q];
+            }
+            G::store(p + off + i, pg);
+        } else {
+            for (int q = 0; q < W && i + q < n; ++q) {
+                T pg = g[off + i + q];
+#pragma unroll
+                for (int j = 0; j < SS_MAXM; ++j)
+                    if (j < m) pg += c[j] * sv.w[j][off + i + q];
+                p[off + i + q] = first ? pg : pg + bk * p[off + i + q];
+            }
         }
     }
 }
@@ -614,7 +635,8 @@ int sstep_precond(const T* g, const SSVec<T>& sv, T* p, long ld, int mb, int mlo
         finish_to(D, out, nch);
     }
     launch(s_sstep, sb, 128, 0, st, s, ss, cz, mb, mloop, pa.d, dV, first);
-    launch(k_ss_p<T>, vg, VT, 0, st, g, sv, p, ld, n, cz, s.bk, mloop, first, s.active);
+    const int gv = grp16_ok<T>(ld, {g, p, sv.w[0], sv.w[1], sv.w[2], sv.w[3]}) ? 1 : 0;
+    launch(k_ss_p<T>, vg, VT, 0, st, g, sv, p, ld, n, cz, s.bk, mloop, first, s.active, gv);
     RS_LAUNCH();
     return RSDFT_OK;
 }
