@@ -31,16 +31,25 @@ __global__ void k_finish(const double* __restrict__ part, int nchunk, int K, int
     out[i] = s * scale;
 }
 
-template <int K>
-struct DotPairs {
-    int a[K], b[K];
+// Dot-product pair tables as types, so every operand index is a compile-time
+// constant and the per-element values stay in registers.
+struct DotsXY {  // <v0|v1>
+    static constexpr int K = 1;
+    __host__ __device__ static constexpr int a(int) { return 0; }
+    __host__ __device__ static constexpr int b(int) { return 1; }
+};
+struct DotsCG6 {  // <x|x>, <p|x>, <p|p>, <x|Hx>, <p|Hx>, <p|Hp> for (x, p, Hx, Hp)
+    static constexpr int K = 6;
+    __host__ __device__ static constexpr int a(int k) { return (k == 0 || k == 3) ? 0 : 1; }
+    __host__ __device__ static constexpr int b(int k) { return k < 2 ? 0 : (k == 2 ? 1 : (k == 5 ? 3 : 2)); }
 };
 
 // K dot products per band among up to 4 vectors, one read of each vector.
-template <typename T, int NV, int K>
+template <typename T, int NV, class P>
 __global__ void __launch_bounds__(VT) k_multidot(const T* v0, const T* v1, const T* v2, const T* v3, long ld,
-                                                 long n, DotPairs<K> pr, double* __restrict__ part,
-                                                 const int* __restrict__ active, int vec) {
+                                                 long n, double* __restrict__ part, const int* __restrict__ active,
+                                                 int vec) {
+    constexpr int K = P::K;
     using G = Grp16<T>;
     constexpr int W = G::W;
     __shared__ double sh[K * (VT / 32)];
@@ -71,7 +80,7 @@ __global__ void __launch_bounds__(VT) k_multidot(const T* v0, const T* v1, const
 #pragma unroll
             for (int q = 0; q < NV; ++q) v[q] = (double)vv[q][e];
 #pragma unroll
-            for (int k = 0; k < K; ++k) acc[k] = fma(v[pr.a[k]], v[pr.b[k]], acc[k]);
+            for (int k = 0; k < K; ++k) acc[k] = fma(v[P::a(k)], v[P::b(k)], acc[k]);
         }
     }
     block_sum_n<VT, K>(acc, sh);
@@ -469,9 +478,8 @@ int esp_device(const double* x, long ld, int nb, int spin, double* e, double* re
     RS_CHECK(workspace_t("esp_part", (size_t)nb * nchunk, &part));
     RS_CHECK(hpsi_device<double>(x, hx, ld, nb, spin, nullptr));
     const dim3 vg(nchunk, nb);
-    DotPairs<1> pr{{0}, {1}};
     const int gv = grp16_ok<double>(ld, {x, hx}) ? 1 : 0;
-    launch(k_multidot<double, 2, 1>, vg, VT, 0, st, x, hx, nullptr, nullptr, ld, n, pr, part, nullptr, gv);
+    launch(k_multidot<double, 2, DotsXY>, vg, VT, 0, st, x, hx, nullptr, nullptr, ld, n, part, nullptr, gv);
     launch(k_finish, div_up(nb, 128), 128, 0, st, part, nchunk, 1, nb, c.dV, e, nullptr);
     if (res) {
         launch(k_resid, vg, VT, 0, st, x, hx, ld, n, e, part);
@@ -528,8 +536,7 @@ static int cg_run(T* x, long ld, int mb, int spin, double* esp, double* res, int
     launch(s_init, sb, 128, 0, st, s, mb);
     RS_CHECK(hpsi_device<T>(x, v.hx, ld, mb, spin, nullptr));
     {
-        DotPairs<1> pr{{0}, {1}};
-        launch(k_multidot<T, 2, 1>, vg, VT, 0, st, x, v.hx, nullptr, nullptr, ld, n, pr, part, nullptr, gv);
+        launch(k_multidot<T, 2, DotsXY>, vg, VT, 0, st, x, v.hx, nullptr, nullptr, ld, n, part, nullptr, gv);
         finish(1, dV, s.E, nullptr);
     }
     launch(k_cg_g<T>, vg, VT, 0, st, v, ld, n, s.E, part, nullptr, gv);
@@ -569,8 +576,7 @@ static int cg_run(T* x, long ld, int mb, int spin, double* esp, double* res, int
             RS_LAUNCH();
             // --- rb = <Pg|g> dV; search direction
             {
-                DotPairs<1> pr{{0}, {1}};
-                launch(k_multidot<T, 2, 1>, vg, VT, 0, st, v.Pg, v.g, nullptr, nullptr, ld, n, pr, part, s.active,
+                launch(k_multidot<T, 2, DotsXY>, vg, VT, 0, st, v.Pg, v.g, nullptr, nullptr, ld, n, part, s.active,
                        gv);
                 finish(1, dV, s.rb, s.active);
             }
@@ -581,8 +587,7 @@ static int cg_run(T* x, long ld, int mb, int spin, double* esp, double* res, int
         RS_CHECK(hpsi_device<T>(v.p, v.hp, ld, mb, spin, s.active));
         // --- six dots: <x|x>, <p|x>, <p|p>, <x|Hx>, <p|Hx>, <p|Hp>
         {
-            DotPairs<6> pr{{0, 1, 1, 0, 1, 1}, {0, 0, 1, 2, 2, 3}};
-            launch(k_multidot<T, 4, 6>, vg, VT, 0, st, x, v.p, v.hx, v.hp, ld, n, pr, part, s.active, gv);
+            launch(k_multidot<T, 4, DotsCG6>, vg, VT, 0, st, x, v.p, v.hx, v.hp, ld, n, part, s.active, gv);
             finish(6, dV, s.dots, s.active);
         }
         launch(s_eig, sb, 128, 0, st, s, mb);
