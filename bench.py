@@ -195,6 +195,12 @@ def run_reference(args, rank, world):
 
 
 # ------------------------------------------------------------- our arm
+# DRAM bytes (read + write) of one hpsi call per band, from the ncu capture of
+# the three hpsi kernels on Si216 with 64 bands (k_nl_project 171.8 MB,
+# k_stencil_tma 378.9 MB, k_nl_scatter 211.4 MB), scaled by the band count.
+HPSI_TRAFFIC_PER_BAND = {"si216": (171.8e6 + 378.9e6 + 211.4e6) / 64}
+
+
 def hpsi_bytes(cell, nb):
     return nb * cell.ML * 16 + cell.ML * 8 + int(cell.lma_ptr[-1]) * 12
 
@@ -403,7 +409,9 @@ def main():
             "forms": {m: {"ms_per_iter": r["ms"], "iter_s": 1000.0 / r["ms"]} for m, r in results.items()},
             "hpsi": {"ms": hms, "gbs": hgbs, "bytes": hb, "frac_of_hbm": hgbs / hbm},
             "roofline": {"bound": "hbm", "achieved": hgbs, "peak": hbm, "unit": "GB/s", "frac": hgbs / hbm,
-                         "traffic": None, "kernel": "hpsi (k_nl_project + k_stencil), all bands",
+                         "traffic": (HPSI_TRAFFIC_PER_BAND[args.workload] * MB
+                                     if args.workload in HPSI_TRAFFIC_PER_BAND else None),
+                         "kernel": "hpsi (k_nl_project + k_stencil_tma + k_nl_scatter), all bands",
                          "peak_source": peak_src},
             "e2e": e2e,
             "gpu_launches": launches,
