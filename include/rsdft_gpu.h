@@ -156,6 +156,15 @@ int rsdft_gpu_subspace_rotv(int k, int s, double *unk, long ld, int mb, const do
  * subspace_diag_la_module.f90:18-232) */
 int rsdft_gpu_subspace_diag(int k, int s, double *unk, long ld, int mb, double *esp, int mode);
 
+/* gram_schmidt followed by subspace_diag, as calc_sweep calls them
+ * (sweep_module.f90:152-155), in one Rayleigh-Ritz step: overlap Cholesky
+ * S = R^T R, eigen-decomposition of R^-T Hsub R^-1 and one rotation by
+ * R^-1 V.  Same eigenvalues and orthonormal bands as the pair (replaces
+ * gram_schmidt_t_module.f90:84-316 + subspace_diag_la_module.f90:18-232);
+ * an ill-conditioned overlap takes the explicit CholeskyQR2 + subspace_diag
+ * path. */
+int rsdft_gpu_orth_subspace_diag(int k, int s, double *unk, long ld, int mb, double *esp, int mode);
+
 /* e(ns:ne) = dV <wf_n|H wf_n>, FP64 (no normalisation, as the reference).
  * (replaces esp_calc(k,s,wf,n1,n2,ns,ne,e), esp_calc_module.f90:15-49) */
 int rsdft_gpu_esp_calc(int k, int s, const double *wf, int n1, int n2, int ns, int ne, double *e);

@@ -152,6 +152,11 @@ class RsdftGpu:
         _lib.call("rsdft_gpu_subspace_diag", k, s, _ptr(unk, name="unk"), _ld(unk), unk.shape[1],
                   _ptr(esp, name="esp"), mode)
 
+    def orth_subspace_diag(self, k, s, unk, esp, *, mode=MODE_FP64) -> None:
+        """gram_schmidt + subspace_diag as one Rayleigh-Ritz step."""
+        _lib.call("rsdft_gpu_orth_subspace_diag", k, s, _ptr(unk, name="unk"), _ld(unk), unk.shape[1],
+                  _ptr(esp, name="esp"), mode)
+
     def subspace_mate_sl(self, k, s, unk, hsub) -> None:
         _lib.call("rsdft_gpu_subspace_mate", k, s, _ptr(unk, name="unk"), _ld(unk), unk.shape[1],
                   _ptr(hsub, name="hsub"), _ld(hsub))
@@ -189,10 +194,14 @@ class RsdftGpu:
         self.gram_schmidt(1, mb, 1, 1, unk, mode=MODE_FP64)
         self.residual(1, 1, unk, esp, res)
 
-    def eigensolver_iteration(self, unk, esp, res, *, ncg=4, mloop=3, mode=MODE_FP64) -> None:
+    def eigensolver_iteration(self, unk, esp, res, *, ncg=4, mloop=3, mode=MODE_FP64, fused=True) -> None:
         """One sweep iteration as calc_sweep runs it (sweep_module.f90:150-155):
-        conjugate_gradient -> gram_schmidt -> subspace_diag."""
+        conjugate_gradient -> gram_schmidt -> subspace_diag; with fused=True
+        the last two run as one Rayleigh-Ritz step (orth_subspace_diag)."""
         ml, mb = unk.shape
         self.conjugate_gradient(1, ml, mb, 1, 1, unk, esp, res, ncg=ncg, mloop=mloop, mode=mode)
-        self.gram_schmidt(1, mb, 1, 1, unk, mode=mode)
-        self.subspace_diag(1, 1, unk, esp, mode=mode)
+        if fused:
+            self.orth_subspace_diag(1, 1, unk, esp, mode=mode)
+        else:
+            self.gram_schmidt(1, mb, 1, 1, unk, mode=mode)
+            self.subspace_diag(1, 1, unk, esp, mode=mode)

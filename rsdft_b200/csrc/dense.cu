@@ -179,6 +179,104 @@ int subspace_diag_device(double* psi, long ld, int mb, int spin, double* esp, in
     return RSDFT_OK;
 }
 
+// min and max of the diagonal of an n x n matrix (one block)
+__global__ void k_diag_minmax(const double* __restrict__ a, int n, int lda, double* __restrict__ out) {
+    __shared__ double smin[256], smax[256];
+    double lo = 1e300, hi = 0.0;
+    for (int i = threadIdx.x; i < n; i += blockDim.x) {
+        const double v = fabs(a[(long)i * lda + i]);
+        lo = fmin(lo, v);
+        hi = fmax(hi, v);
+    }
+    smin[threadIdx.x] = lo;
+    smax[threadIdx.x] = hi;
+    __syncthreads();
+    for (int s = blockDim.x / 2; s > 0; s >>= 1) {
+        if (threadIdx.x < s) {
+            smin[threadIdx.x] = fmin(smin[threadIdx.x], smin[threadIdx.x + s]);
+            smax[threadIdx.x] = fmax(smax[threadIdx.x], smax[threadIdx.x + s]);
+        }
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) {
+        out[0] = smin[0];
+        out[1] = smax[0];
+    }
+}
+
+// Gram-Schmidt followed by subspace_diag (the pair calc_sweep calls,
+// sweep_module.f90:152-155) as one Rayleigh-Ritz step on the CG output:
+//   S = dV psi^T psi = R^T R,  H = dV sym(psi^T H psi),
+//   R^-T H R^-1 = V diag(e) V^T,  psi <- psi (R^-1 V).
+// psi R^-1 is the Gram-Schmidt basis (the unique positive-R QR factor), so
+// the eigenpairs and the rotated bands are those of the pair, with one
+// overlap Cholesky, one eigensolve and one tall rotation instead of two
+// CholeskyQR passes, the eigensolve and a separate rotation.  When the
+// overlap is ill-conditioned (diag(R) spread beyond kappa_max^(1/2); one
+// Cholesky pass then loses orthogonality), the explicit CholeskyQR2 +
+// subspace_diag path runs instead.
+int orth_subspace_diag_device(double* psi, long ld, int mb, int spin, double* esp, int mode) {
+    Context& c = ctx();
+    double *hpsi = nullptr, *S = nullptr, *H = nullptr, *T = nullptr, *mm = nullptr;
+    int* dinfo = nullptr;
+    RS_CHECK(workspace_t("sub_hpsi", (size_t)ld * mb, &hpsi));
+    RS_CHECK(workspace_t("gs_S", (size_t)mb * mb, &S));
+    RS_CHECK(workspace_t("sub_H", (size_t)mb * mb, &H));
+    RS_CHECK(workspace_t("osd_T", (size_t)mb * mb, &T));
+    RS_CHECK(workspace_t("osd_minmax", 2, &mm));
+    RS_CHECK(workspace_t("gs_info", 4, &dinfo));
+    const double zero = 0.0, one = 1.0;
+    RS_CHECK(hpsi_device<double>(psi, hpsi, ld, mb, spin, nullptr));
+    if (mode == RSDFT_MODE_FP64) {
+        RS_CHECK(gemm_tn_splitk(psi, psi, ld, mb, mb, c.dV, 0, S));
+        RS_CHECK(gemm_tn_splitk(psi, hpsi, ld, mb, mb, c.dV, 1, H));
+    } else {
+        RS_CHECK(gram_mixed(psi, psi, ld, mb, c.dV, 0, mode_terms(mode), S));
+        RS_CHECK(gram_mixed(psi, hpsi, ld, mb, c.dV, 1, mode_terms(mode), H));
+    }
+    int lwork = 0;
+    RS_SOLVER(cusolverDnDpotrf_bufferSize(c.solver, CUBLAS_FILL_MODE_UPPER, mb, S, mb, &lwork));
+    double* work = nullptr;
+    RS_CHECK(workspace_t("gs_potrf", (size_t)lwork + 1, &work));
+    RS_SOLVER(cusolverDnDpotrf(c.solver, CUBLAS_FILL_MODE_UPPER, mb, S, mb, work, lwork, dinfo));
+    RS_CHECK(check_info(dinfo, "orth_subspace_diag: overlap Cholesky"));
+    launch(k_diag_minmax, 1, 256, 0, c.stream, S, mb, mb, mm);
+    RS_LAUNCH();
+    double hmm[2] = {0.0, 0.0};
+    RS_CUDA(cudaMemcpyAsync(hmm, mm, sizeof(hmm), cudaMemcpyDeviceToHost, c.stream));
+    RS_CUDA(cudaStreamSynchronize(c.stream));
+    const double kappa_max = mode == RSDFT_MODE_FP64 ? 1e3 : 1e2;
+    if (!(hmm[0] > 0.0) || (hmm[1] / hmm[0]) * (hmm[1] / hmm[0]) > kappa_max) {
+        RS_CHECK(gram_schmidt_device(psi, ld, mb, mode));
+        return subspace_diag_device(psi, ld, mb, spin, esp, mode);
+    }
+    size_t dws = 0, hws = 0;
+    RS_SOLVER(cusolverDnXtrtri_bufferSize(c.solver, CUBLAS_FILL_MODE_UPPER, CUBLAS_DIAG_NON_UNIT, mb, CUDA_R_64F, S,
+                                          mb, &dws, &hws));
+    void* dw = nullptr;
+    RS_CHECK(workspace("gs_trtri", dws + 16, &dw));
+    static std::vector<char> hw;
+    if (hw.size() < hws + 16) hw.resize(hws + 16);
+    RS_SOLVER(cusolverDnXtrtri(c.solver, CUBLAS_FILL_MODE_UPPER, CUBLAS_DIAG_NON_UNIT, mb, CUDA_R_64F, S, mb, dw,
+                               dws, hw.data(), hws, dinfo));
+    RS_CHECK(check_info(dinfo, "orth_subspace_diag: triangular inverse"));
+    launch(k_zero_lower, dim3(div_up(mb, 128), mb), 128, 0, c.stream, S, mb, mb);
+    RS_LAUNCH();
+    // Hr = R^-T H R^-1 (T = H R^-1, then H = R^-T T), eigenpairs, T = R^-1 V
+    RS_BLAS(cublasDgemm(c.blas, CUBLAS_OP_N, CUBLAS_OP_N, mb, mb, mb, &one, H, mb, S, mb, &zero, T, mb));
+    RS_BLAS(cublasDgemm(c.blas, CUBLAS_OP_T, CUBLAS_OP_N, mb, mb, mb, &one, S, mb, T, mb, &zero, H, mb));
+    RS_CHECK(syevd(H, mb, esp, CUBLAS_FILL_MODE_UPPER, "orth_subspace_diag: syevd"));
+    RS_BLAS(cublasDgemm(c.blas, CUBLAS_OP_N, CUBLAS_OP_N, mb, mb, mb, &one, S, mb, H, mb, &zero, T, mb));
+    if (mode == RSDFT_MODE_FP64)
+        RS_BLAS(cublasDgemm(c.blas, CUBLAS_OP_N, CUBLAS_OP_N, (int)c.ml, mb, mb, &one, psi, (int)ld, T, mb, &zero,
+                            hpsi, (int)ld));
+    else
+        RS_CHECK(rotate_mixed(psi, hpsi, ld, mb, T, mb, mode_terms(mode)));
+    RS_CUDA(cudaMemcpy2DAsync(psi, ld * sizeof(double), hpsi, ld * sizeof(double), c.ml * sizeof(double), mb,
+                              cudaMemcpyDeviceToDevice, c.stream));
+    return RSDFT_OK;
+}
+
 }  // namespace rsdft
 
 using namespace rsdft;
@@ -288,6 +386,24 @@ int rsdft_gpu_subspace_rotv(int k, int s, double* unk, long ld, int mb, const do
                         (int)ld));
     RS_CUDA(cudaMemcpy2DAsync(d, ld * sizeof(double), tmp, ld * sizeof(double), c.ml * sizeof(double), mb,
                               cudaMemcpyDeviceToDevice, c.stream));
+    RS_CHECK(wf_release(unk, d, ld, mb, st));
+    return RSDFT_OK;
+}
+
+int rsdft_gpu_orth_subspace_diag(int k, int s, double* unk, long ld, int mb, double* esp, int mode) {
+    RS_CHECK(require_grid());
+    RS_CHECK(check_k_s(k, s, "orth_subspace_diag"));
+    Context& c = ctx();
+    if (ld < c.ml || mb < 1 || !esp || mode < 0 || mode > 2) {
+        set_error("orth_subspace_diag: bad arguments");
+        return RSDFT_EINVAL;
+    }
+    double *d, *W;
+    bool st;
+    RS_CHECK(wf_acquire(unk, ld, mb, "sd_unk", &d, &st));
+    RS_CHECK(workspace_t("sd_W", (size_t)mb, &W));
+    RS_CHECK(orth_subspace_diag_device(d, ld, mb, s, W, mode));
+    RS_CHECK(stage_out(esp, W, sizeof(double) * mb));
     RS_CHECK(wf_release(unk, d, ld, mb, st));
     return RSDFT_OK;
 }

@@ -59,6 +59,9 @@ int gram_schmidt_device(double* psi, long ld, int nb, int mode);
 // Rayleigh-Ritz (subspace_diag_la) on device data.
 int subspace_diag_device(double* psi, long ld, int mb, int spin, double* esp_dev, int mode);
 
+// Gram-Schmidt + Rayleigh-Ritz as one step (device data).
+int orth_subspace_diag_device(double* psi, long ld, int mb, int spin, double* esp_dev, int mode);
+
 // CG over all bands (device data).
 int cg_device(double* unk, long ld, int mb, int spin, double* esp_dev, double* res_dev, int ncg, int mloop,
               int ipc, int mode);

@@ -162,8 +162,12 @@ __global__ void __launch_bounds__(U_THREADS, 1) k_umma(const __grid_constant__ U
     constexpr int ABYTES = UB_M * UB_K * 2;  // one A slice tile
     constexpr int BBYTES = BN * UB_K * 2;
     constexpr int STAGE = NT * (ABYTES + BBYTES);
-    constexpr int NACC = DRAIN ? 2 : 1;
-    constexpr int TCOLS = NACC * BN;  // 256 in both configurations
+    // DRAIN: two accumulators per segment buffer, one for the hi x hi product
+    // and one for the smaller cross products, double-buffered (the FP32
+    // accumulation truncates; keeping the dominant term's chain short keeps
+    // that bias near 2^-24 x 2 U_SEG instead of x 6 x 2 U_SEG)
+    constexpr int NACC = DRAIN ? 4 : 1;
+    constexpr int TCOLS = NACC * BN;  // 512 (DRAIN, BN = 128) or 256 (DIRECT, BN = 256)
     constexpr uint32_t IDESC = umma_idesc_bf16(UB_M, BN);
     extern __shared__ __align__(1024) unsigned char smem[];
     uint64_t* full = reinterpret_cast<uint64_t*>(smem + (size_t)NS * STAGE);
@@ -233,9 +237,10 @@ __global__ void __launch_bounds__(U_THREADS, 1) k_umma(const __grid_constant__ U
                 const int b = seg & 1;
                 if (DRAIN && seg >= 2 && !mbar_wait(&acce[b], ((seg >> 1) - 1) & 1)) ok = false;
                 tc_fence_after();
-                const uint32_t d = tbase + (uint32_t)(b * BN);
+                const uint32_t d = tbase + (uint32_t)((DRAIN ? 2 * b : b) * BN);
+                const uint32_t dx = DRAIN ? d + (uint32_t)BN : d;  // cross products
                 const int itend = DRAIN ? min(nkb, (seg + 1) * U_SEG) : nkb;
-                bool first = true;
+                bool first = true, firstx = true;
                 for (; it < itend; ++it) {
                     const int s = it % NS;
                     if (!mbar_wait(&full[s], (it / NS) & 1)) ok = false;
@@ -250,8 +255,13 @@ __global__ void __launch_bounds__(U_THREADS, 1) k_umma(const __grid_constant__ U
                         for (int kk = 0; kk < UB_K / 16; ++kk) {
                             const uint64_t ad = umma_desc_sw64(sa + ta * ABYTES + kk * 32);
                             const uint64_t bd = umma_desc_sw64(sb + tb * BBYTES + kk * 32);
-                            umma_bf16(d, ad, bd, IDESC, first ? 0u : 1u);
-                            first = false;
+                            if (DRAIN && p > 0) {
+                                umma_bf16(dx, ad, bd, IDESC, firstx ? 0u : 1u);
+                                firstx = false;
+                            } else {
+                                umma_bf16(d, ad, bd, IDESC, first ? 0u : 1u);
+                                first = false;
+                            }
                         }
                     }
                     umma_commit(&empty[s]);
@@ -276,7 +286,12 @@ __global__ void __launch_bounds__(U_THREADS, 1) k_umma(const __grid_constant__ U
 #pragma unroll
                 for (int c0 = 0; c0 < CW; c0 += 32) {
                     uint32_t r[32];
-                    tmem_ld_x32(tbase + ((uint32_t)(32 * q) << 16) + (uint32_t)(b * BN + h * CW + c0), r);
+                    const uint32_t ta = tbase + ((uint32_t)(32 * q) << 16) + (uint32_t)(2 * b * BN + h * CW + c0);
+                    tmem_ld_x32(ta, r);  // hi x hi
+                    tmem_ld_wait();
+#pragma unroll
+                    for (int j = 0; j < 32; ++j) acc[c0 + j] += (double)__uint_as_float(r[j]);
+                    tmem_ld_x32(ta + (uint32_t)BN, r);  // cross products
                     tmem_ld_wait();
 #pragma unroll
                     for (int j = 0; j < 32; ++j) acc[c0 + j] += (double)__uint_as_float(r[j]);

@@ -48,6 +48,22 @@ def test_mixed_subspace_diag(gpu, cells, mode, tol):
     assert overlap_check(host(u), ref, w, c.dV, gap_tol=1e-3) <= 1e3 * tol
 
 
+@pytest.mark.parametrize("mode,tol", [(api.MODE_MIXED_BF16, 3e-6), (api.MODE_MIXED_BF16X3, 1e-4)])
+def test_mixed_orth_subspace_diag(gpu, cells, mode, tol):
+    c, o = prepare(gpu, cells, "si64")
+    nb = 160
+    q = o.gram_schmidt_t(np.asfortranarray(c.psi0()[:, :nb]))
+    u0, _, _, _ = o.conjugate_gradient(q, 4, 3)
+    ref, w, _ = o.subspace_diag_la(o.gram_schmidt_t(u0))
+    u = dev(u0)
+    esp = torch.zeros(nb, dtype=torch.float64, device="cuda")
+    gpu.orth_subspace_diag(1, 1, u, esp, mode=mode)
+    torch.cuda.synchronize()
+    g = host(u)
+    assert np.abs(host(esp) - w).max() <= tol * max(1.0, np.abs(w).max())
+    assert np.abs(g.T @ g * c.dV - np.eye(nb)).max() <= 10 * tol
+
+
 def test_mixed_cg_sweep_fp32(gpu, cells):
     c, o = prepare(gpu, cells, "si8")
     q = o.gram_schmidt_t(c.psi0())

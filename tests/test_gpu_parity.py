@@ -183,6 +183,41 @@ def test_subspace_mate_solv_rotv(gpu, cells):
     assert overlap_check(host(u), rot_ref, w_ref, c.dV) <= 1e-10
 
 
+@pytest.mark.parametrize("name,nb", [("si8", 32), ("si64", 160)])
+def test_orth_subspace_diag_matches_gs_then_subspace(gpu, cells, name, nb):
+    """One Rayleigh-Ritz step on non-orthonormal bands (a CG sweep's output)
+    equals gram_schmidt followed by subspace_diag."""
+    c, o = prepare(gpu, cells, name)
+    q = o.gram_schmidt_t(np.asfortranarray(c.psi0()[:, :nb]))
+    u0, _, _, _ = o.conjugate_gradient(q, 4, 3)
+    ref, w, _ = o.subspace_diag_la(o.gram_schmidt_t(u0))
+    u = dev(u0)
+    esp = torch.zeros(nb, dtype=torch.float64, device="cuda")
+    gpu.orth_subspace_diag(1, 1, u, esp)
+    torch.cuda.synchronize()
+    g = host(u)
+    assert rel(host(esp), w) <= 1e-12
+    assert np.abs(g.T @ g * c.dV - np.eye(nb)).max() <= 1e-12
+    assert overlap_check(g, ref, w, c.dV) <= 1e-9
+
+
+def test_orth_subspace_diag_ill_conditioned_overlap(gpu, cells):
+    """Two nearly parallel bands: the explicit CholeskyQR2 path is taken and
+    the result still equals gram_schmidt followed by subspace_diag."""
+    c, o = prepare(gpu, cells, "si8")
+    nb = 32
+    u0 = np.asfortranarray(c.psi0()[:, :nb]).copy()
+    u0[:, 1] = u0[:, 0] + 1e-4 * u0[:, 1]
+    ref, w, _ = o.subspace_diag_la(o.gram_schmidt_t(u0))
+    u = dev(u0)
+    esp = torch.zeros(nb, dtype=torch.float64, device="cuda")
+    gpu.orth_subspace_diag(1, 1, u, esp)
+    torch.cuda.synchronize()
+    g = host(u)
+    assert rel(host(esp), w) <= 1e-10
+    assert np.abs(g.T @ g * c.dV - np.eye(nb)).max() <= 1e-12
+
+
 def test_eigensolver_iteration_sequence(gpu, cells):
     """CG -> GS -> subspace, two iterations, as calc_sweep calls them."""
     c, o = prepare(gpu, cells, "si8")
