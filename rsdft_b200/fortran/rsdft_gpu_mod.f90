@@ -98,6 +98,13 @@ MODULE rsdft_gpu_mod
        type(c_ptr), value :: unk, esp
        integer(c_long), value :: ld
      end function rsdft_gpu_subspace_diag
+     integer(c_int) function rsdft_gpu_orth_subspace_diag(k, s, unk, ld, mb, esp, mode) &
+          bind(C, name="rsdft_gpu_orth_subspace_diag")
+       import :: c_int, c_long, c_ptr
+       integer(c_int), value :: k, s, mb, mode
+       type(c_ptr), value :: unk, esp
+       integer(c_long), value :: ld
+     end function rsdft_gpu_orth_subspace_diag
      integer(c_int) function rsdft_gpu_subspace_mate(k, s, unk, ld, mb, hsub, ldh) &
           bind(C, name="rsdft_gpu_subspace_mate")
        import :: c_int, c_long, c_ptr
@@ -258,6 +265,16 @@ CONTAINS
     call check(rsdft_gpu_subspace_diag(k, s, c_loc(unk), int(size(unk, 1), c_long), int(size(unk, 2), c_int), &
                c_loc(esp), mode), "subspace_diag")
   END SUBROUTINE gpu_subspace_diag
+
+  ! gram_schmidt + subspace_diag of calc_sweep (sweep_module.f90:152-155) in one
+  ! Rayleigh-Ritz step
+  SUBROUTINE gpu_orth_subspace_diag(k, s, unk, esp, mode)
+    integer, intent(IN) :: k, s, mode
+    real(8), intent(INOUT), target :: unk(:, :)
+    real(8), intent(OUT), target :: esp(:)
+    call check(rsdft_gpu_orth_subspace_diag(k, s, c_loc(unk), int(size(unk, 1), c_long), &
+               int(size(unk, 2), c_int), c_loc(esp), mode), "orth_subspace_diag")
+  END SUBROUTINE gpu_orth_subspace_diag
 
   SUBROUTINE gpu_subspace_mate_sl(k, s, unk, hsub)
     integer, intent(IN) :: k, s
