@@ -284,6 +284,9 @@ int rsdft_gpu_set_grid(const int* ngrid, int md, double coef_lap0, const double*
     c.pc.c1 = -0.5 / (hgrid[0] * hgrid[0]) * g[0];
     c.pc.c2 = -0.5 / (hgrid[1] * hgrid[1]) * g[1];
     c.pc.c3 = -0.5 / (hgrid[2] * hgrid[2]) * g[2];
+    // nonlocal tables sized for an earlier grid must not be used with this one
+    // (Vloc is checked against the grid at use)
+    c.nl_set = false;
     c.grid_set = true;
     return RSDFT_OK;
 }
@@ -301,6 +304,7 @@ int rsdft_gpu_set_vloc(const double* vloc, long ml, int nspin) {
     RS_CHECK(upload(&c.vloc, h.data(), h.size()));
     RS_CHECK(upload(&c.vloc32, h32.data(), h32.size()));
     c.nspin = nspin;
+    c.vloc_ml = ml;
     return RSDFT_OK;
 }
 

@@ -65,6 +65,7 @@ struct Context {
     int nspin = 0;
     double* vloc = nullptr;
     float* vloc32 = nullptr;
+    long vloc_ml = -1;  // grid size Vloc was given for
 
     // nonlocal tables
     bool nl_set = false;

@@ -661,8 +661,8 @@ int hpsi_device(const T* psi, T* hpsi, long ld, int nb, int spin, const int* ban
         set_error("hpsi: nb=%d exceeds 65535", nb);
         return RSDFT_EINVAL;
     }
-    if (!c.vloc) {
-        set_error("hpsi: rsdft_gpu_set_vloc has not been called");
+    if (!c.vloc || c.vloc_ml != c.ml) {
+        set_error("hpsi: rsdft_gpu_set_vloc has not been called for the current grid");
         return RSDFT_ENOTINIT;
     }
     const bool nl = c.nl_set && c.nzlma > 0;
@@ -776,8 +776,8 @@ int noalloc_scratch(double** out) {
 // reads it, so nothing left from an earlier call is ever read.
 int hpsi_static_scratch(const double* psi, double* hpsi, long ld, int nb, int spin) {
     Context& c = ctx();
-    if (!c.vloc) {
-        set_error("hamiltonian_noalloc: rsdft_gpu_set_vloc has not been called");
+    if (!c.vloc || c.vloc_ml != c.ml) {
+        set_error("hamiltonian_noalloc: rsdft_gpu_set_vloc has not been called for the current grid");
         return RSDFT_ENOTINIT;
     }
     const bool nl = c.nl_set && c.nzlma > 0;
