@@ -172,7 +172,9 @@ int subspace_diag_device(double* psi, long ld, int mb, int spin, double* esp, in
         RS_CHECK(hpsi_device<double>(psi, hpsi, ld, mb, spin, nullptr));
         RS_CHECK(gram_mixed(psi, hpsi, ld, mb, c.dV, 1, mode_terms(mode), H));
         RS_CHECK(syevd(H, mb, esp, CUBLAS_FILL_MODE_UPPER, "subspace_diag: syevd"));
-        RS_CHECK(rotate_mixed(psi, hpsi, ld, mb, H, mb, mode_terms(mode)));
+        // reads only the BF16 split of psi: written in place
+        RS_CHECK(rotate_mixed(psi, psi, ld, mb, H, mb, mode_terms(mode)));
+        return RSDFT_OK;
     }
     RS_CUDA(cudaMemcpy2DAsync(psi, ld * sizeof(double), hpsi, ld * sizeof(double), c.ml * sizeof(double), mb,
                               cudaMemcpyDeviceToDevice, c.stream));
@@ -231,8 +233,7 @@ int orth_subspace_diag_device(double* psi, long ld, int mb, int spin, double* es
         RS_CHECK(gemm_tn_splitk(psi, psi, ld, mb, mb, c.dV, 0, S));
         RS_CHECK(gemm_tn_splitk(psi, hpsi, ld, mb, mb, c.dV, 1, H));
     } else {
-        RS_CHECK(gram_mixed(psi, psi, ld, mb, c.dV, 0, mode_terms(mode), S));
-        RS_CHECK(gram_mixed(psi, hpsi, ld, mb, c.dV, 1, mode_terms(mode), H));
+        RS_CHECK(gram_mixed_pair(psi, hpsi, ld, mb, c.dV, mode_terms(mode), S, H));
     }
     int lwork = 0;
     RS_SOLVER(cusolverDnDpotrf_bufferSize(c.solver, CUBLAS_FILL_MODE_UPPER, mb, S, mb, &lwork));
@@ -267,13 +268,16 @@ int orth_subspace_diag_device(double* psi, long ld, int mb, int spin, double* es
     RS_BLAS(cublasDgemm(c.blas, CUBLAS_OP_T, CUBLAS_OP_N, mb, mb, mb, &one, S, mb, T, mb, &zero, H, mb));
     RS_CHECK(syevd(H, mb, esp, CUBLAS_FILL_MODE_UPPER, "orth_subspace_diag: syevd"));
     RS_BLAS(cublasDgemm(c.blas, CUBLAS_OP_N, CUBLAS_OP_N, mb, mb, mb, &one, S, mb, H, mb, &zero, T, mb));
-    if (mode == RSDFT_MODE_FP64)
+    if (mode == RSDFT_MODE_FP64) {
         RS_BLAS(cublasDgemm(c.blas, CUBLAS_OP_N, CUBLAS_OP_N, (int)c.ml, mb, mb, &one, psi, (int)ld, T, mb, &zero,
                             hpsi, (int)ld));
-    else
-        RS_CHECK(rotate_mixed(psi, hpsi, ld, mb, T, mb, mode_terms(mode)));
-    RS_CUDA(cudaMemcpy2DAsync(psi, ld * sizeof(double), hpsi, ld * sizeof(double), c.ml * sizeof(double), mb,
-                              cudaMemcpyDeviceToDevice, c.stream));
+        RS_CUDA(cudaMemcpy2DAsync(psi, ld * sizeof(double), hpsi, ld * sizeof(double), c.ml * sizeof(double), mb,
+                                  cudaMemcpyDeviceToDevice, c.stream));
+    } else {
+        // the tensor-core rotation reads only the BF16 split of psi, so it
+        // can write psi itself
+        RS_CHECK(rotate_mixed(psi, psi, ld, mb, T, mb, mode_terms(mode)));
+    }
     return RSDFT_OK;
 }
 

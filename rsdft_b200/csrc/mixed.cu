@@ -393,31 +393,12 @@ static int launch_umma(const UmmaMaps& maps, const UmmaArgs& g, dim3 grid) {
 
 // C (nb x nb) = alpha * A^T B (symmetrize: alpha/2 (A^T B + B^T A)); A, B tall
 // (ML x nb, leading dimension ld); B == A computes only the upper tiles.
-int gram_mixed(const double* A, const double* B, long ld, int nb, double alpha, int symmetrize, int nterms,
-               double* C) {
+// Gram matrix from BF16 slices (ML x nb each, 3 slices): C = alpha sa^T sb,
+// symmetric tile pairs only when same.
+static int gram_from_slices(__nv_bfloat16* sa, __nv_bfloat16* sb, bool same, int nb, double alpha, int symmetrize,
+                            int nterms, double* C) {
     Context& c = ctx();
     const long ml = c.ml;
-    if (ml % 8 != 0) {
-        set_error("mixed contractions need ML to be a multiple of 8");
-        return RSDFT_EUNSUP;
-    }
-    const size_t nsl = (size_t)ml * nb;
-    __nv_bfloat16 *sa = nullptr, *sb = nullptr;
-    RS_CHECK(workspace_t("umma_sa", 3 * nsl, &sa));
-    const int vec = (ml % 8 == 0 && ld % 2 == 0 && reinterpret_cast<uintptr_t>(A) % 16 == 0 &&
-                     reinterpret_cast<uintptr_t>(B) % 16 == 0)
-                        ? 1
-                        : 0;
-    const dim3 sg(div_up(ml, 2048), nb);
-    launch(k_split_cols, sg, 256, 0, c.stream, A, ld, nb, ml, sa, vec);
-    const bool same = (A == B);
-    if (!same) {
-        RS_CHECK(workspace_t("umma_sb", 3 * nsl, &sb));
-        launch(k_split_cols, sg, 256, 0, c.stream, B, ld, nb, ml, sb, vec);
-    } else {
-        sb = sa;
-    }
-    RS_LAUNCH();
     UmmaMaps maps;
     RS_CHECK(map3(&maps.a, sa, ml, nb, UB_M));
     RS_CHECK(map3(&maps.b, sb, ml, nb, 128));
@@ -442,6 +423,42 @@ int gram_mixed(const double* A, const double* B, long ld, int nb, double alpha, 
            nb, alpha, symmetrize, C);
     RS_LAUNCH();
     return RSDFT_OK;
+}
+
+// BF16 slices of a tall FP64 block into the named workspace
+static int split_cols(const double* A, long ld, int nb, const char* ws, __nv_bfloat16** out) {
+    Context& c = ctx();
+    const long ml = c.ml;
+    if (ml % 8 != 0) {
+        set_error("mixed contractions need ML to be a multiple of 8");
+        return RSDFT_EUNSUP;
+    }
+    RS_CHECK(workspace_t(ws, 3 * (size_t)ml * nb, out));
+    const int vec = (ld % 2 == 0 && reinterpret_cast<uintptr_t>(A) % 16 == 0) ? 1 : 0;
+    launch(k_split_cols, dim3(div_up(ml, 2048), nb), 256, 0, c.stream, A, ld, nb, ml, *out, vec);
+    RS_LAUNCH();
+    return RSDFT_OK;
+}
+
+int gram_mixed(const double* A, const double* B, long ld, int nb, double alpha, int symmetrize, int nterms,
+               double* C) {
+    __nv_bfloat16 *sa = nullptr, *sb = nullptr;
+    RS_CHECK(split_cols(A, ld, nb, "umma_sa", &sa));
+    const bool same = (A == B);
+    if (same)
+        sb = sa;
+    else
+        RS_CHECK(split_cols(B, ld, nb, "umma_sb", &sb));
+    return gram_from_slices(sa, sb, same, nb, alpha, symmetrize, nterms, C);
+}
+
+int gram_mixed_pair(const double* psi, const double* hpsi, long ld, int nb, double alpha, int nterms, double* S,
+                    double* H) {
+    __nv_bfloat16 *sa = nullptr, *sb = nullptr;
+    RS_CHECK(split_cols(psi, ld, nb, "umma_sa", &sa));
+    RS_CHECK(split_cols(hpsi, ld, nb, "umma_sb", &sb));
+    RS_CHECK(gram_from_slices(sa, sa, true, nb, alpha, 0, nterms, S));
+    return gram_from_slices(sa, sb, false, nb, alpha, 1, nterms, H);
 }
 
 // out (ML x nb, leading dimension ldo) = psi V, V (nb x nb, leading dimension ldv)

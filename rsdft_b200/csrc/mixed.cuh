@@ -11,8 +11,14 @@ namespace rsdft {
 int gram_mixed(const double* A, const double* B, long ld, int nb, double alpha, int symmetrize, int nterms,
                double* C);
 
+// S = alpha psi^T psi and H = alpha/2 (psi^T Hpsi + Hpsi^T psi) from one
+// split of each operand.
+int gram_mixed_pair(const double* psi, const double* hpsi, long ld, int nb, double alpha, int nterms, double* S,
+                    double* H);
+
 // out (ML x nb, leading dimension ld) = psi V with V (nb x nb, leading
-// dimension ldv).  out must not alias psi.
+// dimension ldv).  psi is read only into its BF16 split before the product,
+// so out may be psi itself.
 int rotate_mixed(const double* psi, double* out, long ld, int nb, const double* V, int ldv, int nterms);
 
 inline int mode_terms(int mode) { return mode == RSDFT_MODE_MIXED_BF16 ? 3 : 2; }
