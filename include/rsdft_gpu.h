@@ -165,6 +165,15 @@ int rsdft_gpu_subspace_diag(int k, int s, double *unk, long ld, int mb, double *
  * path. */
 int rsdft_gpu_orth_subspace_diag(int k, int s, double *unk, long ld, int mb, double *esp, int mode);
 
+/* One sweep iteration for (k, s) as calc_sweep runs it (sweep_module.f90:
+ * 150-155): conjugate_gradient, then gram_schmidt + subspace_diag as in
+ * rsdft_gpu_orth_subspace_diag.  esp(MB) receives the Ritz values, res(MB)
+ * the CG residuals; ld must equal ML.  In the mixed modes the FP32 bands of
+ * the CG sweep feed the Rayleigh-Ritz step directly (FP32 H psi, exact BF16
+ * split) and the rotated bands are written back in FP64. */
+int rsdft_gpu_eigensolver_sweep(int k, int s, double *unk, long ld, int mb, double *esp, double *res, int ncg,
+                                int mloop, int ipc, int mode);
+
 /* e(ns:ne) = dV <wf_n|H wf_n>, FP64 (no normalisation, as the reference).
  * (replaces esp_calc(k,s,wf,n1,n2,ns,ne,e), esp_calc_module.f90:15-49) */
 int rsdft_gpu_esp_calc(int k, int s, const double *wf, int n1, int n2, int ns, int ne, double *e);

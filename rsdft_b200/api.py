@@ -194,14 +194,20 @@ class RsdftGpu:
         self.gram_schmidt(1, mb, 1, 1, unk, mode=MODE_FP64)
         self.residual(1, 1, unk, esp, res)
 
+    def eigensolver_sweep(self, k, s, unk, esp, res, *, ncg=4, mloop=3, ipc=4, mode=MODE_FP64) -> None:
+        """conjugate_gradient + gram_schmidt + subspace_diag in one call."""
+        _lib.call("rsdft_gpu_eigensolver_sweep", k, s, _ptr(unk, name="unk"), _ld(unk), unk.shape[1],
+                  _ptr(esp, name="esp"), _ptr(res, name="res"), ncg, mloop, ipc, mode)
+
     def eigensolver_iteration(self, unk, esp, res, *, ncg=4, mloop=3, mode=MODE_FP64, fused=True) -> None:
         """One sweep iteration as calc_sweep runs it (sweep_module.f90:150-155):
-        conjugate_gradient -> gram_schmidt -> subspace_diag; with fused=True
-        the last two run as one Rayleigh-Ritz step (orth_subspace_diag)."""
+        conjugate_gradient -> gram_schmidt -> subspace_diag.  fused=True runs it
+        as one eigensolver_sweep call (Gram-Schmidt and Rayleigh-Ritz as one
+        step); fused=False makes the three reference calls."""
         ml, mb = unk.shape
-        self.conjugate_gradient(1, ml, mb, 1, 1, unk, esp, res, ncg=ncg, mloop=mloop, mode=mode)
         if fused:
-            self.orth_subspace_diag(1, 1, unk, esp, mode=mode)
-        else:
-            self.gram_schmidt(1, mb, 1, 1, unk, mode=mode)
-            self.subspace_diag(1, 1, unk, esp, mode=mode)
+            self.eigensolver_sweep(1, 1, unk, esp, res, ncg=ncg, mloop=mloop, mode=mode)
+            return
+        self.conjugate_gradient(1, ml, mb, 1, 1, unk, esp, res, ncg=ncg, mloop=mloop, mode=mode)
+        self.gram_schmidt(1, mb, 1, 1, unk, mode=mode)
+        self.subspace_diag(1, 1, unk, esp, mode=mode)

@@ -602,6 +602,19 @@ static int cg_run(T* x, long ld, int mb, int spin, double* esp, double* res, int
     return RSDFT_OK;
 }
 
+int cg_device_f32(const double* unk, long ld, int mb, int spin, double* esp, double* res, int ncg, int mloop,
+                  int ipc, float** x32_out) {
+    Context& c = ctx();
+    float* x32 = nullptr;
+    const long n = ld * (long)mb;
+    RS_CHECK(workspace_t("cg_x32", (size_t)n, &x32));
+    launch(k_convert<float>, 4 * c.num_sms, 256, 0, c.stream, unk, x32, n);
+    RS_LAUNCH();
+    RS_CHECK(cg_run<float>(x32, ld, mb, spin, esp, res, ncg, mloop, ipc));
+    *x32_out = x32;
+    return RSDFT_OK;
+}
+
 int cg_device(double* unk, long ld, int mb, int spin, double* esp, double* res, int ncg, int mloop, int ipc,
               int mode) {
     if (mode == RSDFT_MODE_FP64) return cg_run<double>(unk, ld, mb, spin, esp, res, ncg, mloop, ipc);

@@ -36,6 +36,11 @@ __global__ void k_zero_lower(double* a, int n, int lda) {
     if (i < n && i > j) a[(long)j * lda + i] = 0.0;
 }
 
+__global__ void k_widen(const float* __restrict__ a, double* __restrict__ b, long n) {
+    for (long i = (long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long)gridDim.x * blockDim.x)
+        b[i] = (double)a[i];
+}
+
 // C = alpha * sum_c P[c] (sym: alpha/2 (G + G^T)), fixed summation order
 __global__ void k_reduce_partials(const double* __restrict__ P, int nch, int m, int n, double alpha, int sym,
                                   double* __restrict__ C) {
@@ -281,6 +286,59 @@ int orth_subspace_diag_device(double* psi, long ld, int mb, int spin, double* es
     return RSDFT_OK;
 }
 
+// The same step on the FP32 bands of a mixed CG sweep: FP32 H psi, BF16
+// split from FP32 (exact), rotated bands written in FP64 to psi.  An
+// ill-conditioned overlap converts x32 to psi and takes the explicit path.
+int orth_subspace_diag_f32(const float* x32, double* psi, long ld, int mb, int spin, double* esp, int mode) {
+    Context& c = ctx();
+    float* h32 = nullptr;
+    double *S = nullptr, *H = nullptr, *T = nullptr, *mm = nullptr;
+    int* dinfo = nullptr;
+    RS_CHECK(workspace_t("sub_h32", (size_t)ld * mb, &h32));
+    RS_CHECK(workspace_t("gs_S", (size_t)mb * mb, &S));
+    RS_CHECK(workspace_t("sub_H", (size_t)mb * mb, &H));
+    RS_CHECK(workspace_t("osd_T", (size_t)mb * mb, &T));
+    RS_CHECK(workspace_t("osd_minmax", 2, &mm));
+    RS_CHECK(workspace_t("gs_info", 4, &dinfo));
+    const double zero = 0.0, one = 1.0;
+    RS_CHECK(hpsi_device<float>(x32, h32, ld, mb, spin, nullptr));
+    RS_CHECK(gram_mixed_pair(x32, h32, ld, mb, c.dV, mode_terms(mode), S, H));
+    int lwork = 0;
+    RS_SOLVER(cusolverDnDpotrf_bufferSize(c.solver, CUBLAS_FILL_MODE_UPPER, mb, S, mb, &lwork));
+    double* work = nullptr;
+    RS_CHECK(workspace_t("gs_potrf", (size_t)lwork + 1, &work));
+    RS_SOLVER(cusolverDnDpotrf(c.solver, CUBLAS_FILL_MODE_UPPER, mb, S, mb, work, lwork, dinfo));
+    RS_CHECK(check_info(dinfo, "eigensolver_sweep: overlap Cholesky"));
+    launch(k_diag_minmax, 1, 256, 0, c.stream, S, mb, mb, mm);
+    RS_LAUNCH();
+    double hmm[2] = {0.0, 0.0};
+    RS_CUDA(cudaMemcpyAsync(hmm, mm, sizeof(hmm), cudaMemcpyDeviceToHost, c.stream));
+    RS_CUDA(cudaStreamSynchronize(c.stream));
+    if (!(hmm[0] > 0.0) || (hmm[1] / hmm[0]) * (hmm[1] / hmm[0]) > 1e2) {
+        launch(k_widen, 4 * c.num_sms, 256, 0, c.stream, x32, psi, ld * (long)mb);
+        RS_LAUNCH();
+        RS_CHECK(gram_schmidt_device(psi, ld, mb, mode));
+        return subspace_diag_device(psi, ld, mb, spin, esp, mode);
+    }
+    size_t dws = 0, hws = 0;
+    RS_SOLVER(cusolverDnXtrtri_bufferSize(c.solver, CUBLAS_FILL_MODE_UPPER, CUBLAS_DIAG_NON_UNIT, mb, CUDA_R_64F, S,
+                                          mb, &dws, &hws));
+    void* dw = nullptr;
+    RS_CHECK(workspace("gs_trtri", dws + 16, &dw));
+    static std::vector<char> hw;
+    if (hw.size() < hws + 16) hw.resize(hws + 16);
+    RS_SOLVER(cusolverDnXtrtri(c.solver, CUBLAS_FILL_MODE_UPPER, CUBLAS_DIAG_NON_UNIT, mb, CUDA_R_64F, S, mb, dw,
+                               dws, hw.data(), hws, dinfo));
+    RS_CHECK(check_info(dinfo, "eigensolver_sweep: triangular inverse"));
+    launch(k_zero_lower, dim3(div_up(mb, 128), mb), 128, 0, c.stream, S, mb, mb);
+    RS_LAUNCH();
+    RS_BLAS(cublasDgemm(c.blas, CUBLAS_OP_N, CUBLAS_OP_N, mb, mb, mb, &one, H, mb, S, mb, &zero, T, mb));
+    RS_BLAS(cublasDgemm(c.blas, CUBLAS_OP_T, CUBLAS_OP_N, mb, mb, mb, &one, S, mb, T, mb, &zero, H, mb));
+    RS_CHECK(syevd(H, mb, esp, CUBLAS_FILL_MODE_UPPER, "eigensolver_sweep: syevd"));
+    RS_BLAS(cublasDgemm(c.blas, CUBLAS_OP_N, CUBLAS_OP_N, mb, mb, mb, &one, S, mb, H, mb, &zero, T, mb));
+    return rotate_mixed(x32, psi, ld, mb, T, mb, mode_terms(mode));
+}
+
 }  // namespace rsdft
 
 using namespace rsdft;
@@ -390,6 +448,35 @@ int rsdft_gpu_subspace_rotv(int k, int s, double* unk, long ld, int mb, const do
                         (int)ld));
     RS_CUDA(cudaMemcpy2DAsync(d, ld * sizeof(double), tmp, ld * sizeof(double), c.ml * sizeof(double), mb,
                               cudaMemcpyDeviceToDevice, c.stream));
+    RS_CHECK(wf_release(unk, d, ld, mb, st));
+    return RSDFT_OK;
+}
+
+int rsdft_gpu_eigensolver_sweep(int k, int s, double* unk, long ld, int mb, double* esp, double* res, int ncg,
+                                int mloop, int ipc, int mode) {
+    RS_CHECK(require_grid());
+    RS_CHECK(check_k_s(k, s, "eigensolver_sweep"));
+    Context& c = ctx();
+    if (ld != c.ml || mb < 1 || mb > 65535 || !esp || !res || ncg < 0 || mloop < 0 || (ipc != 0 && ipc != 4) ||
+        mode < 0 || mode > 2) {
+        set_error("eigensolver_sweep: bad arguments");
+        return RSDFT_EINVAL;
+    }
+    double *d, *W, *R;
+    bool st;
+    RS_CHECK(wf_acquire(unk, ld, mb, "sweep_unk", &d, &st));
+    RS_CHECK(workspace_t("sweep_W", (size_t)mb, &W));
+    RS_CHECK(workspace_t("sweep_R", (size_t)mb, &R));
+    if (mode == RSDFT_MODE_FP64) {
+        RS_CHECK(cg_device(d, ld, mb, s, W, R, ncg, mloop, ipc, mode));
+        RS_CHECK(orth_subspace_diag_device(d, ld, mb, s, W, mode));
+    } else {
+        float* x32 = nullptr;
+        RS_CHECK(cg_device_f32(d, ld, mb, s, W, R, ncg, mloop, ipc, &x32));
+        RS_CHECK(orth_subspace_diag_f32(x32, d, ld, mb, s, W, mode));
+    }
+    RS_CHECK(stage_out(esp, W, sizeof(double) * mb));
+    RS_CHECK(stage_out(res, R, sizeof(double) * mb));
     RS_CHECK(wf_release(unk, d, ld, mb, st));
     return RSDFT_OK;
 }

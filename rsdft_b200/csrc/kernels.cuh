@@ -62,6 +62,15 @@ int subspace_diag_device(double* psi, long ld, int mb, int spin, double* esp_dev
 // Gram-Schmidt + Rayleigh-Ritz as one step (device data).
 int orth_subspace_diag_device(double* psi, long ld, int mb, int spin, double* esp_dev, int mode);
 
+// Mixed forms: the CG sweep on an FP32 copy of unk, left in the workspace
+// (*x32_out, leading dimension ld) for orth_subspace_diag_f32.
+int cg_device_f32(const double* unk, long ld, int mb, int spin, double* esp, double* res, int ncg, int mloop,
+                  int ipc, float** x32_out);
+
+// Gram-Schmidt + Rayleigh-Ritz of FP32 bands x32; the rotated bands are
+// written to psi (FP64).  Mixed forms only.
+int orth_subspace_diag_f32(const float* x32, double* psi, long ld, int mb, int spin, double* esp_dev, int mode);
+
 // CG over all bands (device data).
 int cg_device(double* unk, long ld, int mb, int spin, double* esp_dev, double* res_dev, int ncg, int mloop,
               int ipc, int mode);

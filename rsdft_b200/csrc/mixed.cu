@@ -29,6 +29,7 @@
 #include "common.cuh"
 #include "kernels.cuh"
 #include "mixed.cuh"
+#include "vec16.cuh"
 #include "tmap.cuh"
 #include "umma.cuh"
 
@@ -52,21 +53,24 @@ __device__ __forceinline__ void split_bf16(double x, __nv_bfloat16& h, __nv_bflo
 // band).  grid (ceil(ml / 2048), nb): 8 consecutive k per thread, read as
 // 16-byte pairs and written as one 16-byte group per slice when vec is set
 // (ml % 8 == 0, ld even, 16-byte aligned bases).
-__global__ void __launch_bounds__(256) k_split_cols(const double* __restrict__ psi, long ld, int nb, long ml,
+template <typename TI>
+__global__ void __launch_bounds__(256) k_split_cols(const TI* __restrict__ psi, long ld, int nb, long ml,
                                                     __nv_bfloat16* __restrict__ out, int vec) {
     const long n = ml * nb;
     const int b = blockIdx.y;
     const long k0 = ((long)blockIdx.x * blockDim.x + threadIdx.x) * 8;
     if (k0 >= ml) return;
-    const double* src = psi + (long)b * ld + k0;
+    const TI* src = psi + (long)b * ld + k0;
     __nv_bfloat16* o = out + (long)b * ml + k0;
     if (vec && k0 + 8 <= ml) {
         __nv_bfloat16 h[8], m[8], l[8];
+        constexpr int W = 16 / (int)sizeof(TI);  // elements per 16-byte load
 #pragma unroll
-        for (int q = 0; q < 4; ++q) {
-            const double2 v = *reinterpret_cast<const double2*>(src + 2 * q);
-            split_bf16(v.x, h[2 * q], m[2 * q], l[2 * q]);
-            split_bf16(v.y, h[2 * q + 1], m[2 * q + 1], l[2 * q + 1]);
+        for (int q = 0; q < 8 / W; ++q) {
+            TI v[W];
+            Vec16<TI>::get(*reinterpret_cast<const typename Vec16<TI>::t*>(src + W * q), v);
+#pragma unroll
+            for (int e = 0; e < W; ++e) split_bf16((double)v[e], h[W * q + e], m[W * q + e], l[W * q + e]);
         }
         *reinterpret_cast<uint4*>(o) = *reinterpret_cast<const uint4*>(h);
         *reinterpret_cast<uint4*>(o + n) = *reinterpret_cast<const uint4*>(m);
@@ -75,7 +79,7 @@ __global__ void __launch_bounds__(256) k_split_cols(const double* __restrict__ p
     }
     for (long k = 0; k < 8 && k0 + k < ml; ++k) {
         __nv_bfloat16 h, m, l;
-        split_bf16(src[k], h, m, l);
+        split_bf16((double)src[k], h, m, l);
         o[k] = h;
         o[n + k] = m;
         o[2 * n + k] = l;
@@ -84,7 +88,8 @@ __global__ void __launch_bounds__(256) k_split_cols(const double* __restrict__ p
 
 // slices[s][i][m] = term s of psi(i, m), m fastest, padded to mbk (zeros):
 // the transpose that makes the band index the K dimension of a rotation
-__global__ void k_split_rows(const double* __restrict__ psi, long ld, int nb, long ml, int mbk,
+template <typename TI>
+__global__ void k_split_rows(const TI* __restrict__ psi, long ld, int nb, long ml, int mbk,
                              __nv_bfloat16* __restrict__ out) {
     __shared__ double tile[32][33];
     const long i0 = (long)blockIdx.x * 32;
@@ -93,7 +98,7 @@ __global__ void k_split_rows(const double* __restrict__ psi, long ld, int nb, lo
     for (int r = ty; r < 32; r += 8) {
         const long i = i0 + tx;
         const int m = m0 + r;
-        tile[r][tx] = (i < ml && m < nb) ? psi[(long)m * ld + i] : 0.0;
+        tile[r][tx] = (i < ml && m < nb) ? (double)psi[(long)m * ld + i] : 0.0;
     }
     __syncthreads();
     const long n = ml * mbk;
@@ -425,8 +430,9 @@ static int gram_from_slices(__nv_bfloat16* sa, __nv_bfloat16* sb, bool same, int
     return RSDFT_OK;
 }
 
-// BF16 slices of a tall FP64 block into the named workspace
-static int split_cols(const double* A, long ld, int nb, const char* ws, __nv_bfloat16** out) {
+// BF16 slices of a tall FP64 / FP32 block into the named workspace
+template <typename TI>
+static int split_cols(const TI* A, long ld, int nb, const char* ws, __nv_bfloat16** out) {
     Context& c = ctx();
     const long ml = c.ml;
     if (ml % 8 != 0) {
@@ -434,8 +440,8 @@ static int split_cols(const double* A, long ld, int nb, const char* ws, __nv_bfl
         return RSDFT_EUNSUP;
     }
     RS_CHECK(workspace_t(ws, 3 * (size_t)ml * nb, out));
-    const int vec = (ld % 2 == 0 && reinterpret_cast<uintptr_t>(A) % 16 == 0) ? 1 : 0;
-    launch(k_split_cols, dim3(div_up(ml, 2048), nb), 256, 0, c.stream, A, ld, nb, ml, *out, vec);
+    const int vec = ((ld * (long)sizeof(TI)) % 16 == 0 && reinterpret_cast<uintptr_t>(A) % 16 == 0) ? 1 : 0;
+    launch(k_split_cols<TI>, dim3(div_up(ml, 2048), nb), 256, 0, c.stream, A, ld, nb, ml, *out, vec);
     RS_LAUNCH();
     return RSDFT_OK;
 }
@@ -452,8 +458,8 @@ int gram_mixed(const double* A, const double* B, long ld, int nb, double alpha, 
     return gram_from_slices(sa, sb, same, nb, alpha, symmetrize, nterms, C);
 }
 
-int gram_mixed_pair(const double* psi, const double* hpsi, long ld, int nb, double alpha, int nterms, double* S,
-                    double* H) {
+template <typename TI>
+static int gram_pair(const TI* psi, const TI* hpsi, long ld, int nb, double alpha, int nterms, double* S, double* H) {
     __nv_bfloat16 *sa = nullptr, *sb = nullptr;
     RS_CHECK(split_cols(psi, ld, nb, "umma_sa", &sa));
     RS_CHECK(split_cols(hpsi, ld, nb, "umma_sb", &sb));
@@ -461,15 +467,26 @@ int gram_mixed_pair(const double* psi, const double* hpsi, long ld, int nb, doub
     return gram_from_slices(sa, sb, false, nb, alpha, 1, nterms, H);
 }
 
+int gram_mixed_pair(const double* psi, const double* hpsi, long ld, int nb, double alpha, int nterms, double* S,
+                    double* H) {
+    return gram_pair<double>(psi, hpsi, ld, nb, alpha, nterms, S, H);
+}
+
+int gram_mixed_pair(const float* psi, const float* hpsi, long ld, int nb, double alpha, int nterms, double* S,
+                    double* H) {
+    return gram_pair<float>(psi, hpsi, ld, nb, alpha, nterms, S, H);
+}
+
 // out (ML x nb, leading dimension ldo) = psi V, V (nb x nb, leading dimension ldv)
-int rotate_mixed(const double* psi, double* out, long ld, int nb, const double* V, int ldv, int nterms) {
+template <typename TI>
+static int rotate(const TI* psi, double* out, long ld, int nb, const double* V, int ldv, int nterms) {
     Context& c = ctx();
     const long ml = c.ml;
     const int mbk = (nb + 7) / 8 * 8;
     __nv_bfloat16 *st = nullptr, *sv = nullptr;
     RS_CHECK(workspace_t("umma_st", 3 * (size_t)ml * mbk, &st));
     RS_CHECK(workspace_t("umma_sv", 3 * (size_t)nb * mbk, &sv));
-    launch(k_split_rows, dim3(div_up(ml, 32), div_up(mbk, 32)), dim3(32, 8), 0, c.stream, psi, ld, nb, ml, mbk, st);
+    launch(k_split_rows<TI>, dim3(div_up(ml, 32), div_up(mbk, 32)), dim3(32, 8), 0, c.stream, psi, ld, nb, ml, mbk, st);
     launch(k_split_small, div_up((long)nb * mbk, 256), 256, 0, c.stream, V, nb, ldv, mbk, sv);
     RS_LAUNCH();
     UmmaMaps maps;
@@ -489,6 +506,14 @@ int rotate_mixed(const double* psi, double* out, long ld, int nb, const double* 
     else
         RS_CHECK((launch_umma<256, 2, 3, false>(maps, g, dim3(g.ntm, g.ntn))));
     return RSDFT_OK;
+}
+
+int rotate_mixed(const double* psi, double* out, long ld, int nb, const double* V, int ldv, int nterms) {
+    return rotate<double>(psi, out, ld, nb, V, ldv, nterms);
+}
+
+int rotate_mixed(const float* psi, double* out, long ld, int nb, const double* V, int ldv, int nterms) {
+    return rotate<float>(psi, out, ld, nb, V, ldv, nterms);
 }
 
 }  // namespace rsdft

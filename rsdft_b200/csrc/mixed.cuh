@@ -15,11 +15,16 @@ int gram_mixed(const double* A, const double* B, long ld, int nb, double alpha, 
 // split of each operand.
 int gram_mixed_pair(const double* psi, const double* hpsi, long ld, int nb, double alpha, int nterms, double* S,
                     double* H);
+// the same from FP32 blocks (the split of an FP32 value is exact)
+int gram_mixed_pair(const float* psi, const float* hpsi, long ld, int nb, double alpha, int nterms, double* S,
+                    double* H);
 
 // out (ML x nb, leading dimension ld) = psi V with V (nb x nb, leading
 // dimension ldv).  psi is read only into its BF16 split before the product,
 // so out may be psi itself.
 int rotate_mixed(const double* psi, double* out, long ld, int nb, const double* V, int ldv, int nterms);
+// the same with an FP32 psi (FP64 out)
+int rotate_mixed(const float* psi, double* out, long ld, int nb, const double* V, int ldv, int nterms);
 
 inline int mode_terms(int mode) { return mode == RSDFT_MODE_MIXED_BF16 ? 3 : 2; }
 

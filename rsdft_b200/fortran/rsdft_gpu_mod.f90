@@ -105,6 +105,13 @@ MODULE rsdft_gpu_mod
        type(c_ptr), value :: unk, esp
        integer(c_long), value :: ld
      end function rsdft_gpu_orth_subspace_diag
+     integer(c_int) function rsdft_gpu_eigensolver_sweep(k, s, unk, ld, mb, esp, res, ncg, mloop, ipc, mode) &
+          bind(C, name="rsdft_gpu_eigensolver_sweep")
+       import :: c_int, c_long, c_ptr
+       integer(c_int), value :: k, s, mb, ncg, mloop, ipc, mode
+       type(c_ptr), value :: unk, esp, res
+       integer(c_long), value :: ld
+     end function rsdft_gpu_eigensolver_sweep
      integer(c_int) function rsdft_gpu_subspace_mate(k, s, unk, ld, mb, hsub, ldh) &
           bind(C, name="rsdft_gpu_subspace_mate")
        import :: c_int, c_long, c_ptr
@@ -275,6 +282,15 @@ CONTAINS
     call check(rsdft_gpu_orth_subspace_diag(k, s, c_loc(unk), int(size(unk, 1), c_long), &
                int(size(unk, 2), c_int), c_loc(esp), mode), "orth_subspace_diag")
   END SUBROUTINE gpu_orth_subspace_diag
+
+  ! one calc_sweep iteration for (k, s) (sweep_module.f90:150-155)
+  SUBROUTINE gpu_eigensolver_sweep(k, s, unk, esp, res, ncg, mloop, ipc, mode)
+    integer, intent(IN) :: k, s, ncg, mloop, ipc, mode
+    real(8), intent(INOUT), target :: unk(:, :)
+    real(8), intent(OUT), target :: esp(:), res(:)
+    call check(rsdft_gpu_eigensolver_sweep(k, s, c_loc(unk), int(size(unk, 1), c_long), &
+               int(size(unk, 2), c_int), c_loc(esp), c_loc(res), ncg, mloop, ipc, mode), "eigensolver_sweep")
+  END SUBROUTINE gpu_eigensolver_sweep
 
   SUBROUTINE gpu_subspace_mate_sl(k, s, unk, hsub)
     integer, intent(IN) :: k, s

@@ -64,6 +64,25 @@ def test_mixed_orth_subspace_diag(gpu, cells, mode, tol):
     assert np.abs(g.T @ g * c.dV - np.eye(nb)).max() <= 10 * tol
 
 
+def test_mixed_sweep_matches_separate_calls(gpu, cells):
+    """The one-call sweep (FP32 bands handed to Rayleigh-Ritz) tracks CG +
+    orth_subspace_diag made as separate calls."""
+    c, o = prepare(gpu, cells, "si64")
+    nb = 160
+    q = o.gram_schmidt_t(np.asfortranarray(c.psi0()[:, :nb]))
+    ua, ub = dev(q), dev(q)
+    ea = torch.zeros(nb, dtype=torch.float64, device="cuda")
+    eb, ra, rb = torch.zeros_like(ea), torch.zeros_like(ea), torch.zeros_like(ea)
+    gpu.conjugate_gradient(1, c.ML, nb, 1, 1, ua, ea, ra, ncg=4, mloop=3, mode=api.MODE_MIXED_BF16)
+    gpu.orth_subspace_diag(1, 1, ua, ea, mode=api.MODE_MIXED_BF16)
+    gpu.eigensolver_sweep(1, 1, ub, eb, rb, ncg=4, mloop=3, mode=api.MODE_MIXED_BF16)
+    torch.cuda.synchronize()
+    assert np.abs(host(ea) - host(eb)).max() <= 3e-6 * max(1.0, np.abs(host(ea)).max())
+    assert np.abs(host(ra) - host(rb)).max() <= 1e-12 * max(1.0, np.abs(host(ra)).max())
+    g = host(ub)
+    assert np.abs(g.T @ g * c.dV - np.eye(nb)).max() <= 3e-5
+
+
 def test_mixed_cg_sweep_fp32(gpu, cells):
     c, o = prepare(gpu, cells, "si8")
     q = o.gram_schmidt_t(c.psi0())

@@ -218,6 +218,21 @@ def test_orth_subspace_diag_ill_conditioned_overlap(gpu, cells):
     assert np.abs(g.T @ g * c.dV - np.eye(nb)).max() <= 1e-12
 
 
+def test_sweep_fp64_equals_separate_calls(gpu, cells):
+    """eigensolver_sweep (FP64) runs exactly CG then orth_subspace_diag."""
+    c, o = prepare(gpu, cells, "si8")
+    q = o.gram_schmidt_t(c.psi0())
+    ua, ub = dev(q), dev(q)
+    ea = torch.zeros(c.nband, dtype=torch.float64, device="cuda")
+    eb, ra, rb = torch.zeros_like(ea), torch.zeros_like(ea), torch.zeros_like(ea)
+    gpu.conjugate_gradient(1, c.ML, c.nband, 1, 1, ua, ea, ra, ncg=4, mloop=3)
+    gpu.orth_subspace_diag(1, 1, ua, ea)
+    gpu.eigensolver_sweep(1, 1, ub, eb, rb, ncg=4, mloop=3)
+    torch.cuda.synchronize()
+    assert np.array_equal(host(ea), host(eb)) and np.array_equal(host(ra), host(rb))
+    assert np.array_equal(host(ua), host(ub))
+
+
 def test_eigensolver_iteration_sequence(gpu, cells):
     """CG -> GS -> subspace, two iterations, as calc_sweep calls them."""
     c, o = prepare(gpu, cells, "si8")
