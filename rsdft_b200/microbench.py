@@ -8,8 +8,12 @@
 ``python -m rsdft_b200.microbench iteration --workload si216 --mode fp64``
     eigensolver iterations (CG -> Gram-Schmidt -> subspace) from the seeded
     start, ``--warmup`` untimed and ``--steps`` timed.
+``python -m rsdft_b200.microbench large --workload si512``
+    the large-cell run: FP64 and mixed iterations from one start (each timed),
+    the FP64 closing pass, one adjoint force evaluation per form, eigenvalue
+    and force differences between the forms, hpsi bandwidth on all bands.
 
-Both run on cuda:0 with the library on a dedicated torch stream; timings are
+All run on cuda:0 with the library on a dedicated torch stream; timings are
 CUDA events on that stream.
 """
 from __future__ import annotations
@@ -87,6 +91,54 @@ def run_iteration(args) -> dict:
     return {"what": "iteration", "workload": args.workload, "mode": args.mode, "ms_per_iter": ms}
 
 
+def run_large(args) -> dict:
+    """The large-cell workload: from the same start, ``--steps`` FP64 and mixed
+    iterations (each timed), the FP64 closing pass on the mixed bands, then
+    one adjoint force evaluation per form; eigenvalue and force differences
+    mixed vs FP64, hpsi bandwidth on all bands."""
+    torch, api, g, cell, st, psi = _setup(args.workload)
+    MB, ML = cell.nband, cell.ML
+    start = psi.t().contiguous().t()
+    g.gram_schmidt(1, MB, 1, 1, start)
+    occ = np.zeros(MB)
+    occ[: cell.nocc] = 2.0
+    out = {"what": "large", "workload": args.workload, "grid": list(cell.ngrid), "bands": MB, "steps": args.steps}
+    res = {}
+    for name, mode in (("fp64", 0), ("mixed-bf16", 1)):
+        u = start.t().contiguous().t()
+        esp = torch.zeros(MB, dtype=torch.float64, device="cuda")
+        r = torch.zeros_like(esp)
+        times = []
+        for _ in range(args.steps):
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(st)
+            g.eigensolver_iteration(u, esp, r, ncg=args.ncg, mloop=args.mloop, mode=mode)
+            e1.record(st)
+            torch.cuda.synchronize()
+            times.append(e0.elapsed_time(e1))
+        if mode != 0:
+            g.finalize_fp64(u, esp, r)
+        dv = torch.zeros(ML, dtype=torch.float64, device="cuda")
+        dr = torch.zeros(3 * cell.natom, dtype=torch.float64, device="cuda")
+        f0, f1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        f0.record(st)
+        g.hpsi_adjoint(u, occ=occ, dl_dv=dv, dl_dr=dr)
+        f1.record(st)
+        torch.cuda.synchronize()
+        res[name] = (esp.cpu().numpy(), dr.cpu().numpy())
+        out[name] = {"ms_per_iter": times, "ms_per_iter_last": times[-1],
+                     "adjoint_force_ms": f0.elapsed_time(f1)}
+        del u
+    occn = cell.nocc
+    out["eig_err_max_occupied_ha"] = float(np.abs(res["fp64"][0][:occn] - res["mixed-bf16"][0][:occn]).max())
+    out["force_err_max_ha_bohr"] = float(np.abs(res["fp64"][1] - res["mixed-bf16"][1]).max())
+    h = api.fortran_empty(ML, MB)
+    ms = _timed(torch, st, lambda: g.hamiltonian(1, 1, start, h, 1, ML, 1, MB), 2, 5)
+    nbytes = MB * ML * 16 + ML * 8 + int(cell.lma_ptr[-1]) * 12
+    out["hpsi"] = {"ms": ms, "gbs": nbytes / (ms * 1e-3) / 1e9}
+    return out
+
+
 def main(argv=None) -> None:
     p = argparse.ArgumentParser(description=__doc__, formatter_class=argparse.RawDescriptionHelpFormatter)
     sub = p.add_subparsers(dest="what", required=True)
@@ -103,8 +155,13 @@ def main(argv=None) -> None:
     it.add_argument("--mloop", type=int, default=3)
     it.add_argument("--warmup", type=int, default=3)
     it.add_argument("--steps", type=int, default=2)
+    lg = sub.add_parser("large")
+    lg.add_argument("--workload", default="si512")
+    lg.add_argument("--ncg", type=int, default=4)
+    lg.add_argument("--mloop", type=int, default=3)
+    lg.add_argument("--steps", type=int, default=5)
     args = p.parse_args(argv)
-    out = run_hpsi(args) if args.what == "hpsi" else run_iteration(args)
+    out = {"hpsi": run_hpsi, "iteration": run_iteration, "large": run_large}[args.what](args)
     print(json.dumps(out), flush=True)
 
 

@@ -1,0 +1,158 @@
+"""Differentiation workload: 64-atom Si cell (48^3 grid), 160 bands, atoms
+displaced by N(0, 0.05 bohr), f_n = 2 for the lowest 128 bands.
+
+E = sum_n f_n <psi_n|H|psi_n> dV on converged bands.  The hand-written
+adjoint of hpsi (rsdft_gpu_hpsi_adjoint) gives dE/dV(r) and dE/dR_a; both are
+checked against central finite differences of E (h = 1e-5 Ha on 16 seeded
+grid points, h = 1e-4 bohr on 8 seeded atoms) with the sphere supports held
+fixed, against the nonlocal force routine (F = -dE/dR), and, for one atom
+component, against the finite difference of the re-converged energy (the
+Hellmann-Feynman statement the force relies on).  Bands converged with the
+mixed-precision iterations and the FP64 closing pass give the same forces.
+"""
+import numpy as np
+import pytest
+import torch
+
+from rsdft_b200 import _lib, api
+from rsdft_b200.cell import projector_values
+
+from test_gpu_parity import dev, host, prepare
+
+pytestmark = pytest.mark.gpu
+
+NOCC = 128
+ITERS = 40
+FD_TOL = 1e-5  # Ha/bohr and Ha/Ha, the target for adjoint vs finite differences
+
+
+def converge(gpu, c, o, mode, iters=ITERS, start=None):
+    if start is None:
+        start = o.gram_schmidt_t(np.asfortranarray(c.psi0()))
+    u = dev(start)
+    esp = torch.zeros(c.nband, dtype=torch.float64, device="cuda")
+    res = torch.zeros_like(esp)
+    for _ in range(iters):
+        gpu.eigensolver_iteration(u, esp, res, ncg=4, mloop=3, mode=mode)
+    if mode != api.MODE_FP64:
+        gpu.finalize_fp64(u, esp, res)
+    else:
+        gpu.residual(1, 1, u, esp, res)
+    torch.cuda.synchronize()
+    return u, host(esp), host(res)
+
+
+def energy(gpu, c, u, occ):
+    e = torch.zeros(c.nband, dtype=torch.float64, device="cuda")
+    gpu.esp_calc(1, 1, u, 1, c.ML, 1, c.nband, e)
+    torch.cuda.synchronize()
+    return float(np.dot(occ, host(e)))
+
+
+def set_vloc(c, v):
+    v = np.ascontiguousarray(v, dtype=np.float64)
+    _lib.call("rsdft_gpu_set_vloc", v.ctypes.data, c.ML, 1)
+
+
+@pytest.fixture(scope="module")
+def converged(gpu, cells):
+    c, o = prepare(gpu, cells, "si64_adjoint")
+    u64, e64, r64 = converge(gpu, c, o, api.MODE_FP64)
+    umx, emx, rmx = converge(gpu, c, o, api.MODE_MIXED_BF16)
+    return c, o, (u64, e64, r64), (umx, emx, rmx)
+
+
+def adjoint(gpu, c, u, occ):
+    dv = torch.zeros(c.ML, dtype=torch.float64, device="cuda")
+    dr = torch.zeros(3 * c.natom, dtype=torch.float64, device="cuda")
+    gpu.hpsi_adjoint(u, occ=occ, dl_dv=dv, dl_dr=dr)
+    torch.cuda.synchronize()
+    return host(dv), host(dr).reshape(c.natom, 3)
+
+
+def occupations(c):
+    occ = np.zeros(c.nband)
+    occ[:NOCC] = 2.0
+    return occ
+
+
+@pytest.mark.parametrize("which", ["fp64", "mixed"])
+def test_adjoint_vs_finite_differences(gpu, converged, which):
+    c, o, r64, rmx = converged
+    u, e, res = r64 if which == "fp64" else rmx
+    assert res[:NOCC].max() <= 1e-6  # converged occupied bands
+    gpu.setup(c)
+    occ = occupations(c)
+    dv, dr = adjoint(gpu, c, u, occ)
+    rng = np.random.default_rng(404)
+    # local potential, 16 seeded grid points
+    v0 = np.array(c.vloc, copy=True)
+    h = 1e-5
+    for i in rng.choice(c.ML, 16, replace=False):
+        E = []
+        for s in (1, -1):
+            v = v0.copy()
+            v[i] += s * h
+            set_vloc(c, v)
+            E.append(energy(gpu, c, u, occ))
+        fd = (E[0] - E[1]) / (2 * h)
+        assert abs(dv[i] - fd) <= FD_TOL * max(1.0, abs(fd)), (i, dv[i], fd)
+    set_vloc(c, v0)
+    # atomic positions, 8 seeded atoms (fixed sphere supports)
+    uv0 = c.uv.copy()
+    h = 1e-4
+    try:
+        for ia in rng.choice(c.natom, 8, replace=False):
+            k = int(rng.integers(3))
+            E = []
+            for s in (1, -1):
+                at = c.atoms.copy()
+                at[ia, k] += s * h
+                c.uv[:] = projector_values(c, at)
+                gpu.setup(c)
+                E.append(energy(gpu, c, u, occ))
+            fd = (E[0] - E[1]) / (2 * h)
+            assert abs(dr[ia, k] - fd) <= FD_TOL, (ia, k, dr[ia, k], fd)
+    finally:
+        c.uv[:] = uv0
+        gpu.setup(c)
+    # the nonlocal force routine is the same contraction: F = -dE/dR
+    f = np.zeros((3, c.natom), order="F")
+    gpu.calc_force_ps_nloc2(c.natom, f, u, occ)
+    assert np.abs(f.T + dr).max() <= 1e-12 * max(1.0, np.abs(dr).max())
+
+
+def test_mixed_converged_forces_match_fp64(gpu, converged):
+    c, o, r64, rmx = converged
+    gpu.setup(c)
+    occ = occupations(c)
+    _, d64 = adjoint(gpu, c, r64[0], occ)
+    _, dmx = adjoint(gpu, c, rmx[0], occ)
+    assert np.abs(r64[1][:NOCC] - rmx[1][:NOCC]).max() <= 1e-6  # eigenvalues, Ha
+    assert np.abs(d64 - dmx).max() <= FD_TOL  # forces, Ha/bohr
+
+
+def test_hellmann_feynman_reconverged(gpu, converged):
+    """dE/dR of the re-converged energy equals the adjoint at fixed bands."""
+    c, o, r64, _ = converged
+    gpu.setup(c)
+    occ = occupations(c)
+    u0 = r64[0]
+    _, dr = adjoint(gpu, c, u0, occ)
+    ia, k, h = 5, 1, 1e-4
+    uv0 = c.uv.copy()
+    start = host(u0)
+    E = []
+    try:
+        for s in (1, -1):
+            at = c.atoms.copy()
+            at[ia, k] += s * h
+            c.uv[:] = projector_values(c, at)
+            gpu.setup(c)
+            u, e, res = converge(gpu, c, o, api.MODE_FP64, iters=12, start=start)
+            E.append(float(np.dot(occ, e)))
+    finally:
+        c.uv[:] = uv0
+        gpu.setup(c)
+    fd = (E[0] - E[1]) / (2 * h)
+    assert abs(dr[ia, k] - fd) <= FD_TOL, (dr[ia, k], fd)
