@@ -207,9 +207,9 @@ def hpsi_bytes(cell, nb):
 
 def main():
     args = parse()
-    rank = int(os.environ.get("RANK", "0"))
-    world = int(os.environ.get("WORLD_SIZE", "1"))
-    local = int(os.environ.get("LOCAL_RANK", "0"))
+    from rsdft_b200 import replicas
+
+    rank, world, local = replicas.rank_info()
     if args.impl == "reference":
         run_reference(args, rank, world)
         return
@@ -221,10 +221,7 @@ def main():
     from rsdft_b200.cell import build_cell
 
     torch.cuda.set_device(local)
-    if world > 1:
-        import datetime
-
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    pg = replicas.init(world, "nccl")
     stream = torch.cuda.Stream()
     torch.cuda.set_stream(stream)  # torch and the library share this stream
     g = api.RsdftGpu(local)
@@ -290,11 +287,8 @@ def main():
         if sampler:
             clocks = sampler.stop()
             launches = int(n1 - n0)
-        ms = e0.elapsed_time(e1) / args.steps
-        t = torch.tensor([ms], dtype=torch.float64, device="cuda")
-        if world > 1:
-            dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        results[mode] = {"ms": float(t.item()), "esp": esp.cpu().numpy().copy()}
+        ms = replicas.max_over_ranks(e0.elapsed_time(e1) / args.steps, pg, device="cuda")
+        results[mode] = {"ms": ms, "esp": esp.cpu().numpy().copy()}
 
     # ---- accuracy of the headline form against FP64 from the same start:
     # 10 iterations each, then the FP64 closing pass (CholeskyQR2 + Rayleigh
@@ -375,12 +369,9 @@ def main():
             g.eigensolver_iteration(hn, esp_h, res_h, ncg=args.ncg, mloop=args.mloop, mode=mode_e)
             g.sync_to_host(hn)
         barrier()
-        dt = (time.perf_counter() - t0) / args.steps
-        t = torch.tensor([dt], dtype=torch.float64, device="cuda")
-        if world > 1:
-            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        dt = replicas.max_over_ranks((time.perf_counter() - t0) / args.steps, pg, device="cuda")
         g.unregister_wf(hn)
-        e2e = {"value": world / float(t.item()), "unit": "iter/s", "h2d_bytes_per_step": ML * MB * 8,
+        e2e = {"value": replicas.whole_job_rate(1.0, world, dt), "unit": "iter/s", "h2d_bytes_per_step": ML * MB * 8,
                "d2h_bytes_per_step": ML * MB * 8 + 2 * MB * 8}
 
     cpu = None
@@ -391,7 +382,7 @@ def main():
         ms = results[head]["ms"]
         line = {
             "metric": "eigensolver iter/s (Si216 72^3, 480 bands, CG Ncg=4 + GS + subspace)",
-            "value": world * 1000.0 / ms,
+            "value": replicas.whole_job_rate(1000.0, world, ms),
             "unit": "iter/s",
             "n_gpus": world,
             "steps": args.steps,
