@@ -102,10 +102,11 @@ static int check_info(int* dinfo, const char* what) {
 static int cholqr_pass(const double* psi, double* out, long ld, int nb, double* S, int* dinfo, int mode) {
     Context& c = ctx();
     const double zero = 0.0, one = 1.0;
+    const void* split = nullptr;
     if (mode == RSDFT_MODE_FP64)
         RS_CHECK(gemm_tn_splitk(psi, psi, ld, nb, nb, c.dV, 0, S));
     else
-        RS_CHECK(gram_mixed(psi, psi, ld, nb, c.dV, 0, mode_terms(mode), S));
+        RS_CHECK(gram_mixed(psi, psi, ld, nb, c.dV, 0, mode_terms(mode), S, &split));
     int lwork = 0;
     RS_SOLVER(cusolverDnDpotrf_bufferSize(c.solver, CUBLAS_FILL_MODE_UPPER, nb, S, nb, &lwork));
     double* work = nullptr;
@@ -128,7 +129,7 @@ static int cholqr_pass(const double* psi, double* out, long ld, int nb, double* 
         RS_BLAS(cublasDgemm(c.blas, CUBLAS_OP_N, CUBLAS_OP_N, (int)c.ml, nb, nb, &one, psi, (int)ld, S, nb, &zero, out,
                             (int)ld));
     else
-        RS_CHECK(rotate_mixed(psi, out, ld, nb, S, nb, mode_terms(mode)));
+        RS_CHECK(rotate_mixed(psi, out, ld, nb, S, nb, mode_terms(mode), split));
     return RSDFT_OK;
 }
 
@@ -175,10 +176,11 @@ int subspace_diag_device(double* psi, long ld, int mb, int spin, double* esp, in
                             hpsi, (int)ld));
     } else {
         RS_CHECK(hpsi_device<double>(psi, hpsi, ld, mb, spin, nullptr));
-        RS_CHECK(gram_mixed(psi, hpsi, ld, mb, c.dV, 1, mode_terms(mode), H));
+        const void* split = nullptr;
+        RS_CHECK(gram_mixed(psi, hpsi, ld, mb, c.dV, 1, mode_terms(mode), H, &split));
         RS_CHECK(syevd(H, mb, esp, CUBLAS_FILL_MODE_UPPER, "subspace_diag: syevd"));
         // reads only the BF16 split of psi: written in place
-        RS_CHECK(rotate_mixed(psi, psi, ld, mb, H, mb, mode_terms(mode)));
+        RS_CHECK(rotate_mixed(psi, psi, ld, mb, H, mb, mode_terms(mode), split));
         return RSDFT_OK;
     }
     RS_CUDA(cudaMemcpy2DAsync(psi, ld * sizeof(double), hpsi, ld * sizeof(double), c.ml * sizeof(double), mb,
@@ -233,12 +235,13 @@ int orth_subspace_diag_device(double* psi, long ld, int mb, int spin, double* es
     RS_CHECK(workspace_t("osd_minmax", 2, &mm));
     RS_CHECK(workspace_t("gs_info", 4, &dinfo));
     const double zero = 0.0, one = 1.0;
+    const void* split = nullptr;
     RS_CHECK(hpsi_device<double>(psi, hpsi, ld, mb, spin, nullptr));
     if (mode == RSDFT_MODE_FP64) {
         RS_CHECK(gemm_tn_splitk(psi, psi, ld, mb, mb, c.dV, 0, S));
         RS_CHECK(gemm_tn_splitk(psi, hpsi, ld, mb, mb, c.dV, 1, H));
     } else {
-        RS_CHECK(gram_mixed_pair(psi, hpsi, ld, mb, c.dV, mode_terms(mode), S, H));
+        RS_CHECK(gram_mixed_pair(psi, hpsi, ld, mb, c.dV, mode_terms(mode), S, H, &split));
     }
     int lwork = 0;
     RS_SOLVER(cusolverDnDpotrf_bufferSize(c.solver, CUBLAS_FILL_MODE_UPPER, mb, S, mb, &lwork));
@@ -281,7 +284,7 @@ int orth_subspace_diag_device(double* psi, long ld, int mb, int spin, double* es
     } else {
         // the tensor-core rotation reads only the BF16 split of psi, so it
         // can write psi itself
-        RS_CHECK(rotate_mixed(psi, psi, ld, mb, T, mb, mode_terms(mode)));
+        RS_CHECK(rotate_mixed(psi, psi, ld, mb, T, mb, mode_terms(mode), split));
     }
     return RSDFT_OK;
 }
@@ -302,7 +305,8 @@ int orth_subspace_diag_f32(const float* x32, double* psi, long ld, int mb, int s
     RS_CHECK(workspace_t("gs_info", 4, &dinfo));
     const double zero = 0.0, one = 1.0;
     RS_CHECK(hpsi_device<float>(x32, h32, ld, mb, spin, nullptr));
-    RS_CHECK(gram_mixed_pair(x32, h32, ld, mb, c.dV, mode_terms(mode), S, H));
+    const void* split = nullptr;
+    RS_CHECK(gram_mixed_pair(x32, h32, ld, mb, c.dV, mode_terms(mode), S, H, &split));
     int lwork = 0;
     RS_SOLVER(cusolverDnDpotrf_bufferSize(c.solver, CUBLAS_FILL_MODE_UPPER, mb, S, mb, &lwork));
     double* work = nullptr;
@@ -336,7 +340,7 @@ int orth_subspace_diag_f32(const float* x32, double* psi, long ld, int mb, int s
     RS_BLAS(cublasDgemm(c.blas, CUBLAS_OP_T, CUBLAS_OP_N, mb, mb, mb, &one, S, mb, T, mb, &zero, H, mb));
     RS_CHECK(syevd(H, mb, esp, CUBLAS_FILL_MODE_UPPER, "eigensolver_sweep: syevd"));
     RS_BLAS(cublasDgemm(c.blas, CUBLAS_OP_N, CUBLAS_OP_N, mb, mb, mb, &one, S, mb, H, mb, &zero, T, mb));
-    return rotate_mixed(x32, psi, ld, mb, T, mb, mode_terms(mode));
+    return rotate_mixed(x32, psi, ld, mb, T, mb, mode_terms(mode), split);
 }
 
 }  // namespace rsdft

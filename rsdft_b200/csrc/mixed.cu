@@ -21,7 +21,9 @@
 //     (split-K) and writes an FP64 partial tile; k_reduce_tiles adds the
 //     partials in a fixed order.
 //   DIRECT (rotations psi V, K = MB): D(n, i) = sum_m V(m, n) psi(i, m) is
-//     written to out(i, n) in FP64.
+//     written to out(i, n) in FP64.  Persistent: one CTA per SM walks the
+//     output tiles; two TMEM accumulators let the epilogue of one tile run
+//     while the MMA chain of the next fills the other.
 #include <cuda_bf16.h>
 
 #include <algorithm>
@@ -162,18 +164,23 @@ __device__ __forceinline__ void pair_tiles(const UmmaArgs& g, int pair, int& tm,
     tm = r;
 }
 
-template <int BN, int NT, int NS, bool DRAIN>
+template <int BN, int NT, int NS, bool DRAIN, bool BMN>
 __global__ void __launch_bounds__(U_THREADS, 1) k_umma(const __grid_constant__ UmmaMaps maps, UmmaArgs g) {
     constexpr int ABYTES = UB_M * UB_K * 2;  // one A slice tile
     constexpr int BBYTES = BN * UB_K * 2;
     constexpr int STAGE = NT * (ABYTES + BBYTES);
-    // DRAIN: two accumulators per segment buffer, one for the hi x hi product
-    // and one for the smaller cross products, double-buffered (the FP32
-    // accumulation truncates; keeping the dominant term's chain short keeps
-    // that bias near 2^-24 x 2 U_SEG instead of x 6 x 2 U_SEG)
-    constexpr int NACC = DRAIN ? 4 : 1;
-    constexpr int TCOLS = NACC * BN;  // 512 (DRAIN, BN = 128) or 256 (DIRECT, BN = 256)
-    constexpr uint32_t IDESC = umma_idesc_bf16(UB_M, BN);
+    // Accumulators, double-buffered between the MMA chain and the epilogue.
+    // DRAIN: two per buffer, one for the hi x hi product and one for the
+    // smaller cross products (the FP32 accumulation truncates; keeping the
+    // dominant term's chain short keeps that bias near 2^-24 x 2 U_SEG
+    // instead of x 6 x 2 U_SEG).  DIRECT: one per buffer, so the epilogue of
+    // one output tile overlaps the MMA chain of the next.
+    constexpr int NACC = DRAIN ? 4 : 2;
+    constexpr int TCOLS = NACC * BN;  // 512 for BN = 128 (DRAIN) and BN = 256 (DIRECT)
+    static_assert(TCOLS <= 512, "tensor memory holds 512 columns");
+    constexpr uint32_t IDESC = umma_idesc_bf16(UB_M, BN, BMN);
+    // MN-major B (BMN): the tile is BN / 32 boxes of 32 N values x UB_K K rows
+    constexpr uint32_t B_LBO = 32 * UB_K * 2, B_SBO = 8 * 64;
     extern __shared__ __align__(1024) unsigned char smem[];
     uint64_t* full = reinterpret_cast<uint64_t*>(smem + (size_t)NS * STAGE);
     uint64_t* empty = full + NS;
@@ -182,19 +189,34 @@ __global__ void __launch_bounds__(U_THREADS, 1) k_umma(const __grid_constant__ U
     uint32_t* tslot = reinterpret_cast<uint32_t*>(acce + 2);
 
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    int tm, tn, kb0, kb1;
+    // Work units, each ending in one accumulator hand-off: DRAIN, the K
+    // segments of U_SEG blocks of this CTA's (tile, split); DIRECT, the output
+    // tiles blockIdx.x, blockIdx.x + gridDim.x, ... (tm fastest, so CTAs
+    // running together share B tiles in L2), each over all K blocks.
+    int tm0 = 0, tn0 = 0, kb0 = 0, kb1 = g.kblocks, nunits;
     if (DRAIN) {
-        pair_tiles(g, blockIdx.x, tm, tn);
+        pair_tiles(g, blockIdx.x, tm0, tn0);
         kb0 = blockIdx.y * g.kb_per_split;
         kb1 = min(kb0 + g.kb_per_split, g.kblocks);
+        nunits = (max(kb1 - kb0, 0) + U_SEG - 1) / U_SEG;
     } else {
-        tm = blockIdx.x;
-        tn = blockIdx.y;
-        kb0 = 0;
-        kb1 = g.kblocks;
+        const int ntiles = g.ntm * g.ntn;
+        nunits = blockIdx.x < ntiles ? (ntiles - 1 - (int)blockIdx.x) / (int)gridDim.x + 1 : 0;
     }
-    const int nkb = max(kb1 - kb0, 0);
-    const int nseg = DRAIN ? (nkb + U_SEG - 1) / U_SEG : 1;
+    auto unit = [&](int u, int& tm, int& tn, int& ka, int& kz) {
+        if (DRAIN) {
+            tm = tm0;
+            tn = tn0;
+            ka = kb0 + u * U_SEG;
+            kz = min(ka + U_SEG, kb1);
+        } else {
+            const int t = (int)blockIdx.x + u * (int)gridDim.x;
+            tm = t % g.ntm;
+            tn = t / g.ntm;
+            ka = 0;
+            kz = g.kblocks;
+        }
+    };
 
     if (threadIdx.x == 0) {
         for (int s = 0; s < NS; ++s) {
@@ -220,17 +242,28 @@ __global__ void __launch_bounds__(U_THREADS, 1) k_umma(const __grid_constant__ U
     if (warp == 0) {
         // ------------------------------------------------------ TMA producer
         if (lane == 0) {
-            for (int it = 0; it < nkb; ++it) {
-                const int s = it % NS;
-                if (it >= NS && !mbar_wait(&empty[s], ((it / NS) - 1) & 1)) ok = false;
-                unsigned char* st = smem + (size_t)s * STAGE;
-                mbar_arrive_expect_tx(&full[s], STAGE);
-                const int k = (kb0 + it) * UB_K;
+            int it = 0;
+            for (int u = 0; u < nunits && ok; ++u) {
+                int tm, tn, ka, kz;
+                unit(u, tm, tn, ka, kz);
+                for (int kb = ka; kb < kz; ++kb, ++it) {
+                    const int s = it % NS;
+                    if (it >= NS && !mbar_wait(&empty[s], ((it / NS) - 1) & 1)) {
+                        ok = false;
+                        break;
+                    }
+                    unsigned char* st = smem + (size_t)s * STAGE;
+                    mbar_arrive_expect_tx(&full[s], STAGE);
+                    const int k = kb * UB_K;
 #pragma unroll
-                for (int t = 0; t < NT; ++t) {
-                    // the maps are rank 4 ({K, rows, slice, 1}): 4-D loads, w = 0
-                    tma_load_4d(st + t * ABYTES, &maps.a, k, tm * UB_M, t, 0, &full[s]);
-                    tma_load_4d(st + NT * ABYTES + t * BBYTES, &maps.b, k, tn * BN, t, 0, &full[s]);
+                    for (int t = 0; t < NT; ++t) {
+                        // the maps are rank 4 ({K, rows, slice, 1}): 4-D loads, w = 0
+                        tma_load_4d(st + t * ABYTES, &maps.a, k, tm * UB_M, t, 0, &full[s]);
+                        if (BMN)  // map {32, K, N / 32, slice}
+                            tma_load_4d(st + NT * ABYTES + t * BBYTES, &maps.b, 0, k, tn * (BN / 32), t, &full[s]);
+                        else
+                            tma_load_4d(st + NT * ABYTES + t * BBYTES, &maps.b, k, tn * BN, t, 0, &full[s]);
+                    }
                 }
             }
         }
@@ -238,17 +271,24 @@ __global__ void __launch_bounds__(U_THREADS, 1) k_umma(const __grid_constant__ U
         // ------------------------------------------------------- MMA issuer
         if (lane == 0) {
             int it = 0;
-            for (int seg = 0; seg < nseg; ++seg) {
-                const int b = seg & 1;
-                if (DRAIN && seg >= 2 && !mbar_wait(&acce[b], ((seg >> 1) - 1) & 1)) ok = false;
+            for (int u = 0; u < nunits && ok; ++u) {
+                int tm, tn, ka, kz;
+                unit(u, tm, tn, ka, kz);
+                const int b = u & 1;
+                if (u >= 2 && !mbar_wait(&acce[b], ((u >> 1) - 1) & 1)) {
+                    ok = false;
+                    break;
+                }
                 tc_fence_after();
                 const uint32_t d = tbase + (uint32_t)((DRAIN ? 2 * b : b) * BN);
                 const uint32_t dx = DRAIN ? d + (uint32_t)BN : d;  // cross products
-                const int itend = DRAIN ? min(nkb, (seg + 1) * U_SEG) : nkb;
                 bool first = true, firstx = true;
-                for (; it < itend; ++it) {
+                for (int kb = ka; kb < kz; ++kb, ++it) {
                     const int s = it % NS;
-                    if (!mbar_wait(&full[s], (it / NS) & 1)) ok = false;
+                    if (!mbar_wait(&full[s], (it / NS) & 1)) {
+                        ok = false;
+                        break;
+                    }
                     tc_fence_after();
                     const uint32_t sa = smem_u32(smem + (size_t)s * STAGE);
                     const uint32_t sb = sa + NT * ABYTES;
@@ -259,7 +299,9 @@ __global__ void __launch_bounds__(U_THREADS, 1) k_umma(const __grid_constant__ U
 #pragma unroll
                         for (int kk = 0; kk < UB_K / 16; ++kk) {
                             const uint64_t ad = umma_desc_sw64(sa + ta * ABYTES + kk * 32);
-                            const uint64_t bd = umma_desc_sw64(sb + tb * BBYTES + kk * 32);
+                            const uint64_t bd =
+                                BMN ? umma_desc_mn_sw64(sb + tb * BBYTES + kk * 16 * 64, B_LBO, B_SBO)
+                                    : umma_desc_sw64(sb + tb * BBYTES + kk * 32);
                             if (DRAIN && p > 0) {
                                 umma_bf16(dx, ad, bd, IDESC, firstx ? 0u : 1u);
                                 firstx = false;
@@ -280,18 +322,26 @@ __global__ void __launch_bounds__(U_THREADS, 1) k_umma(const __grid_constant__ U
         const int h = (warp - 2) >> 2;          // column half
         const int row = 32 * q + lane;          // tile row (TMEM lane)
         constexpr int CW = BN / 2;              // columns per warp
+        double acc[DRAIN ? CW : 1];
         if (DRAIN) {
-            double acc[CW];
 #pragma unroll
             for (int c = 0; c < CW; ++c) acc[c] = 0.0;
-            for (int seg = 0; seg < nseg; ++seg) {
-                const int b = seg & 1;
-                if (!mbar_wait(&accf[b], (seg >> 1) & 1)) ok = false;
-                tc_fence_after();
+        }
+        for (int u = 0; u < nunits; ++u) {
+            int tm, tn, ka, kz;
+            unit(u, tm, tn, ka, kz);
+            const int b = u & 1;
+            if (!mbar_wait(&accf[b], (u >> 1) & 1)) {
+                ok = false;
+                break;
+            }
+            tc_fence_after();
+            const uint32_t tq = tbase + ((uint32_t)(32 * q) << 16);
+            if (DRAIN) {
 #pragma unroll
                 for (int c0 = 0; c0 < CW; c0 += 32) {
                     uint32_t r[32];
-                    const uint32_t ta = tbase + ((uint32_t)(32 * q) << 16) + (uint32_t)(2 * b * BN + h * CW + c0);
+                    const uint32_t ta = tq + (uint32_t)(2 * b * BN + h * CW + c0);
                     tmem_ld_x32(ta, r);  // hi x hi
                     tmem_ld_wait();
 #pragma unroll
@@ -301,39 +351,39 @@ __global__ void __launch_bounds__(U_THREADS, 1) k_umma(const __grid_constant__ U
 #pragma unroll
                     for (int j = 0; j < 32; ++j) acc[c0 + j] += (double)__uint_as_float(r[j]);
                 }
-                tc_fence_before();
-                __syncwarp();
-                if (lane == 0) mbar_arrive(&acce[b]);
-            }
-            double* P = g.partial + ((size_t)blockIdx.y * g.npairs + blockIdx.x) * (size_t)(BN * UB_M);
+            } else {
+                const int n = tm * UB_M + row;  // output column (A row)
 #pragma unroll
-            for (int c = 0; c < CW; ++c) P[(size_t)(h * CW + c) * UB_M + row] = acc[c];
-        } else {
-            if (!mbar_wait(&accf[0], 0)) ok = false;
-            tc_fence_after();
-            const int n = tm * UB_M + row;  // output column (A row)
+                for (int c0 = 0; c0 < CW; c0 += 32) {
+                    uint32_t r[32];
+                    tmem_ld_x32(tq + (uint32_t)(b * BN + h * CW + c0), r);
+                    tmem_ld_wait();
+                    if (n < g.mrows) {
+                        const int i0 = tn * BN + h * CW + c0;
+                        double* o = g.out + (size_t)n * g.ldo + i0;
+                        if (i0 + 32 <= g.nrows) {
 #pragma unroll
-            for (int c0 = 0; c0 < CW; c0 += 32) {
-                uint32_t r[32];
-                tmem_ld_x32(tbase + ((uint32_t)(32 * q) << 16) + (uint32_t)(h * CW + c0), r);
-                tmem_ld_wait();
-                if (n < g.mrows) {
-                    const int i0 = tn * BN + h * CW + c0;
-                    double* o = g.out + (size_t)n * g.ldo + i0;
-                    if (i0 + 32 <= g.nrows) {
-#pragma unroll
-                        for (int j = 0; j < 32; j += 2) {
-                            double2 v;
-                            v.x = (double)__uint_as_float(r[j]);
-                            v.y = (double)__uint_as_float(r[j + 1]);
-                            *reinterpret_cast<double2*>(o + j) = v;
+                            for (int j = 0; j < 32; j += 2) {
+                                double2 v;
+                                v.x = (double)__uint_as_float(r[j]);
+                                v.y = (double)__uint_as_float(r[j + 1]);
+                                *reinterpret_cast<double2*>(o + j) = v;
+                            }
+                        } else {
+                            for (int j = 0; j < 32; ++j)
+                                if (i0 + j < g.nrows) o[j] = (double)__uint_as_float(r[j]);
                         }
-                    } else {
-                        for (int j = 0; j < 32; ++j)
-                            if (i0 + j < g.nrows) o[j] = (double)__uint_as_float(r[j]);
                     }
                 }
             }
+            tc_fence_before();
+            __syncwarp();
+            if (lane == 0) mbar_arrive(&acce[b]);
+        }
+        if (DRAIN && ok) {
+            double* P = g.partial + ((size_t)blockIdx.y * g.npairs + blockIdx.x) * (size_t)(BN * UB_M);
+#pragma unroll
+            for (int c = 0; c < CW; ++c) P[(size_t)(h * CW + c) * UB_M + row] = acc[c];
         }
     }
     if (!ok) atomicExch(g.err, 2);
@@ -381,17 +431,17 @@ static int map3(CUtensorMap* mp, const __nv_bfloat16* base, long k, long rows, i
     return encode_tmap_4d_swz64(mp, base, dims, strides, box);
 }
 
-template <int BN, int NT, int NS, bool DRAIN>
+template <int BN, int NT, int NS, bool DRAIN, bool BMN = false>
 static int launch_umma(const UmmaMaps& maps, const UmmaArgs& g, dim3 grid) {
     constexpr int STAGE = NT * (UB_M * UB_K * 2 + BN * UB_K * 2);
     const size_t smem = (size_t)NS * STAGE + 256;
     static bool attr = false;
     if (!attr) {
-        RS_CUDA(cudaFuncSetAttribute(k_umma<BN, NT, NS, DRAIN>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+        RS_CUDA(cudaFuncSetAttribute(k_umma<BN, NT, NS, DRAIN, BMN>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                      (int)smem));
         attr = true;
     }
-    launch(k_umma<BN, NT, NS, DRAIN>, grid, U_THREADS, smem, ctx().stream, maps, g);
+    launch(k_umma<BN, NT, NS, DRAIN, BMN>, grid, U_THREADS, smem, ctx().stream, maps, g);
     RS_LAUNCH();
     return RSDFT_OK;
 }
@@ -447,7 +497,7 @@ static int split_cols(const TI* A, long ld, int nb, const char* ws, __nv_bfloat1
 }
 
 int gram_mixed(const double* A, const double* B, long ld, int nb, double alpha, int symmetrize, int nterms,
-               double* C) {
+               double* C, const void** a_split) {
     __nv_bfloat16 *sa = nullptr, *sb = nullptr;
     RS_CHECK(split_cols(A, ld, nb, "umma_sa", &sa));
     const bool same = (A == B);
@@ -455,43 +505,43 @@ int gram_mixed(const double* A, const double* B, long ld, int nb, double alpha, 
         sb = sa;
     else
         RS_CHECK(split_cols(B, ld, nb, "umma_sb", &sb));
+    if (a_split) *a_split = sa;
     return gram_from_slices(sa, sb, same, nb, alpha, symmetrize, nterms, C);
 }
 
 template <typename TI>
-static int gram_pair(const TI* psi, const TI* hpsi, long ld, int nb, double alpha, int nterms, double* S, double* H) {
+static int gram_pair(const TI* psi, const TI* hpsi, long ld, int nb, double alpha, int nterms, double* S, double* H,
+                     const void** psi_split) {
     __nv_bfloat16 *sa = nullptr, *sb = nullptr;
     RS_CHECK(split_cols(psi, ld, nb, "umma_sa", &sa));
     RS_CHECK(split_cols(hpsi, ld, nb, "umma_sb", &sb));
+    if (psi_split) *psi_split = sa;
     RS_CHECK(gram_from_slices(sa, sa, true, nb, alpha, 0, nterms, S));
     return gram_from_slices(sa, sb, false, nb, alpha, 1, nterms, H);
 }
 
 int gram_mixed_pair(const double* psi, const double* hpsi, long ld, int nb, double alpha, int nterms, double* S,
-                    double* H) {
-    return gram_pair<double>(psi, hpsi, ld, nb, alpha, nterms, S, H);
+                    double* H, const void** psi_split) {
+    return gram_pair<double>(psi, hpsi, ld, nb, alpha, nterms, S, H, psi_split);
 }
 
 int gram_mixed_pair(const float* psi, const float* hpsi, long ld, int nb, double alpha, int nterms, double* S,
-                    double* H) {
-    return gram_pair<float>(psi, hpsi, ld, nb, alpha, nterms, S, H);
+                    double* H, const void** psi_split) {
+    return gram_pair<float>(psi, hpsi, ld, nb, alpha, nterms, S, H, psi_split);
 }
 
-// out (ML x nb, leading dimension ldo) = psi V, V (nb x nb, leading dimension ldv)
-template <typename TI>
-static int rotate(const TI* psi, double* out, long ld, int nb, const double* V, int ldv, int nterms) {
+// The A operand of a rotation: slices[s][n][m] = term s of V(m, n), K = m
+// padded to mbk with zeros.
+static int split_v(const double* V, int nb, int ldv, int mbk, UmmaMaps* maps) {
     Context& c = ctx();
-    const long ml = c.ml;
-    const int mbk = (nb + 7) / 8 * 8;
-    __nv_bfloat16 *st = nullptr, *sv = nullptr;
-    RS_CHECK(workspace_t("umma_st", 3 * (size_t)ml * mbk, &st));
+    __nv_bfloat16* sv = nullptr;
     RS_CHECK(workspace_t("umma_sv", 3 * (size_t)nb * mbk, &sv));
-    launch(k_split_rows<TI>, dim3(div_up(ml, 32), div_up(mbk, 32)), dim3(32, 8), 0, c.stream, psi, ld, nb, ml, mbk, st);
     launch(k_split_small, div_up((long)nb * mbk, 256), 256, 0, c.stream, V, nb, ldv, mbk, sv);
     RS_LAUNCH();
-    UmmaMaps maps;
-    RS_CHECK(map3(&maps.a, sv, mbk, nb, UB_M));
-    RS_CHECK(map3(&maps.b, st, mbk, ml, 256));
+    return map3(&maps->a, sv, mbk, nb, UB_M);
+}
+
+static UmmaArgs rotate_args(long ml, int nb, int mbk, double* out, long ld) {
     UmmaArgs g{};
     g.kblocks = (mbk + UB_K - 1) / UB_K;
     g.ntm = (nb + UB_M - 1) / UB_M;
@@ -500,20 +550,68 @@ static int rotate(const TI* psi, double* out, long ld, int nb, const double* V, 
     g.ldo = ld;
     g.mrows = nb;
     g.nrows = (int)ml;
-    g.err = c.err_flag;
-    if (nterms == 3)
-        RS_CHECK((launch_umma<256, 3, 3, false>(maps, g, dim3(g.ntm, g.ntn))));
-    else
-        RS_CHECK((launch_umma<256, 2, 3, false>(maps, g, dim3(g.ntm, g.ntn))));
-    return RSDFT_OK;
+    g.err = ctx().err_flag;
+    return g;
 }
 
-int rotate_mixed(const double* psi, double* out, long ld, int nb, const double* V, int ldv, int nterms) {
-    return rotate<double>(psi, out, ld, nb, V, ldv, nterms);
+template <bool BMN>
+static int launch_rotate(const UmmaMaps& maps, const UmmaArgs& g, int nterms) {
+    Context& c = ctx();
+    const int sms = c.num_sms > 0 ? c.num_sms : 148;
+    const dim3 grid((unsigned)std::min(g.ntm * g.ntn, sms));
+    if (nterms == 3) return launch_umma<256, 3, 3, false, BMN>(maps, g, grid);
+    return launch_umma<256, 2, 3, false, BMN>(maps, g, grid);
 }
 
-int rotate_mixed(const float* psi, double* out, long ld, int nb, const double* V, int ldv, int nterms) {
-    return rotate<float>(psi, out, ld, nb, V, ldv, nterms);
+// B operand from the split of psi as the Gram product leaves it (slices
+// [s][band][grid], grid fastest), read MN-major: the map views the grid
+// index as (32, ML / 32) so that one box is BN / 32 groups of 32 grid values
+// x UB_K bands.  Returns RSDFT_EUNSUP when that view is not available.
+static int rotate_from_split(const __nv_bfloat16* sp, double* out, long ld, int nb, const double* V, int ldv,
+                             int nterms) {
+    Context& c = ctx();
+    const long ml = c.ml;
+    if (ml % 32 != 0) return RSDFT_EUNSUP;
+    UmmaMaps maps;
+    const unsigned long long dims[4] = {32ull, (unsigned long long)nb, (unsigned long long)(ml / 32), 3ull};
+    const unsigned long long strides[3] = {(unsigned long long)ml * 2, 64ull, (unsigned long long)ml * nb * 2};
+    const unsigned int box[4] = {32u, (unsigned)UB_K, 256u / 32u, 1u};
+    if (encode_tmap_4d_swz64(&maps.b, sp, dims, strides, box) != RSDFT_OK) return RSDFT_EUNSUP;
+    const int mbk = (nb + 7) / 8 * 8;
+    RS_CHECK(split_v(V, nb, ldv, mbk, &maps));
+    return launch_rotate<true>(maps, rotate_args(ml, nb, mbk, out, ld), nterms);
+}
+
+// out (ML x nb, leading dimension ldo) = psi V, V (nb x nb, leading dimension ldv)
+template <typename TI>
+static int rotate(const TI* psi, double* out, long ld, int nb, const double* V, int ldv, int nterms,
+                  const void* psi_split) {
+    if (psi_split) {
+        const int r = rotate_from_split(static_cast<const __nv_bfloat16*>(psi_split), out, ld, nb, V, ldv, nterms);
+        if (r != RSDFT_EUNSUP) return r;
+    }
+    // transposed split: slices[s][i][m], K = band index fastest
+    Context& c = ctx();
+    const long ml = c.ml;
+    const int mbk = (nb + 7) / 8 * 8;
+    __nv_bfloat16* st = nullptr;
+    RS_CHECK(workspace_t("umma_st", 3 * (size_t)ml * mbk, &st));
+    launch(k_split_rows<TI>, dim3(div_up(ml, 32), div_up(mbk, 32)), dim3(32, 8), 0, c.stream, psi, ld, nb, ml, mbk, st);
+    RS_LAUNCH();
+    UmmaMaps maps;
+    RS_CHECK(split_v(V, nb, ldv, mbk, &maps));
+    RS_CHECK(map3(&maps.b, st, mbk, ml, 256));
+    return launch_rotate<false>(maps, rotate_args(ml, nb, mbk, out, ld), nterms);
+}
+
+int rotate_mixed(const double* psi, double* out, long ld, int nb, const double* V, int ldv, int nterms,
+                 const void* psi_split) {
+    return rotate<double>(psi, out, ld, nb, V, ldv, nterms, psi_split);
+}
+
+int rotate_mixed(const float* psi, double* out, long ld, int nb, const double* V, int ldv, int nterms,
+                 const void* psi_split) {
+    return rotate<float>(psi, out, ld, nb, V, ldv, nterms, psi_split);
 }
 
 }  // namespace rsdft

@@ -1,10 +1,11 @@
 // tcgen05 (5th-generation tensor core) helpers for sm_100a, inline PTX.
 //
 // Conventions: cta_group::1, kind::f16 with BF16 operands and FP32
-// accumulation in tensor memory (TMEM), both operands K-major in shared
-// memory with the 64-byte swizzle (8 rows x 64 B atoms), which is the layout
-// a TMA tile load with CU_TENSOR_MAP_SWIZZLE_64B and a 32-element inner box
-// produces.
+// accumulation in tensor memory (TMEM), operands in shared memory with the
+// 64-byte swizzle (8 rows x 64 B atoms), which is the layout a TMA tile load
+// with CU_TENSOR_MAP_SWIZZLE_64B and a 32-element inner box produces: K-major
+// (rows along M/N, 32 K values per row) or, for B, MN-major (rows along K,
+// 32 N values per row).
 #pragma once
 
 #include <cstdint>
@@ -27,9 +28,24 @@ __device__ __forceinline__ uint64_t umma_desc_sw64(uint32_t smem_addr) {
     return d;
 }
 
-// Instruction descriptor, kind::f16: D = F32, A = B = BF16, both K-major.
-__host__ __device__ constexpr uint32_t umma_idesc_bf16(int M, int N) {
-    return (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(N >> 3) << 17) | ((uint32_t)(M >> 4) << 24);
+// MN-major operand with the 64-byte swizzle: 32-element (64 B) rows along MN,
+// 8 K rows per 512-byte atom; atoms repeat along K every sbo bytes and along
+// MN every lbo bytes.
+__device__ __forceinline__ uint64_t umma_desc_mn_sw64(uint32_t smem_addr, uint32_t lbo, uint32_t sbo) {
+    uint64_t d = 0;
+    d |= (uint64_t)((smem_addr & 0x3FFFFu) >> 4);
+    d |= (uint64_t)((lbo >> 4) & 0x3FFFu) << 16;
+    d |= (uint64_t)((sbo >> 4) & 0x3FFFu) << 32;
+    d |= (uint64_t)1 << 46;
+    d |= (uint64_t)4 << 61;
+    return d;
+}
+
+// Instruction descriptor, kind::f16: D = F32, A = B = BF16, A K-major, B
+// K-major (b_mn = false) or MN-major (b_mn = true, bit 16).
+__host__ __device__ constexpr uint32_t umma_idesc_bf16(int M, int N, bool b_mn = false) {
+    return (1u << 4) | (1u << 7) | (1u << 10) | ((b_mn ? 1u : 0u) << 16) | ((uint32_t)(N >> 3) << 17) |
+           ((uint32_t)(M >> 4) << 24);
 }
 
 // ------------------------------------------------------------------ TMEM

@@ -8,6 +8,10 @@
 ``python -m rsdft_b200.microbench iteration --workload si216 --mode fp64``
     eigensolver iterations (CG -> Gram-Schmidt -> subspace) from the seeded
     start, ``--warmup`` untimed and ``--steps`` timed.
+``python -m rsdft_b200.microbench rr --workload si216 --mode mixed-bf16``
+    the Gram-Schmidt + Rayleigh-Ritz step alone (``rsdft_gpu_orth_subspace_diag``)
+    on orthonormalised seeded bands; ``--ngrid`` / ``--bands`` shrink the cell
+    (same atoms, coarser grid) for small profiler captures.
 ``python -m rsdft_b200.microbench large --workload si512``
     the large-cell run: FP64 and mixed iterations from one start (each timed),
     the FP64 closing pass, one adjoint force evaluation per form, eigenvalue
@@ -32,17 +36,23 @@ if ROOT not in sys.path:
 MODES = {"fp64": 0, "mixed-bf16": 1, "mixed-bf16x3": 2}
 
 
-def _setup(workload: str):
+def _setup(workload: str, ngrid: int = 0, bands: int = 0):
+    import dataclasses
+
     import torch
 
     from rsdft_b200 import api
-    from rsdft_b200.cell import build_cell
+    from rsdft_b200.cell import WORKLOADS, build_cell
 
     st = torch.cuda.Stream()
     torch.cuda.set_stream(st)
     g = api.RsdftGpu(0)
     g.set_stream(st.cuda_stream)
-    cell = build_cell(workload)
+    w = WORKLOADS[workload]
+    if ngrid or bands:
+        w = dataclasses.replace(w, ngrid=ngrid or w.ngrid, nband=bands or w.nband,
+                                nocc=min(w.nocc, bands or w.nband))
+    cell = build_cell(w)
     g.setup(cell)
     psi = torch.from_numpy(np.ascontiguousarray(cell.psi0().T)).cuda().t()
     return torch, api, g, cell, st, psi
@@ -89,6 +99,18 @@ def run_iteration(args) -> dict:
     ms = _timed(torch, st, lambda: g.eigensolver_iteration(u, esp, res, ncg=args.ncg, mloop=args.mloop, mode=mode),
                 args.warmup, args.steps)
     return {"what": "iteration", "workload": args.workload, "mode": args.mode, "ms_per_iter": ms}
+
+
+def run_rr(args) -> dict:
+    torch, api, g, cell, st, psi = _setup(args.workload, args.ngrid, args.bands)
+    MB = cell.nband
+    u = psi.t().contiguous().t()
+    g.gram_schmidt(1, MB, 1, 1, u)
+    esp = torch.zeros(MB, dtype=torch.float64, device="cuda")
+    mode = MODES[args.mode]
+    ms = _timed(torch, st, lambda: g.orth_subspace_diag(1, 1, u, esp, mode=mode), args.warmup, args.reps)
+    return {"what": "rr", "workload": args.workload, "grid": list(cell.ngrid), "bands": MB, "mode": args.mode,
+            "ms": ms}
 
 
 def run_large(args) -> dict:
@@ -155,13 +177,20 @@ def main(argv=None) -> None:
     it.add_argument("--mloop", type=int, default=3)
     it.add_argument("--warmup", type=int, default=3)
     it.add_argument("--steps", type=int, default=2)
+    rr = sub.add_parser("rr")
+    rr.add_argument("--workload", default="si216")
+    rr.add_argument("--mode", default="mixed-bf16", choices=sorted(MODES))
+    rr.add_argument("--ngrid", type=int, default=0)
+    rr.add_argument("--bands", type=int, default=0)
+    rr.add_argument("--warmup", type=int, default=2)
+    rr.add_argument("--reps", type=int, default=5)
     lg = sub.add_parser("large")
     lg.add_argument("--workload", default="si512")
     lg.add_argument("--ncg", type=int, default=4)
     lg.add_argument("--mloop", type=int, default=3)
     lg.add_argument("--steps", type=int, default=5)
     args = p.parse_args(argv)
-    out = {"hpsi": run_hpsi, "iteration": run_iteration, "large": run_large}[args.what](args)
+    out = {"hpsi": run_hpsi, "iteration": run_iteration, "rr": run_rr, "large": run_large}[args.what](args)
     print(json.dumps(out), flush=True)
 
 
