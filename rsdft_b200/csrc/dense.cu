@@ -151,6 +151,8 @@ int gram_schmidt_device(double* psi, long ld, int nb, int mode) {
 // symmetric eigensolve in place: A (n x n, lda n) -> eigenvectors, W ascending
 static int syevd(double* A, int n, double* W, cublasFillMode_t uplo, const char* what) {
     Context& c = ctx();
+    const int r = syevd_fast(A, n, W, uplo);
+    if (r != RSDFT_EUNSUP) return r;
     int lwork = 0;
     RS_SOLVER(cusolverDnDsyevd_bufferSize(c.solver, CUSOLVER_EIG_MODE_VECTOR, uplo, n, A, n, W, &lwork));
     double* work = nullptr;

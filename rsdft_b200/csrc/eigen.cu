@@ -1,0 +1,654 @@
+// Symmetric eigensolver for the small dense matrices of the subspace steps
+// (the Rayleigh-Ritz matrix, n = number of bands, up to ~620): the same
+// result as LAPACK dsyevd / cuSOLVER syevd (eigenvalues ascending, an
+// orthonormal eigenvector basis), in three steps:
+//
+//  1. k_sytrd: Householder tridiagonalisation A = Q T Q^T (LAPACK dsytd2,
+//     lower form) by ONE thread-block cluster of 16 CTAs with the whole
+//     matrix resident in their shared memory: CTA c holds the full rows
+//     i = c, c + 16, ... .  Column j: every CTA holds the reflector v, forms
+//     p = tau A v on its own rows and its part of p^T v, pulls the rest of p
+//     and the look-ahead row j+1 over distributed shared memory, applies the
+//     rank-2 update A -= v w^T + w v^T (w = p - tau/2 (p^T v) v) to its own
+//     rows and to that row, and forms the next reflector itself.  One
+//     cluster barrier per column; nothing leaves the SMs until T and the
+//     reflectors are written.
+//  2. k_tri_bisect: eigenvalues of T by multisection on Sturm counts (one
+//     warp per eigenvalue, 32 trial points per round; LAPACK dstebz's count
+//     with its pivmin guard).  k_tri_invit: eigenvectors of T by inverse
+//     iteration with partial-pivoting LU of T - lambda I (LAPACK dstein:
+//     dgttrf/dgttrs steps, its start-vector scaling, convergence test and two
+//     extra iterations, perturbed shifts and modified Gram-Schmidt for
+//     eigenvalues closer than 1e-10 |T|_1), one thread per group.  A
+//     vector computed on its own is the exact eigenvector of T + F with
+//     |F| ~ eps |T|, so two vectors with eigenvalue gap g overlap by
+//     ~eps |T| / g; dstein removes that by Gram-Schmidt over chains of gaps
+//     below 1e-3 |T|, which turns the compressed spectra of unconverged
+//     Rayleigh-Ritz matrices into one serial chain.  Here the chains are
+//     cut at 1e-10 |T| (overlaps stay below ~1e-6) and two Newton-Schulz
+//     steps Z <- Z (3 I - Z^T Z) / 2 (four DGEMMs) make the basis orthonormal
+//     to rounding; they mix vectors i, j by ~eps |T| / |l_i - l_j|, which
+//     moves the residuals by ~eps |T| only.
+//  3. cusolverDnDormtr applies Q to the eigenvectors of T.
+//
+// cuSOLVER's one-stage syevd spends ~80 % of its time in sytrd for these
+// sizes (3.9 of 5.0 ms at n = 480 on B200), one short kernel per column;
+// here each column costs one cluster barrier.
+#include <cfloat>
+
+#include "common.cuh"
+#include "kernels.cuh"
+
+namespace rsdft {
+
+constexpr int TD_C = 16;          // CTAs in the cluster
+constexpr int TD_T = 512;         // threads per CTA
+constexpr int TD_W = TD_T / 32;
+
+__device__ __forceinline__ uint32_t cluster_rank() {
+    uint32_t r;
+    asm volatile("mov.u32 %0, %%cluster_ctarank;" : "=r"(r));
+    return r;
+}
+
+// all threads of all CTAs of the cluster; orders shared-memory writes before
+// the barrier against reads after it, cluster-wide
+__device__ __forceinline__ void cluster_sync() {
+    asm volatile(
+        "barrier.cluster.arrive.release.aligned;\n"
+        "barrier.cluster.wait.acquire.aligned;\n" ::
+            : "memory");
+}
+
+// load of the double at the same shared-memory offset as p in CTA `rank`
+__device__ __forceinline__ double dsmem_ld(const double* p, uint32_t rank) {
+    const uint32_t a = (uint32_t)__cvta_generic_to_shared(p);
+    uint32_t r;
+    asm volatile("mapa.shared::cluster.u32 %0, %1, %2;" : "=r"(r) : "r"(a), "r"(rank));
+    double v;
+    asm volatile("ld.shared::cluster.f64 %0, [%1];" : "=d"(v) : "r"(r) : "memory");
+    return v;
+}
+
+__device__ __forceinline__ double warp_sum_d(double v) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    return v;
+}
+
+// Shared-memory layout of k_sytrd (doubles): own rows R x n, the current
+// reflector v, p / w, the look-ahead row, the published p pieces, row and
+// partial dot (double-buffered), the pulled partial dots, reduction slots and
+// scalars.
+struct TdLayout {
+    int R, np;
+    size_t rows, vl, pf, rr, pb, rb, kb, kr, red, sc, total;
+    __host__ __device__ TdLayout(int n) {
+        R = (n + TD_C - 1) / TD_C;
+        np = (n + 1) & ~1;
+        rows = 0;
+        vl = rows + (size_t)R * n;
+        pf = vl + np;
+        rr = pf + np;
+        pb = rr + np;
+        rb = pb + 2 * (size_t)np;
+        kb = rb + 2 * (size_t)np;
+        kr = kb + 2;
+        red = kr + TD_C;
+        sc = red + TD_W;
+        total = sc + 8;
+    }
+};
+
+// dlarfg on x[0..len): v (v_0 = 1) into vl, sc[0] = tau, sc[1] = beta.  All
+// threads of the CTA; fixed reduction order, so every CTA that runs it on
+// the same x gets the same bits.
+__device__ __forceinline__ void td_reflector(const double* x, int len, double* vl, double* red, double* sc) {
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    double s = 0.0;
+    for (int k = 1 + tid; k < len; k += TD_T) s = fma(x[k], x[k], s);
+    s = warp_sum_d(s);
+    if (lane == 0) red[warp] = s;
+    __syncthreads();
+    if (tid == 0) {
+        double sig = 0.0;
+        for (int w = 0; w < TD_W; ++w) sig += red[w];
+        const double alpha = x[0];
+        double t = 0.0, beta = alpha, scal = 0.0;
+        if (sig > 0.0) {
+            beta = -copysign(hypot(alpha, sqrt(sig)), alpha);
+            t = (beta - alpha) / beta;
+            scal = 1.0 / (alpha - beta);
+        }
+        sc[0] = t;
+        sc[1] = beta;
+        sc[2] = scal;
+        sc[3] = sig > 0.0 ? 1.0 : 0.0;
+    }
+    __syncthreads();
+    const double scal = sc[2];
+    const bool nontriv = sc[3] != 0.0;
+    for (int k = tid; k < len; k += TD_T) vl[k] = k == 0 ? 1.0 : (nontriv ? x[k] * scal : 0.0);
+    __syncthreads();
+}
+
+// A (n x n, lda; the `upper` or lower triangle is read) -> d (n), e (n-1),
+// tau (n-1) and the reflectors in the strict lower part of Q (n x n, ld n;
+// Q(j+1+k, j) = v_k for k >= 1, dsytrd's 'L' storage).
+//
+// Column j with one cluster barrier: every CTA holds v_j.  Each forms p on
+// its own rows and its part of p^T v, and the owner of row j+1 publishes
+// that row as it stands; barrier; each pulls p, the partial dots and row
+// j+1, forms w, updates its own rows and its copy of row j+1, and runs
+// dlarfg on that copy for v_{j+1} itself (the same bits in every CTA).
+__global__ void __launch_bounds__(TD_T, 1) k_sytrd(const double* __restrict__ A, int lda, int n, int upper,
+                                                  double* __restrict__ Q, double* __restrict__ d,
+                                                  double* __restrict__ e, double* __restrict__ tau) {
+    extern __shared__ __align__(16) double sm[];
+    const TdLayout L(n);
+    const int R = L.R, np = L.np;
+    double* rows = sm + L.rows;
+    double* vl = sm + L.vl;
+    double* pf = sm + L.pf;
+    double* rr = sm + L.rr;
+    double* pb = sm + L.pb;
+    double* rb = sm + L.rb;
+    double* kb = sm + L.kb;
+    double* kr = sm + L.kr;
+    double* red = sm + L.red;
+    double* sc = sm + L.sc;
+    const int cr = (int)cluster_rank();
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+
+    for (int l = 0; l < R; ++l) {
+        const int i = l * TD_C + cr;
+        if (i >= n) break;
+        for (int k = tid; k < n; k += TD_T) {
+            const int a = i < k ? i : k, b = i < k ? k : i;  // (min, max)
+            rows[(size_t)l * n + k] = upper ? A[a + (size_t)b * lda] : A[b + (size_t)a * lda];
+        }
+    }
+    __syncthreads();
+    cluster_sync();
+    // v_0 from row 0 (CTA 0, local row 0)
+    for (int k = tid; k < n; k += TD_T) rr[k] = dsmem_ld(rows + k, 0);
+    __syncthreads();
+    td_reflector(rr + 1, n - 1, vl, red, sc);
+    if (cr == 0 && tid == 0) {
+        d[0] = rr[0];
+        e[0] = sc[1];
+        tau[0] = sc[0];
+        Q[0] = rr[0];
+        Q[1] = sc[1];
+    }
+    if (cr == 0)
+        for (int k = 1 + tid; k < n - 1; k += TD_T) Q[(size_t)(1 + k)] = vl[k];
+
+    for (int j = 0; j <= n - 2; ++j) {
+        const int m = n - 1 - j;  // length of v_j
+        const int par = j & 1;
+        const double t = sc[0];
+        // p_i = tau sum_k A(i, j+1+k) v_k on own rows i > j, and p^T v
+        double kacc = 0.0;
+        for (int l = warp; l < R; l += TD_W) {
+            const int i = l * TD_C + cr;
+            if (i <= j || i >= n) continue;
+            const double* a = rows + (size_t)l * n + j + 1;
+            double s0 = 0.0, s1 = 0.0;
+            int k = lane;
+            for (; k + 32 < m; k += 64) {
+                s0 = fma(a[k], vl[k], s0);
+                s1 = fma(a[k + 32], vl[k + 32], s1);
+            }
+            if (k < m) s0 = fma(a[k], vl[k], s0);
+            const double p = t * warp_sum_d(s0 + s1);
+            if (lane == 0) {
+                pb[par * np + (i - j - 1)] = p;
+                kacc = fma(p, vl[i - j - 1], kacc);
+            }
+        }
+        if (lane == 0) red[warp] = kacc;
+        if (cr == (j + 1) % TD_C) {  // publish row j+1, columns j+1..n-1, before this step's update
+            const double* a = rows + (size_t)((j + 1) / TD_C) * n + j + 1;
+            for (int k = tid; k < m; k += TD_T) rb[par * np + k] = a[k];
+        }
+        __syncthreads();
+        if (warp == 0) {
+            const double s = warp_sum_d(lane < TD_W ? red[lane] : 0.0);
+            if (lane == 0) kb[par] = s;
+        }
+        cluster_sync();  // p pieces, partial dots and row j+1 visible
+        for (int k = tid; k < m; k += TD_T) {
+            pf[k] = dsmem_ld(pb + par * np + k, (uint32_t)((j + 1 + k) % TD_C));
+            rr[k] = dsmem_ld(rb + par * np + k, (uint32_t)((j + 1) % TD_C));
+        }
+        if (tid < TD_C) kr[tid] = dsmem_ld(kb + par, (uint32_t)tid);
+        __syncthreads();
+        {
+            double ks = 0.0;
+            for (int c = 0; c < TD_C; ++c) ks += kr[c];
+            const double al = -0.5 * t * ks;
+            for (int k = tid; k < m; k += TD_T) pf[k] = fma(al, vl[k], pf[k]);  // w = p + alpha v
+        }
+        __syncthreads();
+        // A(i, j+1:n) -= v_i w^T + w_i v^T on own rows i > j, and on the copy
+        // of row j+1, whose columns j+3.. also give sigma of the next reflector
+        for (int l = warp; l < R; l += TD_W) {
+            const int i = l * TD_C + cr;
+            if (i <= j || i >= n) continue;
+            const int ii = i - j - 1;
+            const double vi = vl[ii], wi = pf[ii];
+            double* a = rows + (size_t)l * n + j + 1;
+            for (int k = lane; k < m; k += 32) a[k] = fma(-wi, vl[k], fma(-vi, pf[k], a[k]));
+        }
+        double sg = 0.0;
+        {
+            const double vi = vl[0], wi = pf[0];
+            for (int k = tid; k < m; k += TD_T) {
+                const double r = fma(-wi, vl[k], fma(-vi, pf[k], rr[k]));
+                rr[k] = r;
+                if (k >= 2) sg = fma(r, r, sg);
+            }
+        }
+        sg = warp_sum_d(sg);
+        if (lane == 0) red[warp] = sg;
+        __syncthreads();
+        if (j + 1 <= n - 2) {
+            // dlarfg on x = rr[1..m): v_{j+1} (the same bits in every CTA)
+            const int len = m - 1;
+            if (warp == 0) {
+                const double sig = warp_sum_d(lane < TD_W ? red[lane] : 0.0);
+                if (lane == 0) {
+                    const double alpha = rr[1];
+                    double tt = 0.0, beta = alpha, scal = 0.0;
+                    if (sig > 0.0) {
+                        beta = -copysign(hypot(alpha, sqrt(sig)), alpha);
+                        tt = (beta - alpha) / beta;
+                        scal = 1.0 / (alpha - beta);
+                    }
+                    sc[0] = tt;
+                    sc[1] = beta;
+                    sc[2] = scal;
+                    sc[3] = sig > 0.0 ? 1.0 : 0.0;
+                    if (cr == 0) {
+                        d[j + 1] = rr[0];
+                        e[j + 1] = beta;
+                        tau[j + 1] = tt;
+                        Q[(size_t)(j + 1) + (size_t)(j + 1) * n] = rr[0];
+                        Q[(size_t)(j + 2) + (size_t)(j + 1) * n] = beta;
+                    }
+                }
+            }
+            __syncthreads();
+            const double scal = sc[2];
+            const bool nontriv = sc[3] != 0.0;
+            for (int k = tid; k < len; k += TD_T) {
+                const double v = k == 0 ? 1.0 : (nontriv ? rr[1 + k] * scal : 0.0);
+                vl[k] = v;
+                if (cr == 0 && k > 0) Q[(size_t)(j + 2 + k) + (size_t)(j + 1) * n] = v;
+            }
+            __syncthreads();
+        } else if (cr == 0 && tid == 0) {
+            d[n - 1] = rr[0];
+            Q[(size_t)(n - 1) + (size_t)(n - 1) * n] = rr[0];
+        }
+    }
+    cluster_sync();  // no CTA leaves while another may still read its shared memory
+}
+
+// Sturm count: eigenvalues of T below x (dlaebz's recurrence and guard)
+__device__ __forceinline__ int sturm_count(const double* sd, const double* se2, int n, double x, double pivmin) {
+    double q = sd[0] - x;
+    if (fabs(q) <= pivmin) q = -pivmin;
+    int c = q < 0.0 ? 1 : 0;
+    for (int i = 1; i < n; ++i) {
+        q = sd[i] - x - se2[i - 1] / q;
+        if (fabs(q) <= pivmin) q = -pivmin;
+        c += q < 0.0 ? 1 : 0;
+    }
+    return c;
+}
+
+constexpr int BS_WARPS = 8;
+constexpr int BS_PTS = 4;  // trial points per lane (independent Sturm chains)
+
+// w[k] = k-th smallest eigenvalue of T (d, e), one warp per k, 32 x BS_PTS
+// trial points per round; aux[0] = |T|_1
+__global__ void __launch_bounds__(32 * BS_WARPS) k_tri_bisect(const double* __restrict__ d,
+                                                             const double* __restrict__ e, int n,
+                                                             double* __restrict__ w, double* __restrict__ aux) {
+    extern __shared__ double bsh[];
+    double* sd = bsh;
+    double* se2 = bsh + n;
+    for (int i = threadIdx.x; i < n; i += blockDim.x) {
+        sd[i] = d[i];
+        se2[i] = i < n - 1 ? e[i] * e[i] : 0.0;
+    }
+    __syncthreads();
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    double glo = DBL_MAX, ghi = -DBL_MAX, em2 = 0.0, nrm1 = 0.0;
+    for (int i = lane; i < n; i += 32) {
+        const double r = (i > 0 ? fabs(e[i - 1]) : 0.0) + (i < n - 1 ? fabs(e[i]) : 0.0);
+        glo = fmin(glo, sd[i] - r);
+        ghi = fmax(ghi, sd[i] + r);
+        em2 = fmax(em2, se2[i]);
+        nrm1 = fmax(nrm1, fabs(sd[i]) + r);
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        glo = fmin(glo, __shfl_xor_sync(0xffffffffu, glo, o));
+        ghi = fmax(ghi, __shfl_xor_sync(0xffffffffu, ghi, o));
+        em2 = fmax(em2, __shfl_xor_sync(0xffffffffu, em2, o));
+        nrm1 = fmax(nrm1, __shfl_xor_sync(0xffffffffu, nrm1, o));
+    }
+    if (blockIdx.x == 0 && threadIdx.x == 0) aux[0] = nrm1;
+    const int k = blockIdx.x * BS_WARPS + warp;
+    if (k >= n) return;
+    const double pivmin = DBL_MIN * fmax(1.0, em2);
+    const double tnorm = fmax(fabs(glo), fabs(ghi));
+    double lo = glo - 2.0 * DBL_EPSILON * tnorm * n - 2.0 * pivmin;
+    double hi = ghi + 2.0 * DBL_EPSILON * tnorm * n + 2.0 * pivmin;
+    constexpr int NPT = 32 * BS_PTS;
+    for (int round = 0; round < 64; ++round) {
+        if (hi - lo <= 2.0 * DBL_EPSILON * tnorm + pivmin) break;  // dstebz's absolute tolerance
+        const double h = hi - lo;
+        double x[BS_PTS], q[BS_PTS];
+        int c[BS_PTS];
+#pragma unroll
+        for (int u = 0; u < BS_PTS; ++u) {
+            x[u] = lo + h * ((double)(lane * BS_PTS + u + 1) / (double)(NPT + 1));
+            q[u] = sd[0] - x[u];
+            if (fabs(q[u]) <= pivmin) q[u] = -pivmin;
+            c[u] = q[u] < 0.0 ? 1 : 0;
+        }
+        for (int i = 1; i < n; ++i) {
+            const double di = sd[i], ei = se2[i - 1];
+#pragma unroll
+            for (int u = 0; u < BS_PTS; ++u) {
+                q[u] = di - x[u] - ei / q[u];
+                if (fabs(q[u]) <= pivmin) q[u] = -pivmin;
+                c[u] += q[u] < 0.0 ? 1 : 0;
+            }
+        }
+        // first trial point (in x order) with more than k eigenvalues below it
+        int first = NPT;
+#pragma unroll
+        for (int u = BS_PTS - 1; u >= 0; --u)
+            if (c[u] > k) first = lane * BS_PTS + u;
+        const int f = __reduce_min_sync(0xffffffffu, first);
+        const double xf = f < NPT ? lo + h * ((double)(f + 1) / (double)(NPT + 1)) : hi;
+        const double xb = f > 0 ? lo + h * ((double)f / (double)(NPT + 1)) : lo;
+        const double nlo = fmax(lo, xb), nhi = fmin(hi, xf);
+        if (nlo == lo && nhi == hi) break;  // the trial points no longer split the interval
+        lo = nlo;
+        hi = nhi;
+    }
+    if (lane == 0) w[k] = 0.5 * (lo + hi);
+}
+
+// Deterministic start vector entry in [-1, 1) (SplitMix64 of (eigenvalue, row))
+__device__ __forceinline__ double start_entry(int j, int i) {
+    unsigned long long z = ((unsigned long long)j << 32 | (unsigned)i) + 0x9E3779B97F4A7C15ull;
+    z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
+    z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
+    z ^= z >> 31;
+    return (double)(z >> 11) * (2.0 / 9007199254740992.0) - 1.0;
+}
+
+// Eigenvectors of T into Z (columns in the order of w).  One warp per group
+// of (nearly) equal eigenvalues, the vectors in registers: lane l holds rows
+// l*IV_RPL .. l*IV_RPL + IV_RPL - 1.  Each solve of (T - x I) y = b
+// eliminates with partial pivoting row by row (dgttrf's choices), the
+// current row handed from lane to lane, keeping U's diagonal reciprocal,
+// first and second super-diagonals and the transformed right-hand side in
+// the owning lane, then back-substitutes in reverse lane order.
+constexpr int IV_RPL = 20;  // rows per lane: n <= 640
+constexpr int IV_WARPS = 4;
+
+__global__ void __launch_bounds__(32 * IV_WARPS) k_tri_invit(const double* __restrict__ d,
+                                                            const double* __restrict__ e,
+                                                            const double* __restrict__ w,
+                                                            const double* __restrict__ aux, int n,
+                                                            double* __restrict__ Z, int ldz) {
+    extern __shared__ double ish[];  // d, e of T for the block's warps
+    double* sd = ish;
+    double* se = ish + n;
+    for (int i = threadIdx.x; i < n; i += blockDim.x) {
+        sd[i] = d[i];
+        se[i] = i < n - 1 ? e[i] : 0.0;
+    }
+    __syncthreads();
+    const int lane = threadIdx.x & 31;
+    const int k = blockIdx.x * IV_WARPS + (threadIdx.x >> 5);
+    if (k >= n) return;
+    const double onenrm = aux[0];
+    const double gtol = 1e-10 * onenrm;  // groups solved with Gram-Schmidt
+    if (k > 0 && w[k] - w[k - 1] <= gtol) return;  // inside a group started below
+    const double tol = DBL_EPSILON * onenrm;
+    const int i0 = lane * IV_RPL;
+    double ri[IV_RPL], u1[IV_RPL], u2[IV_RPL], y[IV_RPL];
+    double xjm = 0.0;
+    for (int j = k; j < n; ++j) {
+        if (j > k && w[j] - w[j - 1] > gtol) break;
+        const bool grp = j > k || (j + 1 < n && w[j + 1] - w[j] <= gtol);
+        double xj = w[j];
+        if (j > k) {
+            const double pertol = 10.0 * fabs(DBL_EPSILON * xj);
+            if (xj - xjm < pertol) xj = xjm + pertol;
+        }
+        xjm = xj;
+#pragma unroll
+        for (int r = 0; r < IV_RPL; ++r) y[r] = i0 + r < n ? start_entry(j, i0 + r) : 0.0;
+        const int nsolve = grp ? 4 : 2;
+        double nrm2 = 0.0;
+        for (int its = 0; its < nsolve; ++its) {
+            const double bnext = __shfl_down_sync(0xffffffffu, y[0], 1);  // b of the next lane's first row
+            // forward elimination; current row (D, C1, R) handed lane to lane
+            double D = 0.0, C1 = 0.0, R = 0.0;
+            for (int l = 0; l < 32 && l * IV_RPL < n; ++l) {
+                if (lane == l) {
+                    if (l == 0) {
+                        D = sd[0] - xj;
+                        C1 = se[0];
+                        R = y[0];
+                    }
+#pragma unroll
+                    for (int r = 0; r < IV_RPL; ++r) {
+                        const int i = i0 + r;
+                        if (i >= n - 1) break;
+                        const double sub = se[i];          // T(i+1, i)
+                        const double dn = sd[i + 1] - xj;  // T(i+1, i+1)
+                        const double up = se[i + 1];       // T(i+1, i+2) (0 past the end)
+                        const double bn = r + 1 < IV_RPL ? y[r + 1] : bnext;
+                        double ud, v1, v2, rf;
+                        if (fabs(D) >= fabs(sub)) {  // pivot on the current row
+                            const double f = D != 0.0 ? sub / D : 0.0;
+                            ud = D;
+                            v1 = C1;
+                            v2 = 0.0;
+                            rf = R;
+                            D = dn - f * C1;
+                            C1 = up;
+                            R = bn - f * R;
+                        } else {  // interchange: the next row is the pivot
+                            const double f = D / sub;
+                            ud = sub;
+                            v1 = dn;
+                            v2 = up;
+                            rf = bn;
+                            D = C1 - f * dn;
+                            C1 = -f * up;
+                            R = R - f * bn;
+                        }
+                        if (fabs(ud) < tol) ud = copysign(tol, ud);
+                        ri[r] = 1.0 / ud;
+                        u1[r] = v1;
+                        u2[r] = v2;
+                        y[r] = rf;
+                    }
+                }
+                D = __shfl_sync(0xffffffffu, D, l);
+                C1 = __shfl_sync(0xffffffffu, C1, l);
+                R = __shfl_sync(0xffffffffu, R, l);
+            }
+            // last row
+            if (fabs(D) < tol) D = copysign(tol, D);
+            const int ln = (n - 1) / IV_RPL, rn = (n - 1) - ln * IV_RPL;
+            // back substitution in reverse lane order, carrying y(i+1), y(i+2)
+            double y1 = R / D, y2 = 0.0;
+            for (int l = ln; l >= 0; --l) {
+                if (lane == l) {
+#pragma unroll
+                    for (int r = IV_RPL - 1; r >= 0; --r) {
+                        const int i = i0 + r;
+                        if (i > n - 1) continue;
+                        if (i == n - 1) {
+                            y[r] = y1;
+                            continue;
+                        }
+                        const double v = (y[r] - u1[r] * y1 - u2[r] * y2) * ri[r];
+                        y[r] = v;
+                        y2 = y1;
+                        y1 = v;
+                    }
+                }
+                y1 = __shfl_sync(0xffffffffu, y1, l);
+                y2 = __shfl_sync(0xffffffffu, y2, l);
+            }
+            (void)rn;
+            // Gram-Schmidt against the group's earlier vectors
+            for (int p = k; p < j; ++p) {
+                double dot = 0.0;
+#pragma unroll
+                for (int r = 0; r < IV_RPL; ++r)
+                    if (i0 + r < n) dot = fma(Z[i0 + r + (long)p * ldz], y[r], dot);
+                dot = warp_sum_d(dot);
+#pragma unroll
+                for (int r = 0; r < IV_RPL; ++r)
+                    if (i0 + r < n) y[r] = fma(-dot, Z[i0 + r + (long)p * ldz], y[r]);
+            }
+            double ss = 0.0;
+#pragma unroll
+            for (int r = 0; r < IV_RPL; ++r) ss = fma(y[r], y[r], ss);
+            nrm2 = warp_sum_d(ss);
+            const double sc1 = 1.0 / sqrt(nrm2);  // the next right-hand side is y / |y|
+#pragma unroll
+            for (int r = 0; r < IV_RPL; ++r) y[r] *= sc1;
+        }
+        // the largest component positive (dstein's convention); lowest row on ties
+        double big = -1.0;
+        int at = n;
+#pragma unroll
+        for (int r = 0; r < IV_RPL; ++r)
+            if (i0 + r < n && fabs(y[r]) > big) {
+                big = fabs(y[r]);
+                at = i0 + r;
+            }
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) {
+            const double ob = __shfl_xor_sync(0xffffffffu, big, o);
+            const int oa = __shfl_xor_sync(0xffffffffu, at, o);
+            if (ob > big || (ob == big && oa < at)) {
+                big = ob;
+                at = oa;
+            }
+        }
+        double vat = 0.0;
+#pragma unroll
+        for (int r = 0; r < IV_RPL; ++r)
+            if (i0 + r == at) vat = y[r];
+        vat = __shfl_sync(0xffffffffu, vat, at / IV_RPL);
+        const double sg = vat < 0.0 ? -1.0 : 1.0;
+#pragma unroll
+        for (int r = 0; r < IV_RPL; ++r)
+            if (i0 + r < n) Z[i0 + r + (long)j * ldz] = y[r] * sg;
+    }
+}
+
+static size_t td_smem_bytes(int n) { return TdLayout(n).total * sizeof(double); }
+
+int syevd_fast(double* A, int n, double* W, cublasFillMode_t uplo) {
+    Context& c = ctx();
+    if (n < 3 || n > 32 * IV_RPL) return RSDFT_EUNSUP;
+    const size_t smem = td_smem_bytes(n);
+    static int max_optin = -1, max_clusters = -1;
+    if (max_optin < 0) {
+        int dev = 0;
+        RS_CUDA(cudaGetDevice(&dev));
+        RS_CUDA(cudaDeviceGetAttribute(&max_optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev));
+    }
+    if (smem > (size_t)max_optin) return RSDFT_EUNSUP;
+    static size_t smem_set = 0;
+    if (smem > smem_set) {
+        RS_CUDA(cudaFuncSetAttribute(k_sytrd, cudaFuncAttributeNonPortableClusterSizeAllowed, 1));
+        RS_CUDA(cudaFuncSetAttribute(k_sytrd, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+        smem_set = smem;
+        max_clusters = -1;
+    }
+    cudaLaunchConfig_t cfg{};
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeClusterDimension;
+    attr[0].val.clusterDim.x = TD_C;
+    attr[0].val.clusterDim.y = 1;
+    attr[0].val.clusterDim.z = 1;
+    cfg.gridDim = dim3(TD_C);
+    cfg.blockDim = dim3(TD_T);
+    cfg.dynamicSmemBytes = smem;
+    cfg.stream = c.stream;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    if (max_clusters < 0) {
+        if (cudaOccupancyMaxActiveClusters(&max_clusters, k_sytrd, &cfg) != cudaSuccess) {
+            cudaGetLastError();
+            max_clusters = 0;
+        }
+    }
+    if (max_clusters < 1) return RSDFT_EUNSUP;
+
+    double *Q = nullptr, *dd = nullptr, *ws = nullptr, *work = nullptr;
+    int* dinfo = nullptr;
+    RS_CHECK(workspace_t("eig_Q", (size_t)n * n, &Q));
+    RS_CHECK(workspace_t("eig_dd", (size_t)4 * n + 8, &dd));
+    RS_CHECK(workspace_t("eig_ws", (size_t)2 * n * n, &ws));
+    RS_CHECK(workspace_t("eig_info", 4, &dinfo));
+    double* d = dd;
+    double* e = dd + n;
+    double* tau = dd + 2 * n;
+    double* aux = dd + 3 * n;
+    ++g_kernel_launches;
+    RS_CUDA(cudaLaunchKernelEx(&cfg, k_sytrd, (const double*)A, n, n, uplo == CUBLAS_FILL_MODE_UPPER ? 1 : 0, Q, d,
+                               e, tau));
+    RS_LAUNCH();
+    launch(k_tri_bisect, div_up(n, BS_WARPS), 32 * BS_WARPS, (size_t)2 * n * sizeof(double), c.stream,
+           (const double*)d, (const double*)e, n, W, aux);
+    RS_LAUNCH();
+    launch(k_tri_invit, div_up(n, IV_WARPS), 32 * IV_WARPS, (size_t)2 * n * sizeof(double), c.stream, (const double*)d, (const double*)e,
+           (const double*)W, (const double*)aux, n, A, n);
+    RS_LAUNCH();
+    // two Newton-Schulz steps on Z (in A), through Z2 (in ws)
+    {
+        const double one = 1.0, zero = 0.0, half = -0.5, c15 = 1.5;
+        double* G = ws;
+        double* Z2 = ws + (size_t)n * n;
+        double* src = A;
+        double* dst = Z2;
+        for (int it = 0; it < 2; ++it) {
+            RS_BLAS(cublasDgemm(c.blas, CUBLAS_OP_T, CUBLAS_OP_N, n, n, n, &one, src, n, src, n, &zero, G, n));
+            RS_CUDA(cudaMemcpyAsync(dst, src, sizeof(double) * (size_t)n * n, cudaMemcpyDeviceToDevice, c.stream));
+            RS_BLAS(cublasDgemm(c.blas, CUBLAS_OP_N, CUBLAS_OP_N, n, n, n, &half, src, n, G, n, &c15, dst, n));
+            double* t = src;
+            src = dst;
+            dst = t;
+        }
+        (void)src;  // two steps: the result is back in A
+    }
+    int lwork = 0;
+    RS_SOLVER(cusolverDnDormtr_bufferSize(c.solver, CUBLAS_SIDE_LEFT, CUBLAS_FILL_MODE_LOWER, CUBLAS_OP_N, n, n, Q, n,
+                                          tau, A, n, &lwork));
+    RS_CHECK(workspace_t("eig_work", (size_t)lwork + 1, &work));
+    RS_SOLVER(cusolverDnDormtr(c.solver, CUBLAS_SIDE_LEFT, CUBLAS_FILL_MODE_LOWER, CUBLAS_OP_N, n, n, Q, n, tau, A, n,
+                               work, lwork, dinfo));
+    return RSDFT_OK;
+}
+
+}  // namespace rsdft

@@ -220,41 +220,102 @@ struct TmaMaps {
     CUtensorMap vloc;                   // Vloc box of height TY
 };
 
+// Stencil coefficients in the kernel's arithmetic type, so every FMA takes
+// its coefficient straight from the parameter bank (no per-use conversion).
+template <typename T>
+struct CoefT {
+    T c0;
+    T cx[MAXMD], cy[MAXMD], cz[MAXMD];
+};
+
+template <typename T>
+static CoefT<T> coef_as(const StencilCoef& cf) {
+    CoefT<T> o{};
+    o.c0 = (T)cf.c0;
+    for (int m = 0; m < MAXMD; ++m) {
+        o.cx[m] = (T)cf.cx[m];
+        o.cy[m] = (T)cf.cy[m];
+        o.cz[m] = (T)cf.cz[m];
+    }
+    return o;
+}
+
+// Arithmetic lanes of the TMA stencil: one double, or two floats through the
+// packed FP32 instructions of sm_100 (__ffma2_rn and friends: two
+// independent IEEE operations per instruction, bitwise the same results as
+// the scalar ones, half the issue slots).  A 16-byte shared-memory vector
+// holds two packs in both cases.
+template <typename T>
+struct Pk;
+template <>
+struct Pk<double> {
+    using t = double;
+    static constexpr int W = 1;
+    __device__ static __forceinline__ t fma(t a, t b, t c) { return __fma_rn(a, b, c); }
+    __device__ static __forceinline__ t add(t a, t b) { return __dadd_rn(a, b); }
+    __device__ static __forceinline__ t mul(t a, t b) { return __dmul_rn(a, b); }
+    __device__ static __forceinline__ t splat(double v) { return v; }
+    __device__ static __forceinline__ t of(const double* p) { return p[0]; }
+    __device__ static __forceinline__ void get2(const double2& v, t* o) {
+        o[0] = v.x;
+        o[1] = v.y;
+    }
+    __device__ static __forceinline__ double2 put2(const t* o) { return make_double2(o[0], o[1]); }
+};
+template <>
+struct Pk<float> {
+    using t = float2;
+    static constexpr int W = 2;
+    __device__ static __forceinline__ t fma(t a, t b, t c) { return __ffma2_rn(a, b, c); }
+    __device__ static __forceinline__ t add(t a, t b) { return __fadd2_rn(a, b); }
+    __device__ static __forceinline__ t mul(t a, t b) { return __fmul2_rn(a, b); }
+    __device__ static __forceinline__ t splat(float v) { return make_float2(v, v); }
+    __device__ static __forceinline__ t of(const float* p) { return make_float2(p[0], p[1]); }
+    __device__ static __forceinline__ void get2(const float4& v, t* o) {
+        o[0] = make_float2(v.x, v.y);
+        o[1] = make_float2(v.z, v.w);
+    }
+    __device__ static __forceinline__ float4 put2(const t* o) { return make_float4(o[0].x, o[0].y, o[1].x, o[1].y); }
+};
+
 // One arrival's z pushes for accumulator slot U (compile time): outputs
 // U + m (first touch at m = Md) and U - m get cz_m c, slot U gets the in-plane
 // part when the plane is one of the tile's own, and slot U + Md + 1 (the
-// output completed by this arrival) is written when hp is set.
-template <typename T, int MD, int NP, int BY, int VX, int U>
-__device__ __forceinline__ void push_body(T (&acc)[2 * MD + 1][NP], const T* c, const T* in, bool inner,
-                                          const StencilCoef& cf, T* hp, int n1) {
-    using VT = Vec16<T>;
-    using V = typename VT::t;
+// output completed by this arrival) is written when hp is set.  NK packs per
+// thread, two per row.
+template <typename T, int MD, int NK, int BY, int U>
+__device__ __forceinline__ void push_body(typename Pk<T>::t (&acc)[2 * MD + 1][NK], const typename Pk<T>::t* c,
+                                          const typename Pk<T>::t* in, bool inner, const CoefT<T>& cf, T* hp,
+                                          int n1) {
+    using P = Pk<T>;
     constexpr int Q = 2 * MD + 1;
 #pragma unroll
-    for (int i = 0; i < NP; ++i) {
-        acc[(U + MD) % Q][i] = (T)cf.cz[MD - 1] * c[i];
+    for (int i = 0; i < NK; ++i) {
+        acc[(U + MD) % Q][i] = P::mul(P::splat(cf.cz[MD - 1]), c[i]);
 #pragma unroll
-        for (int m = 1; m < MD; ++m) acc[(U + m) % Q][i] += (T)cf.cz[m - 1] * c[i];
+        for (int m = 1; m < MD; ++m) acc[(U + m) % Q][i] = P::fma(P::splat(cf.cz[m - 1]), c[i], acc[(U + m) % Q][i]);
 #pragma unroll
-        for (int m = 1; m <= MD; ++m) acc[(U + Q - m) % Q][i] += (T)cf.cz[m - 1] * c[i];
-        if (inner) acc[U][i] += in[i];
+        for (int m = 1; m <= MD; ++m)
+            acc[(U + Q - m) % Q][i] = P::fma(P::splat(cf.cz[m - 1]), c[i], acc[(U + Q - m) % Q][i]);
+        if (inner) acc[U][i] = P::add(acc[U][i], in[i]);
     }
     if (hp) {
 #pragma unroll
         for (int r = 0; r < BY; ++r)
-            *reinterpret_cast<V*>(hp + (long)r * n1) = VT::make(&acc[(U + MD + 1) % Q][r * VX]);
+            *reinterpret_cast<typename Vec16<T>::t*>(hp + (long)r * n1) = P::put2(&acc[(U + MD + 1) % Q][2 * r]);
     }
 }
 
 // Runtime slot -> compile-time slot: only the short push runs per case, so
 // the loop body is not replicated 2 Md + 1 times.
-template <typename T, int MD, int NP, int BY, int VX>
-__device__ __forceinline__ void push_slot(int u, T (&acc)[2 * MD + 1][NP], const T* c, const T* in, bool inner,
-                                          const StencilCoef& cf, T* hp, int n1) {
+template <typename T, int MD, int NK, int BY>
+__device__ __forceinline__ void push_slot(int u, typename Pk<T>::t (&acc)[2 * MD + 1][NK], const typename Pk<T>::t* c,
+                                          const typename Pk<T>::t* in, bool inner, const CoefT<T>& cf, T* hp,
+                                          int n1) {
     constexpr int Q = 2 * MD + 1;
 #define RS_PUSH_CASE(K)                                                                  \
     case K:                                                                              \
-        if constexpr (K < Q) push_body<T, MD, NP, BY, VX, K>(acc, c, in, inner, cf, hp, n1); \
+        if constexpr (K < Q) push_body<T, MD, NK, BY, K>(acc, c, in, inner, cf, hp, n1); \
         break;
     switch (u) {
         RS_PUSH_CASE(0) RS_PUSH_CASE(1) RS_PUSH_CASE(2) RS_PUSH_CASE(3) RS_PUSH_CASE(4) RS_PUSH_CASE(5)
@@ -280,7 +341,7 @@ __device__ __forceinline__ void push_slot(int u, T (&acc)[2 * MD + 1][NP], const
 // while its own plane is current and the ring can stay shallow.
 template <typename T, int MD, int BY>
 __global__ void __launch_bounds__(384, 1) k_stencil_tma(const __grid_constant__ TmaMaps maps, StencilArgs<T> a,
-                                                       StencilCoef cf, int TY, int RS, int S, int ncw,
+                                                       const CoefT<T> cf, int TY, int RS, int S, int ncw,
                                                        int* __restrict__ err) {
     using VT = Vec16<T>;
     using V = typename VT::t;
@@ -366,13 +427,16 @@ __global__ void __launch_bounds__(384, 1) k_stencil_tma(const __grid_constant__ 
     const int x = VX * px, yl = BY * py;
     const int xw = x - MDX;  // first x of the periodic window
     T* __restrict__ hb = a.hpsi + (long)band * a.ld + (long)n1 * (y0 + yl) + x;
-    const T c0 = (T)cf.c0;
+    using P = Pk<T>;
+    using PT = typename P::t;
+    constexpr int W = P::W;
+    constexpr int NK = NP / W;  // packs per thread, two per row
 
-    T acc[Q][NP];
+    PT acc[Q][NK];
 #pragma unroll
     for (int q = 0; q < Q; ++q)
 #pragma unroll
-        for (int i = 0; i < NP; ++i) acc[q][i] = (T)0;
+        for (int i = 0; i < NK; ++i) acc[q][i] = P::splat((T)0);
 
     bool ok = true;
     int s = 0, u = 0;
@@ -381,26 +445,26 @@ __global__ void __launch_bounds__(384, 1) k_stencil_tma(const __grid_constant__ 
         if (!mbar_wait(&full[s], ph)) ok = false;
         const T* st = stages + (size_t)s * SE;
         const bool inner = k >= MD && k < MD + zlen;  // uniform
-        T c[NP], in[NP];
+        PT c[NK], in[NK];
         if (inner) {
             const T* sp = st + yl * RS + x;
 #pragma unroll
-            for (int i = 0; i < NP; ++i) in[i] = (T)0;
+            for (int i = 0; i < NK; ++i) in[i] = P::splat((T)0);
             // y neighbours (the window also holds the thread's own rows)
 #pragma unroll
             for (int j = 0; j < BY + 2 * MD; ++j) {
-                T v[VX];
-                VT::get(*reinterpret_cast<const V*>(sp + j * RS), v);
+                PT v[2];
+                P::get2(*reinterpret_cast<const V*>(sp + j * RS), v);
 #pragma unroll
                 for (int r = 0; r < BY; ++r) {
                     const int m = j - MD - r;
                     if (m == 0) {
-#pragma unroll
-                        for (int e = 0; e < VX; ++e) c[r * VX + e] = v[e];
+                        c[2 * r] = v[0];
+                        c[2 * r + 1] = v[1];
                     } else if (m >= -MD && m <= MD) {
-                        const T cy = (T)cf.cy[(m > 0 ? m : -m) - 1];
+                        const PT cy = P::splat(cf.cy[(m > 0 ? m : -m) - 1]);
 #pragma unroll
-                        for (int e = 0; e < VX; ++e) in[r * VX + e] += cy * v[e];
+                        for (int e = 0; e < 2; ++e) in[2 * r + e] = P::fma(cy, v[e], in[2 * r + e]);
                     }
                 }
             }
@@ -416,33 +480,32 @@ __global__ void __launch_bounds__(384, 1) k_stencil_tma(const __grid_constant__ 
                     VT::get(*reinterpret_cast<const V*>(rp + xx), w + j * VX);
                 }
 #pragma unroll
-                for (int e = 0; e < VX; ++e)
+                for (int e = 0; e < 2; ++e)
 #pragma unroll
                     for (int m = 1; m <= MD; ++m)
-                        in[r * VX + e] += (T)cf.cx[m - 1] * (w[MDX + e - m] + w[MDX + e + m]);
+                        in[2 * r + e] = P::fma(P::splat(cf.cx[m - 1]),
+                                               P::add(P::of(w + MDX + W * e - m), P::of(w + MDX + W * e + m)),
+                                               in[2 * r + e]);
             }
             // centre and local potential
 #pragma unroll
             for (int r = 0; r < BY; ++r) {
-                T vl[VX];
-                VT::get(*reinterpret_cast<const V*>(sp + (ROWS + r) * RS), vl);
+                PT vl[2];
+                P::get2(*reinterpret_cast<const V*>(sp + (ROWS + r) * RS), vl);
 #pragma unroll
-                for (int e = 0; e < VX; ++e) {
-                    const int i = r * VX + e;
-                    in[i] += (c0 + vl[e]) * c[i];
-                }
+                for (int e = 0; e < 2; ++e)
+                    in[2 * r + e] = P::fma(P::add(P::splat(cf.c0), vl[e]), c[2 * r + e], in[2 * r + e]);
             }
         } else {
 #pragma unroll
-            for (int r = 0; r < BY; ++r)
-                VT::get(*reinterpret_cast<const V*>(st + (MD + yl + r) * RS + x), c + r * VX);
+            for (int r = 0; r < BY; ++r) P::get2(*reinterpret_cast<const V*>(st + (MD + yl + r) * RS + x), c + 2 * r);
         }
         __syncwarp();
         if (lane == 0) mbar_arrive(&empty[s]);  // this warp is done with the stage
         // z pushes into the accumulator ring (slot = output arrival mod Q)
         // and, from arrival 2 Md on, the write of the completed output k - Md
         T* hp = (k >= 2 * MD && thr) ? hb + plane * (zs + k - 2 * MD) : nullptr;
-        push_slot<T, MD, NP, BY, VX>(u, acc, c, in, inner, cf, hp, n1);
+        push_slot<T, MD, NK, BY>(u, acc, c, in, inner, cf, hp, n1);
         if (++s == S) {
             s = 0;
             ph ^= 1u;
@@ -601,7 +664,8 @@ static int launch_tma(StencilArgs<T> a, const StencilCoef& cf, int nb, cudaStrea
         attr_set = true;
     }
     dim3 grid(a.n2 / g.TY, (unsigned)(nb * a.nzc));
-    launch(k_stencil_tma<T, MD, BY>, grid, g.threads, g.smem, st, maps, a, cf, g.TY, g.RS, g.S, g.ncw, c.err_flag);
+    launch(k_stencil_tma<T, MD, BY>, grid, g.threads, g.smem, st, maps, a, coef_as<T>(cf), g.TY, g.RS, g.S, g.ncw,
+           c.err_flag);
     RS_LAUNCH();
     *used = true;
     return RSDFT_OK;

@@ -71,6 +71,14 @@ int cg_device_f32(const double* unk, long ld, int mb, int spin, double* esp, dou
 // written to psi (FP64).  Mixed forms only.
 int orth_subspace_diag_f32(const float* x32, double* psi, long ld, int mb, int spin, double* esp_dev, int mode);
 
+// Eigen-decomposition of the symmetric n x n A (column-major, ld n; the
+// `uplo` triangle is read): W ascending, A overwritten by the eigenvectors.
+// Cluster-resident tridiagonalisation + bisection / inverse iteration +
+// cuSOLVER ormtr; RSDFT_EUNSUP when n is outside its range (n < 3, or the
+// rows do not fit the cluster's shared memory) or 16-CTA clusters are not
+// available, so the caller takes cuSOLVER's syevd.
+int syevd_fast(double* A, int n, double* W, cublasFillMode_t uplo);
+
 // CG over all bands (device data).
 int cg_device(double* unk, long ld, int mb, int spin, double* esp_dev, double* res_dev, int ncg, int mloop,
               int ipc, int mode);

@@ -89,7 +89,7 @@ def run_hpsi(args) -> dict:
 
 
 def run_iteration(args) -> dict:
-    torch, api, g, cell, st, psi = _setup(args.workload)
+    torch, api, g, cell, st, psi = _setup(args.workload, args.ngrid, args.bands)
     MB = cell.nband
     u = psi.t().contiguous().t()
     g.gram_schmidt(1, MB, 1, 1, u)
@@ -98,7 +98,8 @@ def run_iteration(args) -> dict:
     mode = MODES[args.mode]
     ms = _timed(torch, st, lambda: g.eigensolver_iteration(u, esp, res, ncg=args.ncg, mloop=args.mloop, mode=mode),
                 args.warmup, args.steps)
-    return {"what": "iteration", "workload": args.workload, "mode": args.mode, "ms_per_iter": ms}
+    return {"what": "iteration", "workload": args.workload, "grid": list(cell.ngrid), "bands": MB, "mode": args.mode,
+            "ms_per_iter": ms}
 
 
 def run_rr(args) -> dict:
@@ -177,6 +178,8 @@ def main(argv=None) -> None:
     it.add_argument("--mloop", type=int, default=3)
     it.add_argument("--warmup", type=int, default=3)
     it.add_argument("--steps", type=int, default=2)
+    it.add_argument("--ngrid", type=int, default=0)
+    it.add_argument("--bands", type=int, default=0)
     rr = sub.add_parser("rr")
     rr.add_argument("--workload", default="si216")
     rr.add_argument("--mode", default="mixed-bf16", choices=sorted(MODES))
