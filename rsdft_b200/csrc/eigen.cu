@@ -76,20 +76,35 @@ __device__ __forceinline__ double warp_sum_d(double v) {
     return v;
 }
 
+// 1/q for normal q by Newton-Raphson iteration for the reciprocal
+// (r <- r + r (1 - q r), quadratic convergence) from the PTX approximate
+// reciprocal: two steps take the ~2^-22 seed past double precision (checked
+// against 1/q on 7.6e7 samples spanning exponents +-1000: no difference).
+// A dependent IEEE division costs ~310 cycles on B200, this ~60, and the
+// serial chains below (Sturm counts, pivots, reflector scalars) are made of
+// them.
+__device__ __forceinline__ double rcp_nr(double q) {
+    double r;
+    asm("rcp.approx.ftz.f64 %0, %1;" : "=d"(r) : "d"(q));
+    r = fma(r, fma(-q, r, 1.0), r);
+    return fma(r, fma(-q, r, 1.0), r);
+}
+
 // Shared-memory layout of k_sytrd (doubles): own rows R x n, the current
 // reflector v, p / w, the look-ahead row, the published p pieces, row and
 // partial dot (double-buffered), the pulled partial dots, reduction slots and
 // scalars.
 struct TdLayout {
     int R, np;
-    size_t rows, vl, pf, rr, pb, rb, kb, kr, red, sc, total;
+    size_t rows, vl, pf, wf, rr, pb, rb, kb, kr, red, sc, total;
     __host__ __device__ TdLayout(int n) {
         R = (n + TD_C - 1) / TD_C;
         np = (n + 1) & ~1;
         rows = 0;
-        vl = rows + (size_t)R * n;
-        pf = vl + np;
-        rr = pf + np;
+        vl = rows + (size_t)R * n;  // [2][np]: v_j and v_{j+1}
+        pf = vl + 2 * (size_t)np;
+        wf = pf + np;
+        rr = wf + np;
         pb = rr + np;
         rb = pb + 2 * (size_t)np;
         kb = rb + 2 * (size_t)np;
@@ -116,9 +131,9 @@ __device__ __forceinline__ void td_reflector(const double* x, int len, double* v
         const double alpha = x[0];
         double t = 0.0, beta = alpha, scal = 0.0;
         if (sig > 0.0) {
-            beta = -copysign(hypot(alpha, sqrt(sig)), alpha);
-            t = (beta - alpha) / beta;
-            scal = 1.0 / (alpha - beta);
+            beta = -copysign(sqrt(fma(alpha, alpha, sig)), alpha);
+            t = (beta - alpha) * rcp_nr(beta);
+            scal = rcp_nr(alpha - beta);
         }
         sc[0] = t;
         sc[1] = beta;
@@ -136,11 +151,14 @@ __device__ __forceinline__ void td_reflector(const double* x, int len, double* v
 // tau (n-1) and the reflectors in the strict lower part of Q (n x n, ld n;
 // Q(j+1+k, j) = v_k for k >= 1, dsytrd's 'L' storage).
 //
-// Column j with one cluster barrier: every CTA holds v_j.  Each forms p on
-// its own rows and its part of p^T v, and the owner of row j+1 publishes
-// that row as it stands; barrier; each pulls p, the partial dots and row
-// j+1, forms w, updates its own rows and its copy of row j+1, and runs
-// dlarfg on that copy for v_{j+1} itself (the same bits in every CTA).
+// Column j with one cluster barrier.  Before it every CTA has published p_j
+// = tau_j A v_j on its own rows and its part of p_j^T v_j, and the owner of
+// row j+1 that row as it stands.  After it every CTA pulls them, forms w_j,
+// brings its copy of row j+1 up to date and runs dlarfg on it for v_{j+1}
+// (the same bits in every CTA), then makes one pass over its own rows that
+// applies A -= v_j w_j^T + w_j v_j^T and, on the updated values, forms
+// p_{j+1} and publishes it (and row j+2, if it owns it) for the next
+// barrier.
 __global__ void __launch_bounds__(TD_T, 1) k_sytrd(const double* __restrict__ A, int lda, int n, int upper,
                                                   double* __restrict__ Q, double* __restrict__ d,
                                                   double* __restrict__ e, double* __restrict__ tau) {
@@ -148,8 +166,9 @@ __global__ void __launch_bounds__(TD_T, 1) k_sytrd(const double* __restrict__ A,
     const TdLayout L(n);
     const int R = L.R, np = L.np;
     double* rows = sm + L.rows;
-    double* vl = sm + L.vl;
+    double* vb = sm + L.vl;  // [2][np]
     double* pf = sm + L.pf;
+    double* wf = sm + L.wf;
     double* rr = sm + L.rr;
     double* pb = sm + L.pb;
     double* rb = sm + L.rb;
@@ -173,7 +192,7 @@ __global__ void __launch_bounds__(TD_T, 1) k_sytrd(const double* __restrict__ A,
     // v_0 from row 0 (CTA 0, local row 0)
     for (int k = tid; k < n; k += TD_T) rr[k] = dsmem_ld(rows + k, 0);
     __syncthreads();
-    td_reflector(rr + 1, n - 1, vl, red, sc);
+    td_reflector(rr + 1, n - 1, vb, red, sc);
     if (cr == 0 && tid == 0) {
         d[0] = rr[0];
         e[0] = sc[1];
@@ -182,70 +201,65 @@ __global__ void __launch_bounds__(TD_T, 1) k_sytrd(const double* __restrict__ A,
         Q[1] = sc[1];
     }
     if (cr == 0)
-        for (int k = 1 + tid; k < n - 1; k += TD_T) Q[(size_t)(1 + k)] = vl[k];
-
-    for (int j = 0; j <= n - 2; ++j) {
-        const int m = n - 1 - j;  // length of v_j
-        const int par = j & 1;
-        const double t = sc[0];
-        // p_i = tau sum_k A(i, j+1+k) v_k on own rows i > j, and p^T v
+        for (int k = 1 + tid; k < n - 1; k += TD_T) Q[(size_t)(1 + k)] = vb[k];
+    double tcur = sc[0];  // tau of the current column
+    // p_0 on own rows i > 0, and row 1 published by its owner
+    {
+        const double t = tcur;
+        const int m = n - 1;
         double kacc = 0.0;
         for (int l = warp; l < R; l += TD_W) {
             const int i = l * TD_C + cr;
-            if (i <= j || i >= n) continue;
-            const double* a = rows + (size_t)l * n + j + 1;
-            double s0 = 0.0, s1 = 0.0;
-            int k = lane;
-            for (; k + 32 < m; k += 64) {
-                s0 = fma(a[k], vl[k], s0);
-                s1 = fma(a[k + 32], vl[k + 32], s1);
-            }
-            if (k < m) s0 = fma(a[k], vl[k], s0);
-            const double p = t * warp_sum_d(s0 + s1);
+            if (i < 1 || i >= n) continue;
+            const double* a = rows + (size_t)l * n + 1;
+            double s0 = 0.0;
+            for (int k = lane; k < m; k += 32) s0 = fma(a[k], vb[k], s0);
+            const double pv = t * warp_sum_d(s0);
             if (lane == 0) {
-                pb[par * np + (i - j - 1)] = p;
-                kacc = fma(p, vl[i - j - 1], kacc);
+                pb[i - 1] = pv;
+                kacc = fma(pv, vb[i - 1], kacc);
             }
+            if (i == 1)
+                for (int k = lane; k < m; k += 32) rb[k] = a[k];
         }
         if (lane == 0) red[warp] = kacc;
-        if (cr == (j + 1) % TD_C) {  // publish row j+1, columns j+1..n-1, before this step's update
-            const double* a = rows + (size_t)((j + 1) / TD_C) * n + j + 1;
-            for (int k = tid; k < m; k += TD_T) rb[par * np + k] = a[k];
-        }
         __syncthreads();
         if (warp == 0) {
-            const double s = warp_sum_d(lane < TD_W ? red[lane] : 0.0);
-            if (lane == 0) kb[par] = s;
+            const double s1 = warp_sum_d(lane < TD_W ? red[lane] : 0.0);
+            if (lane == 0) kb[0] = s1;
         }
-        cluster_sync();  // p pieces, partial dots and row j+1 visible
+    }
+
+    for (int j = 0; j <= n - 2; ++j) {
+        const int m = n - 1 - j;  // length of v_j
+        const int par = j & 1, nxt = par ^ 1;
+        const double* vj = vb + par * np;
+        double* vn = vb + nxt * np;
+        const double t = tcur;
+        cluster_sync();  // p_j pieces, partial dots and row j+1 visible
         for (int k = tid; k < m; k += TD_T) {
             pf[k] = dsmem_ld(pb + par * np + k, (uint32_t)((j + 1 + k) % TD_C));
             rr[k] = dsmem_ld(rb + par * np + k, (uint32_t)((j + 1) % TD_C));
         }
         if (tid < TD_C) kr[tid] = dsmem_ld(kb + par, (uint32_t)tid);
         __syncthreads();
-        {
-            double ks = 0.0;
-            for (int c = 0; c < TD_C; ++c) ks += kr[c];
-            const double al = -0.5 * t * ks;
-            for (int k = tid; k < m; k += TD_T) pf[k] = fma(al, vl[k], pf[k]);  // w = p + alpha v
-        }
-        __syncthreads();
-        // A(i, j+1:n) -= v_i w^T + w_i v^T on own rows i > j, and on the copy
-        // of row j+1, whose columns j+3.. also give sigma of the next reflector
-        for (int l = warp; l < R; l += TD_W) {
-            const int i = l * TD_C + cr;
-            if (i <= j || i >= n) continue;
-            const int ii = i - j - 1;
-            const double vi = vl[ii], wi = pf[ii];
-            double* a = rows + (size_t)l * n + j + 1;
-            for (int k = lane; k < m; k += 32) a[k] = fma(-wi, vl[k], fma(-vi, pf[k], a[k]));
-        }
+        // w = p + alpha v (into wf), row j+1 up to date; its columns j+3..
+        // give sigma of v_{j+1}
         double sg = 0.0;
         {
-            const double vi = vl[0], wi = pf[0];
+            double kp[TD_C / 2];  // pairwise sum of the 16 partial dots (fixed order)
+#pragma unroll
+            for (int c = 0; c < TD_C / 2; ++c) kp[c] = kr[2 * c] + kr[2 * c + 1];
+#pragma unroll
+            for (int h = TD_C / 4; h >= 1; h >>= 1)
+#pragma unroll
+                for (int c = 0; c < h; ++c) kp[c] = kp[2 * c] + kp[2 * c + 1];
+            const double al = -0.5 * t * kp[0];
+            const double vi = vj[0], wi = fma(al, vi, pf[0]);
             for (int k = tid; k < m; k += TD_T) {
-                const double r = fma(-wi, vl[k], fma(-vi, pf[k], rr[k]));
+                const double wk = fma(al, vj[k], pf[k]);
+                wf[k] = wk;
+                const double r = fma(-wi, vj[k], fma(-vi, wk, rr[k]));
                 rr[k] = r;
                 if (k >= 2) sg = fma(r, r, sg);
             }
@@ -253,45 +267,91 @@ __global__ void __launch_bounds__(TD_T, 1) k_sytrd(const double* __restrict__ A,
         sg = warp_sum_d(sg);
         if (lane == 0) red[warp] = sg;
         __syncthreads();
-        if (j + 1 <= n - 2) {
-            // dlarfg on x = rr[1..m): v_{j+1} (the same bits in every CTA)
-            const int len = m - 1;
-            if (warp == 0) {
-                const double sig = warp_sum_d(lane < TD_W ? red[lane] : 0.0);
-                if (lane == 0) {
-                    const double alpha = rr[1];
-                    double tt = 0.0, beta = alpha, scal = 0.0;
-                    if (sig > 0.0) {
-                        beta = -copysign(hypot(alpha, sqrt(sig)), alpha);
-                        tt = (beta - alpha) / beta;
-                        scal = 1.0 / (alpha - beta);
-                    }
-                    sc[0] = tt;
-                    sc[1] = beta;
-                    sc[2] = scal;
-                    sc[3] = sig > 0.0 ? 1.0 : 0.0;
-                    if (cr == 0) {
-                        d[j + 1] = rr[0];
-                        e[j + 1] = beta;
-                        tau[j + 1] = tt;
-                        Q[(size_t)(j + 1) + (size_t)(j + 1) * n] = rr[0];
-                        Q[(size_t)(j + 2) + (size_t)(j + 1) * n] = beta;
-                    }
+        if (j + 1 > n - 2) {
+            if (cr == 0 && tid == 0) {
+                d[n - 1] = rr[0];
+                Q[(size_t)(n - 1) + (size_t)(n - 1) * n] = rr[0];
+            }
+            break;
+        }
+        // dlarfg on x = rr[1..m): v_{j+1}; every warp forms the scalars itself
+        const int len = m - 1;
+        double tn, scal;
+        bool nontriv;
+        {
+            const double sig = warp_sum_d(lane < TD_W ? red[lane] : 0.0);
+            const double alpha = rr[1];
+            double tt = 0.0, beta = alpha, sl = 0.0;
+            if (sig > 0.0) {
+                beta = -copysign(sqrt(fma(alpha, alpha, sig)), alpha);
+                tt = (beta - alpha) * rcp_nr(beta);
+                sl = rcp_nr(alpha - beta);
+            }
+            tn = tt;
+            scal = sl;
+            nontriv = sig > 0.0;
+            if (cr == 0 && tid == 0) {
+                sc[0] = tt;
+                d[j + 1] = rr[0];
+                e[j + 1] = beta;
+                tau[j + 1] = tt;
+                Q[(size_t)(j + 1) + (size_t)(j + 1) * n] = rr[0];
+                Q[(size_t)(j + 2) + (size_t)(j + 1) * n] = beta;
+            }
+        }
+        for (int k = tid; k < len; k += TD_T) {
+            const double v = k == 0 ? 1.0 : (nontriv ? rr[1 + k] * scal : 0.0);
+            vn[k] = v;
+            if (cr == 0 && k > 0) Q[(size_t)(j + 2 + k) + (size_t)(j + 1) * n] = v;
+        }
+        __syncthreads();
+        // one pass over own rows i > j: the step-j update, then p_{j+1} on rows i > j+1
+        double kacc = 0.0;
+        for (int l = warp; l < R; l += TD_W) {
+            const int i = l * TD_C + cr;
+            if (i <= j || i >= n) continue;
+            const int ii = i - j - 1;
+            const double vi = vj[ii], wi = wf[ii];
+            double* a = rows + (size_t)l * n + j + 1;
+            const bool pub = i == j + 2;  // the next look-ahead row
+            double* rbn = rb + nxt * np - 1;
+            double s0 = 0.0, s1 = 0.0;
+            // two elements per lane per trip, loads first (vn[-1] is never used:
+            // column j+1 of the update does not enter p_{j+1})
+            for (int k0 = lane; k0 < m; k0 += 64) {
+                const int k1 = k0 + 32;
+                const bool h1 = k1 < m;
+                const double a0 = a[k0], v0 = vj[k0], w0 = wf[k0], n0 = k0 >= 1 ? vn[k0 - 1] : 0.0;
+                const double a1 = h1 ? a[k1] : 0.0, v1 = h1 ? vj[k1] : 0.0, w1 = h1 ? wf[k1] : 0.0;
+                const double n1 = h1 ? vn[k1 - 1] : 0.0;
+                const double x0 = fma(-wi, v0, fma(-vi, w0, a0));
+                const double x1 = fma(-wi, v1, fma(-vi, w1, a1));
+                a[k0] = x0;
+                s0 = fma(x0, n0, s0);
+                if (h1) {
+                    a[k1] = x1;
+                    s1 = fma(x1, n1, s1);
+                }
+                if (pub) {
+                    if (k0 >= 1) rbn[k0] = x0;
+                    if (h1) rbn[k1] = x1;
                 }
             }
-            __syncthreads();
-            const double scal = sc[2];
-            const bool nontriv = sc[3] != 0.0;
-            for (int k = tid; k < len; k += TD_T) {
-                const double v = k == 0 ? 1.0 : (nontriv ? rr[1 + k] * scal : 0.0);
-                vl[k] = v;
-                if (cr == 0 && k > 0) Q[(size_t)(j + 2 + k) + (size_t)(j + 1) * n] = v;
+            if (i >= j + 2) {
+                const double pv = tn * warp_sum_d(s0 + s1);
+                if (lane == 0) {
+                    pb[nxt * np + (i - j - 2)] = pv;
+                    kacc = fma(pv, vn[i - j - 2], kacc);
+                }
             }
-            __syncthreads();
-        } else if (cr == 0 && tid == 0) {
-            d[n - 1] = rr[0];
-            Q[(size_t)(n - 1) + (size_t)(n - 1) * n] = rr[0];
         }
+        if (lane == 0) red[warp] = kacc;
+        __syncthreads();
+        if (warp == 0) {
+            const double s1 = warp_sum_d(lane < TD_W ? red[lane] : 0.0);
+            if (lane == 0) kb[nxt] = s1;
+        }
+        tcur = tn;
     }
     cluster_sync();  // no CTA leaves while another may still read its shared memory
 }
@@ -302,14 +362,14 @@ __device__ __forceinline__ int sturm_count(const double* sd, const double* se2, 
     if (fabs(q) <= pivmin) q = -pivmin;
     int c = q < 0.0 ? 1 : 0;
     for (int i = 1; i < n; ++i) {
-        q = sd[i] - x - se2[i - 1] / q;
+        q = sd[i] - x - se2[i - 1] * rcp_nr(q);  // |q| > pivmin >= DBL_MIN: normal
         if (fabs(q) <= pivmin) q = -pivmin;
         c += q < 0.0 ? 1 : 0;
     }
     return c;
 }
 
-constexpr int BS_WARPS = 8;
+constexpr int BS_WARPS = 2;  // small blocks: the 480-odd warps spread over all SMs
 constexpr int BS_PTS = 4;  // trial points per lane (independent Sturm chains)
 
 // w[k] = k-th smallest eigenvalue of T (d, e), one warp per k, 32 x BS_PTS
@@ -365,7 +425,7 @@ __global__ void __launch_bounds__(32 * BS_WARPS) k_tri_bisect(const double* __re
             const double di = sd[i], ei = se2[i - 1];
 #pragma unroll
             for (int u = 0; u < BS_PTS; ++u) {
-                q[u] = di - x[u] - ei / q[u];
+                q[u] = di - x[u] - ei * rcp_nr(q[u]);  // |q| > pivmin >= DBL_MIN: normal
                 if (fabs(q[u]) <= pivmin) q[u] = -pivmin;
                 c[u] += q[u] < 0.0 ? 1 : 0;
             }
@@ -462,7 +522,7 @@ __global__ void __launch_bounds__(32 * IV_WARPS) k_tri_invit(const double* __res
                         const double bn = r + 1 < IV_RPL ? y[r + 1] : bnext;
                         double ud, v1, v2, rf;
                         if (fabs(D) >= fabs(sub)) {  // pivot on the current row
-                            const double f = D != 0.0 ? sub / D : 0.0;
+                            const double f = fabs(D) >= DBL_MIN ? sub * rcp_nr(D) : (D != 0.0 ? sub / D : 0.0);
                             ud = D;
                             v1 = C1;
                             v2 = 0.0;
@@ -471,7 +531,7 @@ __global__ void __launch_bounds__(32 * IV_WARPS) k_tri_invit(const double* __res
                             C1 = up;
                             R = bn - f * R;
                         } else {  // interchange: the next row is the pivot
-                            const double f = D / sub;
+                            const double f = fabs(sub) >= DBL_MIN ? D * rcp_nr(sub) : D / sub;
                             ud = sub;
                             v1 = dn;
                             v2 = up;
@@ -481,7 +541,7 @@ __global__ void __launch_bounds__(32 * IV_WARPS) k_tri_invit(const double* __res
                             R = R - f * bn;
                         }
                         if (fabs(ud) < tol) ud = copysign(tol, ud);
-                        ri[r] = 1.0 / ud;
+                        ri[r] = fabs(ud) >= DBL_MIN ? rcp_nr(ud) : 1.0 / ud;
                         u1[r] = v1;
                         u2[r] = v2;
                         y[r] = rf;
@@ -495,7 +555,7 @@ __global__ void __launch_bounds__(32 * IV_WARPS) k_tri_invit(const double* __res
             if (fabs(D) < tol) D = copysign(tol, D);
             const int ln = (n - 1) / IV_RPL, rn = (n - 1) - ln * IV_RPL;
             // back substitution in reverse lane order, carrying y(i+1), y(i+2)
-            double y1 = R / D, y2 = 0.0;
+            double y1 = R * rcp_nr(D), y2 = 0.0;  // |D| >= tol
             for (int l = ln; l >= 0; --l) {
                 if (lane == l) {
 #pragma unroll
