@@ -310,10 +310,11 @@ __global__ void __launch_bounds__(VT) k_cg_upd2(CGVec<T> v, long ld, long n, CGS
             G::load(v.x + off + i, x);
             G::load(v.p + off + i, p);
 #pragma unroll
-            for (int q = 0; q < W; ++q) x[q] = u11 * x[q] + u21 * p[q];
+            for (int q = 0; q < W; ++q) x[q] = cg_upd2_elem(x[q], p[q], u11, u21);
             G::store(v.x + off + i, x);
         } else {
-            for (int q = 0; q < W && i + q < n; ++q) v.x[off + i + q] = u11 * v.x[off + i + q] + u21 * v.p[off + i + q];
+            for (int q = 0; q < W && i + q < n; ++q)
+                v.x[off + i + q] = cg_upd2_elem(v.x[off + i + q], v.p[off + i + q], u11, u21);
         }
     }
 }
@@ -326,6 +327,7 @@ __global__ void s_init(CGScal s, int nb) {
     s.gkgk[b] = 0.0;
     s.active[b] = 1;
     s.reject[b] = 0;
+    s.pend[b] = 0;
     s.res[b] = 0.0;
 }
 
@@ -426,12 +428,17 @@ __global__ void s_eig(CGScal s, int nb) {
 
 __global__ void s_rej(CGScal s, int nb) {  // cg_module.f90:359-365
     int b = blockIdx.x * blockDim.x + threadIdx.x;
-    if (b >= nb || !s.active[b]) return;
+    if (b >= nb) return;
+    if (!s.active[b]) {
+        s.pend[b] = 0;
+        return;
+    }
     s.reject[b] = 0;
     if (s.rb[b] / s.res[b] > 1e8) {
         s.E[b] = s.E1[b];
         s.reject[b] = 1;
     }
+    s.pend[b] = !s.reject[b];
 }
 
 template <typename T>
@@ -518,8 +525,8 @@ static int cg_run(T* x, long ld, int mb, int spin, double* esp, double* res, int
     double* ss = scal + 20 * mb;                 // s-step Gram / g-dot slots, SS_STRIDE per band
     double* cz = ss + (size_t)SS_STRIDE * mb;    // s-step coefficients, SS_MAXM per band
     int* flags = nullptr;
-    RS_CHECK(workspace_t("cg_flags", (size_t)mb * 3, &flags));
-    s.active = flags; s.pc_active = flags + mb; s.reject = flags + 2 * mb;
+    RS_CHECK(workspace_t("cg_flags", (size_t)mb * 4, &flags));
+    s.active = flags; s.pc_active = flags + mb; s.reject = flags + 2 * mb; s.pend = flags + 3 * mb;
     double* part = nullptr;
     RS_CHECK(workspace_t("cg_part", (size_t)mb * nchunk * 8, &part));
 
@@ -543,16 +550,17 @@ static int cg_run(T* x, long ld, int mb, int spin, double* esp, double* res, int
     finish(1, dV, s.rb, nullptr);
     RS_LAUNCH();
 
+    const bool sstep = ipc == 4 && mloop >= 1 && mloop <= SS_MAXM;
     for (int icg = 1; icg <= ncg + 1; ++icg) {
         const int last = icg == ncg + 1;
         launch(s_top, sb, 128, 0, st, s, mb, last);
         if (last) break;
-        if (ipc == 4 && mloop >= 1 && mloop <= SS_MAXM) {
+        if (sstep) {
             // --- preconditioner, rb = <Pg|g> dV and the search direction p
             // in mloop + 2 passes (s-step form; w_j in r, q, Pg, hp, which
             // are free until hpsi(p))
             const SSVec<T> sv{{v.r, v.q, v.Pg, v.hp}};
-            RS_CHECK(sstep_precond<T>(v.g, sv, v.p, ld, mb, mloop, icg == 1, s, ss, cz, part, pa, dV));
+            RS_CHECK(sstep_precond<T>(v.g, sv, v.p, x, ld, mb, mloop, icg == 1, s, ss, cz, part, pa, dV));
         } else {
             // --- preconditioning (Pgk = gk on entry)
             if (ipc == 4 && mloop > 0) {
@@ -594,7 +602,13 @@ static int cg_run(T* x, long ld, int mb, int spin, double* esp, double* res, int
         launch(k_cg_upd1<T>, vg, VT, 0, st, v, ld, n, s, part, s.active, gv);
         finish(1, dV, s.rb, s.active);
         launch(s_rej, sb, 128, 0, st, s, mb);
-        launch(k_cg_upd2<T>, vg, VT, 0, st, v, ld, n, s, s.active, gv);
+        // s-step form: the x update waits for the next search-direction pass,
+        // which reads the old p anyway
+        if (!sstep) launch(k_cg_upd2<T>, vg, VT, 0, st, v, ld, n, s, s.active, gv);
+        RS_LAUNCH();
+    }
+    if (sstep) {  // the last step's update
+        launch(k_cg_upd2<T>, vg, VT, 0, st, v, ld, n, s, (const int*)s.pend, gv);
         RS_LAUNCH();
     }
     RS_CUDA(cudaMemcpyAsync(esp, s.E, sizeof(double) * mb, cudaMemcpyDeviceToDevice, st));

@@ -43,7 +43,15 @@ inline bool grp16_ok(long ld, std::initializer_list<const void*> ptrs) {
 struct CGScal {
     double *E, *E1, *rb, *gkgk, *res, *u11, *u21, *W, *rr0, *rr1, *pa, *pb, *bk, *dots;
     int *active, *pc_active, *reject;
+    int* pend;  // x = u11 x + u21 p still to be applied (s-step form: by the next p pass)
 };
+
+// x = u11 x + u21 p (cg_module.f90:366-369), shared by the plain update and
+// the one folded into the next search-direction pass so both give the same bits
+template <typename T>
+__device__ __forceinline__ T cg_upd2_elem(T x, T p, T u11, T u21) {
+    return fma(u11, x, u21 * p);
+}
 
 template <typename T>
 struct CGVec {
@@ -137,7 +145,7 @@ __device__ __forceinline__ T pc_offdiag(const T* __restrict__ f, long i, int i1,
 // ss and cz hold SS_STRIDE and SS_MAXM doubles per band, part the per-CTA
 // partial sums (mb x nchunk x 8 doubles).
 template <typename T>
-int sstep_precond(const T* g, const SSVec<T>& sv, T* p, long ld, int mb, int mloop, int first, const CGScal& s,
+int sstep_precond(const T* g, const SSVec<T>& sv, T* p, T* x, long ld, int mb, int mloop, int first, const CGScal& s,
                   double* ss, double* cz, double* part, const PcArgs& pa, double dV);
 
 }  // namespace rsdft

@@ -352,27 +352,36 @@ __global__ void __launch_bounds__(U_THREADS, 1) k_umma(const __grid_constant__ U
                     for (int j = 0; j < 32; ++j) acc[c0 + j] += (double)__uint_as_float(r[j]);
                 }
             } else {
-                const int n = tm * UB_M + row;  // output column (A row)
+                // 32 x 32 blocks (TMEM lane = band, column = grid point) transposed
+                // in registers by a shuffle butterfly, so that each store
+                // instruction writes 32 consecutive grid points of one band
+                const int n0 = tm * UB_M + 32 * q;  // first band of this warp's block
 #pragma unroll
                 for (int c0 = 0; c0 < CW; c0 += 32) {
                     uint32_t r[32];
                     tmem_ld_x32(tq + (uint32_t)(b * BN + h * CW + c0), r);
                     tmem_ld_wait();
-                    if (n < g.mrows) {
-                        const int i0 = tn * BN + h * CW + c0;
-                        double* o = g.out + (size_t)n * g.ldo + i0;
-                        if (i0 + 32 <= g.nrows) {
 #pragma unroll
-                            for (int j = 0; j < 32; j += 2) {
-                                double2 v;
-                                v.x = (double)__uint_as_float(r[j]);
-                                v.y = (double)__uint_as_float(r[j + 1]);
-                                *reinterpret_cast<double2*>(o + j) = v;
-                            }
-                        } else {
-                            for (int j = 0; j < 32; ++j)
-                                if (i0 + j < g.nrows) o[j] = (double)__uint_as_float(r[j]);
+                    for (int sft = 16; sft >= 1; sft >>= 1) {
+                        const bool upper = (lane & sft) != 0;
+#pragma unroll
+                        for (int j = 0; j < 32; ++j) {
+                            if (j & sft) continue;
+                            const uint32_t send = upper ? r[j] : r[j + sft];
+                            const uint32_t recv = __shfl_xor_sync(0xffffffffu, send, sft);
+                            if (upper)
+                                r[j] = recv;
+                            else
+                                r[j + sft] = recv;
                         }
+                    }
+                    // lane: grid point i0 + lane; r[j]: band n0 + j
+                    const int i = tn * BN + h * CW + c0 + lane;
+                    if (i < g.nrows) {
+                        double* o = g.out + (size_t)n0 * g.ldo + i;
+#pragma unroll
+                        for (int j = 0; j < 32; ++j)
+                            if (n0 + j < g.mrows) o[(size_t)j * g.ldo] = (double)__uint_as_float(r[j]);
                     }
                 }
             }

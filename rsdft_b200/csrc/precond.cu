@@ -140,23 +140,41 @@ __global__ void s_sstep(CGScal s, const double* __restrict__ ss, double* __restr
 
 // p = g + sum_j cz_j w_j (+ bk p after the first step)
 template <typename T>
-__global__ void __launch_bounds__(VT) k_ss_p(const T* __restrict__ g, SSVec<T> sv, T* __restrict__ p, long ld,
-                                             long n, const double* __restrict__ cz, const double* __restrict__ bk_,
-                                             int m, int first, const int* __restrict__ active, int vec) {
+__global__ void __launch_bounds__(VT) k_ss_p(const T* __restrict__ g, SSVec<T> sv, T* __restrict__ p,
+                                             T* __restrict__ x, long ld, long n, const double* __restrict__ cz,
+                                             const double* __restrict__ bk_, int m, int first,
+                                             const int* __restrict__ active, const int* __restrict__ pend,
+                                             const double* __restrict__ u11_, const double* __restrict__ u21_,
+                                             int vec) {
     using G = Grp16<T>;
     constexpr int W = G::W;
     const int b = blockIdx.y;
-    if (active && !active[b]) return;
+    const bool act = !active || active[b];
+    const bool upd = pend && pend[b];  // the previous step's x update, which needs the old p
+    if (!act && !upd) return;
     const long off = (long)b * ld, base = (long)blockIdx.x * VCHUNK;
     T c[SS_MAXM];
 #pragma unroll
     for (int j = 0; j < SS_MAXM; ++j) c[j] = (T)cz[(long)b * SS_MAXM + j];
     const T bk = (T)bk_[b];
+    const T u11 = upd ? (T)u11_[b] : (T)0, u21 = upd ? (T)u21_[b] : (T)0;
 #pragma unroll 2
     for (int it = 0; it < VITEMS / W; ++it) {
         const long i = base + ((long)it * VT + threadIdx.x) * W;
         if (vec && i + W <= n) {
             T pg[W], t[W];
+            if (upd || !first) G::load(p + off + i, t);
+            if (upd) {
+                T xv[W];
+                G::load(x + off + i, xv);
+#pragma unroll
+                for (int q = 0; q < W; ++q) xv[q] = cg_upd2_elem(xv[q], t[q], u11, u21);
+                G::store(x + off + i, xv);
+            }
+            if (!act) continue;
+            T pn[W];
+#pragma unroll
+            for (int q = 0; q < W; ++q) pn[q] = t[q];
             G::load(g + off + i, pg);
 #pragma unroll
             for (int j = 0; j < SS_MAXM; ++j) {
@@ -167,18 +185,21 @@ __global__ void __launch_bounds__(VT) k_ss_p(const T* __restrict__ g, SSVec<T> s
                 }
             }
             if (!first) {
-                G::load(p + off + i, t);
 #pragma unroll
-                for (int q = 0; q < W; ++q) pg[q] += bk * t[q];
+                for (int q = 0; q < W; ++q) pg[q] += bk * pn[q];
             }
             G::store(p + off + i, pg);
         } else {
             for (int q = 0; q < W && i + q < n; ++q) {
-                T pg = g[off + i + q];
+                const long k = off + i + q;
+                const T po = (upd || !first) ? p[k] : (T)0;
+                if (upd) x[k] = cg_upd2_elem(x[k], po, u11, u21);
+                if (!act) continue;
+                T pg = g[k];
 #pragma unroll
                 for (int j = 0; j < SS_MAXM; ++j)
-                    if (j < m) pg += c[j] * sv.w[j][off + i + q];
-                p[off + i + q] = first ? pg : pg + bk * p[off + i + q];
+                    if (j < m) pg += c[j] * sv.w[j][k];
+                p[k] = first ? pg : pg + bk * po;
             }
         }
     }
@@ -604,7 +625,7 @@ static int pc_tma_dispatch(int K, bool store, const T* g, const SSVec<T>& sv, co
 }
 
 template <typename T>
-int sstep_precond(const T* g, const SSVec<T>& sv, T* p, long ld, int mb, int mloop, int first, const CGScal& s,
+int sstep_precond(const T* g, const SSVec<T>& sv, T* p, T* x, long ld, int mb, int mloop, int first, const CGScal& s,
                   double* ss, double* cz, double* part, const PcArgs& pa, double dV) {
     const Context& c = ctx();
     cudaStream_t st = c.stream;
@@ -635,15 +656,16 @@ int sstep_precond(const T* g, const SSVec<T>& sv, T* p, long ld, int mb, int mlo
         finish_to(D, out, nch);
     }
     launch(s_sstep, sb, 128, 0, st, s, ss, cz, mb, mloop, pa.d, dV, first);
-    const int gv = grp16_ok<T>(ld, {g, p, sv.w[0], sv.w[1], sv.w[2], sv.w[3]}) ? 1 : 0;
-    launch(k_ss_p<T>, vg, VT, 0, st, g, sv, p, ld, n, cz, s.bk, mloop, first, s.active, gv);
+    const int gv = grp16_ok<T>(ld, {g, p, x, sv.w[0], sv.w[1], sv.w[2], sv.w[3]}) ? 1 : 0;
+    launch(k_ss_p<T>, vg, VT, 0, st, g, sv, p, x, ld, n, cz, s.bk, mloop, first, s.active,
+           (const int*)(first ? nullptr : s.pend), (const double*)s.u11, (const double*)s.u21, gv);
     RS_LAUNCH();
     return RSDFT_OK;
 }
 
-template int sstep_precond<double>(const double*, const SSVec<double>&, double*, long, int, int, int, const CGScal&,
-                                   double*, double*, double*, const PcArgs&, double);
-template int sstep_precond<float>(const float*, const SSVec<float>&, float*, long, int, int, int, const CGScal&,
-                                  double*, double*, double*, const PcArgs&, double);
+template int sstep_precond<double>(const double*, const SSVec<double>&, double*, double*, long, int, int, int,
+                                   const CGScal&, double*, double*, double*, const PcArgs&, double);
+template int sstep_precond<float>(const float*, const SSVec<float>&, float*, float*, long, int, int, int,
+                                  const CGScal&, double*, double*, double*, const PcArgs&, double);
 
 }  // namespace rsdft
