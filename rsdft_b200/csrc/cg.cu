@@ -328,6 +328,7 @@ __global__ void s_init(CGScal s, int nb) {
     s.active[b] = 1;
     s.reject[b] = 0;
     s.pend[b] = 0;
+    if (b == 0) *s.rej_any = 0;
     s.res[b] = 0.0;
 }
 
@@ -437,6 +438,7 @@ __global__ void s_rej(CGScal s, int nb) {  // cg_module.f90:359-365
     if (s.rb[b] / s.res[b] > 1e8) {
         s.E[b] = s.E1[b];
         s.reject[b] = 1;
+        *s.rej_any = 1;
     }
     s.pend[b] = !s.reject[b];
 }
@@ -525,8 +527,9 @@ static int cg_run(T* x, long ld, int mb, int spin, double* esp, double* res, int
     double* ss = scal + 20 * mb;                 // s-step Gram / g-dot slots, SS_STRIDE per band
     double* cz = ss + (size_t)SS_STRIDE * mb;    // s-step coefficients, SS_MAXM per band
     int* flags = nullptr;
-    RS_CHECK(workspace_t("cg_flags", (size_t)mb * 4, &flags));
+    RS_CHECK(workspace_t("cg_flags", (size_t)mb * 4 + 1, &flags));
     s.active = flags; s.pc_active = flags + mb; s.reject = flags + 2 * mb; s.pend = flags + 3 * mb;
+    s.rej_any = flags + 4 * mb;
     double* part = nullptr;
     RS_CHECK(workspace_t("cg_part", (size_t)mb * nchunk * 8, &part));
 
@@ -617,7 +620,7 @@ static int cg_run(T* x, long ld, int mb, int spin, double* esp, double* res, int
 }
 
 int cg_device_f32(const double* unk, long ld, int mb, int spin, double* esp, double* res, int ncg, int mloop,
-                  int ipc, float** x32_out) {
+                  int ipc, float** x32_out, const float** hx_out) {
     Context& c = ctx();
     float* x32 = nullptr;
     const long n = ld * (long)mb;
@@ -626,6 +629,19 @@ int cg_device_f32(const double* unk, long ld, int mb, int spin, double* esp, dou
     RS_LAUNCH();
     RS_CHECK(cg_run<float>(x32, ld, mb, spin, esp, res, ncg, mloop, ipc));
     *x32_out = x32;
+    if (hx_out) {
+        // the sweep's H x: the CG keeps hx = H x through its updates, except
+        // for a band whose update was rejected (cg_module.f90:359-365)
+        *hx_out = nullptr;
+        float* hx = nullptr;
+        int* flags = nullptr;
+        RS_CHECK(workspace_t("cg_vec", (size_t)ld * mb * 7, &hx));
+        RS_CHECK(workspace_t("cg_flags", (size_t)mb * 4 + 1, &flags));
+        int rej = 1;
+        RS_CUDA(cudaMemcpyAsync(&rej, flags + 4 * mb, sizeof(int), cudaMemcpyDeviceToHost, c.stream));
+        RS_CUDA(cudaStreamSynchronize(c.stream));
+        if (rej == 0) *hx_out = hx;
+    }
     return RSDFT_OK;
 }
 

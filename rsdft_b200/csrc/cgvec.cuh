@@ -43,7 +43,8 @@ inline bool grp16_ok(long ld, std::initializer_list<const void*> ptrs) {
 struct CGScal {
     double *E, *E1, *rb, *gkgk, *res, *u11, *u21, *W, *rr0, *rr1, *pa, *pb, *bk, *dots;
     int *active, *pc_active, *reject;
-    int* pend;  // x = u11 x + u21 p still to be applied (s-step form: by the next p pass)
+    int* pend;     // x = u11 x + u21 p still to be applied (s-step form: by the next p pass)
+    int* rej_any;  // set when any band's update was rejected (its hx then no longer equals H x)
 };
 
 // x = u11 x + u21 p (cg_module.f90:366-369), shared by the plain update and

@@ -294,19 +294,24 @@ int orth_subspace_diag_device(double* psi, long ld, int mb, int spin, double* es
 // The same step on the FP32 bands of a mixed CG sweep: FP32 H psi, BF16
 // split from FP32 (exact), rotated bands written in FP64 to psi.  An
 // ill-conditioned overlap converts x32 to psi and takes the explicit path.
-int orth_subspace_diag_f32(const float* x32, double* psi, long ld, int mb, int spin, double* esp, int mode) {
+int orth_subspace_diag_f32(const float* x32, const float* hx, double* psi, long ld, int mb, int spin, double* esp,
+                           int mode) {
     Context& c = ctx();
     float* h32 = nullptr;
     double *S = nullptr, *H = nullptr, *T = nullptr, *mm = nullptr;
     int* dinfo = nullptr;
-    RS_CHECK(workspace_t("sub_h32", (size_t)ld * mb, &h32));
     RS_CHECK(workspace_t("gs_S", (size_t)mb * mb, &S));
     RS_CHECK(workspace_t("sub_H", (size_t)mb * mb, &H));
     RS_CHECK(workspace_t("osd_T", (size_t)mb * mb, &T));
     RS_CHECK(workspace_t("osd_minmax", 2, &mm));
     RS_CHECK(workspace_t("gs_info", 4, &dinfo));
     const double zero = 0.0, one = 1.0;
-    RS_CHECK(hpsi_device<float>(x32, h32, ld, mb, spin, nullptr));
+    if (hx) {
+        h32 = const_cast<float*>(hx);
+    } else {
+        RS_CHECK(workspace_t("sub_h32", (size_t)ld * mb, &h32));
+        RS_CHECK(hpsi_device<float>(x32, h32, ld, mb, spin, nullptr));
+    }
     const void* split = nullptr;
     RS_CHECK(gram_mixed_pair(x32, h32, ld, mb, c.dV, mode_terms(mode), S, H, &split));
     int lwork = 0;
@@ -478,8 +483,9 @@ int rsdft_gpu_eigensolver_sweep(int k, int s, double* unk, long ld, int mb, doub
         RS_CHECK(orth_subspace_diag_device(d, ld, mb, s, W, mode));
     } else {
         float* x32 = nullptr;
-        RS_CHECK(cg_device_f32(d, ld, mb, s, W, R, ncg, mloop, ipc, &x32));
-        RS_CHECK(orth_subspace_diag_f32(x32, d, ld, mb, s, W, mode));
+        const float* hx = nullptr;
+        RS_CHECK(cg_device_f32(d, ld, mb, s, W, R, ncg, mloop, ipc, &x32, &hx));
+        RS_CHECK(orth_subspace_diag_f32(x32, hx, d, ld, mb, s, W, mode));
     }
     RS_CHECK(stage_out(esp, W, sizeof(double) * mb));
     RS_CHECK(stage_out(res, R, sizeof(double) * mb));

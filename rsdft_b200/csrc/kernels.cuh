@@ -63,13 +63,17 @@ int subspace_diag_device(double* psi, long ld, int mb, int spin, double* esp_dev
 int orth_subspace_diag_device(double* psi, long ld, int mb, int spin, double* esp_dev, int mode);
 
 // Mixed forms: the CG sweep on an FP32 copy of unk, left in the workspace
-// (*x32_out, leading dimension ld) for orth_subspace_diag_f32.
+// (*x32_out, leading dimension ld) for orth_subspace_diag_f32.  hx_out (if
+// given) receives the sweep's H x32 (in the CG workspace), or null when an
+// update was rejected and H x must be formed again.
 int cg_device_f32(const double* unk, long ld, int mb, int spin, double* esp, double* res, int ncg, int mloop,
-                  int ipc, float** x32_out);
+                  int ipc, float** x32_out, const float** hx_out = nullptr);
 
-// Gram-Schmidt + Rayleigh-Ritz of FP32 bands x32; the rotated bands are
-// written to psi (FP64).  Mixed forms only.
-int orth_subspace_diag_f32(const float* x32, double* psi, long ld, int mb, int spin, double* esp_dev, int mode);
+// Gram-Schmidt + Rayleigh-Ritz of FP32 bands x32 (h32 = H x32 if already
+// known, else null); the rotated bands are written to psi (FP64).  Mixed
+// forms only.
+int orth_subspace_diag_f32(const float* x32, const float* h32, double* psi, long ld, int mb, int spin,
+                           double* esp_dev, int mode);
 
 // Eigen-decomposition of the symmetric n x n A (column-major, ld n; the
 // `uplo` triangle is read): W ascending, A overwritten by the eigenvectors.

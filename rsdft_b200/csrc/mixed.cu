@@ -460,7 +460,7 @@ static int launch_umma(const UmmaMaps& maps, const UmmaArgs& g, dim3 grid) {
 // Gram matrix from BF16 slices (ML x nb each, 3 slices): C = alpha sa^T sb,
 // symmetric tile pairs only when same.
 static int gram_from_slices(__nv_bfloat16* sa, __nv_bfloat16* sb, bool same, int nb, double alpha, int symmetrize,
-                            int nterms, double* C) {
+                            int nterms, double* C, bool upper_only = false) {
     Context& c = ctx();
     const long ml = c.ml;
     UmmaMaps maps;
@@ -469,8 +469,12 @@ static int gram_from_slices(__nv_bfloat16* sa, __nv_bfloat16* sb, bool same, int
     UmmaArgs g{};
     g.kblocks = (int)((ml + UB_K - 1) / UB_K);
     g.ntm = g.ntn = (nb + UB_M - 1) / UB_M;
-    g.sym = same ? 1 : 0;
-    g.npairs = same ? g.ntm * (g.ntm + 1) / 2 : g.ntm * g.ntn;
+    // tile pairs tm <= tn only when the product is symmetric: A^T A, or (with
+    // upper_only) A^T B for a symmetric operator B = H A, whose lower tiles
+    // equal the transposed upper ones
+    const bool sym = same || upper_only;
+    g.sym = sym ? 1 : 0;
+    g.npairs = sym ? g.ntm * (g.ntm + 1) / 2 : g.ntm * g.ntn;
     const int sms = c.num_sms > 0 ? c.num_sms : 148;
     int nsplit = std::max(1, sms / g.npairs);
     nsplit = std::min(nsplit, g.kblocks);
@@ -526,7 +530,9 @@ static int gram_pair(const TI* psi, const TI* hpsi, long ld, int nb, double alph
     RS_CHECK(split_cols(hpsi, ld, nb, "umma_sb", &sb));
     if (psi_split) *psi_split = sa;
     RS_CHECK(gram_from_slices(sa, sa, true, nb, alpha, 0, nterms, S));
-    return gram_from_slices(sa, sb, false, nb, alpha, 1, nterms, H);
+    // psi^T (H psi) is symmetric: the upper tile pairs, the diagonal tiles
+    // symmetrised (subspace_mate_sl likewise forms one triangle)
+    return gram_from_slices(sa, sb, false, nb, alpha, 1, nterms, H, true);
 }
 
 int gram_mixed_pair(const double* psi, const double* hpsi, long ld, int nb, double alpha, int nterms, double* S,

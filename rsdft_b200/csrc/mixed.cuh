@@ -13,8 +13,10 @@ namespace rsdft {
 int gram_mixed(const double* A, const double* B, long ld, int nb, double alpha, int symmetrize, int nterms,
                double* C, const void** a_split = nullptr);
 
-// S = alpha psi^T psi and H = alpha/2 (psi^T Hpsi + Hpsi^T psi) from one
-// split of each operand; psi_split as a_split above.
+// S = alpha psi^T psi and H = alpha psi^T Hpsi from one split of each
+// operand, for a symmetric operator (psi^T Hpsi symmetric): only the tile
+// pairs on and above the diagonal are formed, the lower ones mirrored and the
+// diagonal tiles symmetrised.  psi_split as a_split above.
 int gram_mixed_pair(const double* psi, const double* hpsi, long ld, int nb, double alpha, int nterms, double* S,
                     double* H, const void** psi_split = nullptr);
 // the same from FP32 blocks (the split of an FP32 value is exact)
