@@ -120,6 +120,9 @@ WORKLOADS = {
     # small cells for dense-matrix and finite-difference checks
     "si8_g12": Workload("si8_g12", 1, 12, 16, 8, 0.03, 1006),
     "si8_g16": Workload("si8_g16", 1, 16, 24, 12, 0.03, 1007),
+    # ML = 18^3 = 5832 (a multiple of 8, not of 32) and 36 bands (not a
+    # multiple of 8): the general-shape paths of the mixed contractions
+    "si8_g18": Workload("si8_g18", 1, 18, 36, 16, 0.03, 1008),
 }
 
 

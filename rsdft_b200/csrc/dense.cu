@@ -215,6 +215,17 @@ __global__ void k_diag_minmax(const double* __restrict__ a, int n, int lda, doub
     }
 }
 
+// Largest (max diag R / min diag R)^2 of the overlap's Cholesky factor for
+// which the one-step Rayleigh-Ritz is kept.  The eigenvalue error of the
+// R^-T H R^-1 form grows with the overlap's condition, and the Gram matrices'
+// own error with the precision form: FP64 1e3, 3-term split-BF16 1e2, 2-term
+// (~16 significant bits) 1e1 (measured: an overlap with diag ratio^2 93 and
+// condition 2.4e3 gave 6.5e-4 relative eigenvalue error in the 2-term form,
+// 3e-6 in the 3-term form).
+static double fused_rr_kappa_max(int mode) {
+    return mode == RSDFT_MODE_FP64 ? 1e3 : (mode == RSDFT_MODE_MIXED_BF16 ? 1e2 : 1e1);
+}
+
 // Gram-Schmidt followed by subspace_diag (the pair calc_sweep calls,
 // sweep_module.f90:152-155) as one Rayleigh-Ritz step on the CG output:
 //   S = dV psi^T psi = R^T R,  H = dV sym(psi^T H psi),
@@ -223,7 +234,7 @@ __global__ void k_diag_minmax(const double* __restrict__ a, int n, int lda, doub
 // the eigenpairs and the rotated bands are those of the pair, with one
 // overlap Cholesky, one eigensolve and one tall rotation instead of two
 // CholeskyQR passes, the eigensolve and a separate rotation.  When the
-// overlap is ill-conditioned (diag(R) spread beyond kappa_max^(1/2); one
+// overlap is ill-conditioned (diag(R) spread beyond fused_rr_kappa_max^(1/2); one
 // Cholesky pass then loses orthogonality), the explicit CholeskyQR2 +
 // subspace_diag path runs instead.
 int orth_subspace_diag_device(double* psi, long ld, int mb, int spin, double* esp, int mode) {
@@ -256,8 +267,7 @@ int orth_subspace_diag_device(double* psi, long ld, int mb, int spin, double* es
     double hmm[2] = {0.0, 0.0};
     RS_CUDA(cudaMemcpyAsync(hmm, mm, sizeof(hmm), cudaMemcpyDeviceToHost, c.stream));
     RS_CUDA(cudaStreamSynchronize(c.stream));
-    const double kappa_max = mode == RSDFT_MODE_FP64 ? 1e3 : 1e2;
-    if (!(hmm[0] > 0.0) || (hmm[1] / hmm[0]) * (hmm[1] / hmm[0]) > kappa_max) {
+    if (!(hmm[0] > 0.0) || (hmm[1] / hmm[0]) * (hmm[1] / hmm[0]) > fused_rr_kappa_max(mode)) {
         RS_CHECK(gram_schmidt_device(psi, ld, mb, mode));
         return subspace_diag_device(psi, ld, mb, spin, esp, mode);
     }
@@ -325,7 +335,7 @@ int orth_subspace_diag_f32(const float* x32, const float* hx, double* psi, long 
     double hmm[2] = {0.0, 0.0};
     RS_CUDA(cudaMemcpyAsync(hmm, mm, sizeof(hmm), cudaMemcpyDeviceToHost, c.stream));
     RS_CUDA(cudaStreamSynchronize(c.stream));
-    if (!(hmm[0] > 0.0) || (hmm[1] / hmm[0]) * (hmm[1] / hmm[0]) > 1e2) {
+    if (!(hmm[0] > 0.0) || (hmm[1] / hmm[0]) * (hmm[1] / hmm[0]) > fused_rr_kappa_max(mode)) {
         launch(k_widen, 4 * c.num_sms, 256, 0, c.stream, x32, psi, ld * (long)mb);
         RS_LAUNCH();
         RS_CHECK(gram_schmidt_device(psi, ld, mb, mode));

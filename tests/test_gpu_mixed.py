@@ -129,3 +129,29 @@ def test_mixed_then_fp64_closing_pass(gpu, cells):
     g = host(ub)
     assert np.abs(g.T @ g * c.dV - np.eye(c.nband)).max() <= 1e-12
     assert np.abs(host(ea) - host(eb)).max() <= 1e-5
+
+
+@pytest.mark.parametrize("mode,tol", [(api.MODE_MIXED_BF16, 3e-6), (api.MODE_MIXED_BF16X3, 1e-4)])
+def test_mixed_general_shapes(gpu, cells, mode, tol):
+    """ML = 18^3 (not a multiple of 32: the rotation takes the transposed
+    split; FP32 rows of 18 take the general stencil) and 36 bands (the band
+    dimension padded to 40): Rayleigh-Ritz step and sweep against the oracle."""
+    c, o = prepare(gpu, cells, "si8_g18")
+    nb = c.nband
+    q = o.gram_schmidt_t(np.asfortranarray(c.psi0()))
+    u0, _, _, _ = o.conjugate_gradient(q, 4, 3)
+    ref, w, _ = o.subspace_diag_la(o.gram_schmidt_t(u0))
+    u = dev(u0)
+    esp = torch.zeros(nb, dtype=torch.float64, device="cuda")
+    gpu.orth_subspace_diag(1, 1, u, esp, mode=mode)
+    torch.cuda.synchronize()
+    g = host(u)
+    assert np.abs(host(esp) - w).max() <= tol * max(1.0, np.abs(w).max())
+    assert np.abs(g.T @ g * c.dV - np.eye(nb)).max() <= 10 * tol
+    ub = dev(q)
+    eb = torch.zeros(nb, dtype=torch.float64, device="cuda")
+    rb = torch.zeros_like(eb)
+    gpu.eigensolver_sweep(1, 1, ub, eb, rb, ncg=4, mloop=3, mode=mode)
+    torch.cuda.synchronize()
+    # FP32 CG sweep: eigenvalue estimates to ~1e-5 of the FP64 sequence
+    assert np.abs(host(eb) - w).max() <= max(1e-5, tol) * max(1.0, np.abs(w).max())
