@@ -250,6 +250,10 @@ template <int K, bool STORE>
 struct PcStep {
     static constexpr int NA = (K >= 2 ? K - 1 : 0) + (STORE ? 0 : 1);  // w_0..w_{K-2}, then g
     static constexpr int D = K == 0 ? 1 : (STORE ? K + 1 : 2 * K);
+    // CTAs per SM: the first two steps have no epilogue operands and few
+    // dots, so two CTAs (<= 85 registers, half the stage ring each) fit and
+    // hide the per-plane latency better
+    static constexpr int CTAS = K <= 1 ? 2 : 1;
 };
 
 __device__ __forceinline__ int pc_pwrap(int i, int n) {
@@ -258,7 +262,8 @@ __device__ __forceinline__ int pc_pwrap(int i, int n) {
 }
 
 template <typename T, int K, bool STORE>
-__global__ void __launch_bounds__(384, 1) k_pc_tma(const __grid_constant__ PcMaps maps, T* __restrict__ wout,
+__global__ void __launch_bounds__(384, PcStep<K, STORE>::CTAS) k_pc_tma(const __grid_constant__ PcMaps maps,
+                                                                      T* __restrict__ wout,
                                                    StencilCoef cf, int n1, int n2, int n3, long ld, int zlen0,
                                                    int nzc, int TY, int RS, int S, int ncw,
                                                    double* __restrict__ part, const int* __restrict__ active,
@@ -508,7 +513,7 @@ struct PcGeom {
 };
 
 template <typename T>
-static PcGeom pc_geometry(int n1, int n2, int na, int d) {
+static PcGeom pc_geometry(int n1, int n2, int na, int d, int ctas) {
     PcGeom best;
     constexpr int VX = 16 / (int)sizeof(T);
     const int RS = (int)((((size_t)n1 * sizeof(T) + 127) / 128) * 128 / sizeof(T));
@@ -521,7 +526,9 @@ static PcGeom pc_geometry(int n1, int n2, int na, int d) {
         if (threads > 384) continue;
         const size_t stage = (size_t)(TY + 2 + na * TY) * RS * sizeof(T);
         const size_t fixed = (size_t)ncw * d * sizeof(double);
-        const int S = (int)std::min<size_t>((220 * 1024 - fixed) / (stage + 16), 8);
+        const size_t budget = (ctas > 1 ? 110 : 220) * 1024;
+        if (budget <= fixed) continue;
+        const int S = (int)std::min<size_t>((budget - fixed) / (stage + 16), 8);
         if (S < 2) continue;
         const double used = (double)((n1 / VX) * (TY / 2)) / threads;
         const double score = 100.0 * TY / (TY + 2) + 10.0 * used + 2.0 * std::min(S, 4);
@@ -548,7 +555,7 @@ static int pc_tma_step(const T* src, const T* const* aux, T* wout, const PcArgs&
     constexpr int NA = PcStep<K, STORE>::NA;
     constexpr int D = PcStep<K, STORE>::D;
     const int n1 = pa.n1, n2 = pa.n2, n3 = pa.n3;
-    const PcGeom g = pc_geometry<T>(n1, n2, NA, D);
+    const PcGeom g = pc_geometry<T>(n1, n2, NA, D, PcStep<K, STORE>::CTAS);
     if (g.TY == 0 || (ld * sizeof(T)) % 16 != 0) return RSDFT_OK;
     if (STORE && reinterpret_cast<uintptr_t>(wout) % 16 != 0) return RSDFT_OK;
     const int sms = c.num_sms > 0 ? c.num_sms : 148;
