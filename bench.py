@@ -9,8 +9,9 @@ Printed JSON line (rank 0):
   value        eigensolver iterations/s of the headline form over all ranks,
                inputs resident in HBM (device-timed with CUDA events)
   e2e          the same through the C ABI with the wavefunction in pinned host
-               memory: every step uploads it, runs the iteration on the
-               registered mirror and downloads it with the eigenvalues
+               memory: every step is one eigensolver_sweep call on the host
+               array, which uploads it (band blocks overlapped with the CG),
+               runs the iteration and downloads it with the eigenvalues
   roofline     hpsi (projection + fused stencil/Vloc/nonlocal kernels) on all
                bands: algorithmic bytes / measured duration vs measured HBM peak
   cpu_baseline the oracle (C/OpenMP + numpy BLAS) on the host cores, a
@@ -356,21 +357,15 @@ def main():
         hn = host.numpy().T  # (ML, MB) Fortran view of pinned memory
         esp_h = np.zeros(MB)
         res_h = np.zeros(MB)
-        g.register_wf(hn)
         mode_e = MODES[head]
         for _ in range(1):
-            g.sync_to_device(hn)
             g.eigensolver_iteration(hn, esp_h, res_h, ncg=args.ncg, mloop=args.mloop, mode=mode_e)
-            g.sync_to_host(hn)
         barrier()
         t0 = time.perf_counter()
         for _ in range(args.steps):
-            g.sync_to_device(hn)
             g.eigensolver_iteration(hn, esp_h, res_h, ncg=args.ncg, mloop=args.mloop, mode=mode_e)
-            g.sync_to_host(hn)
         barrier()
         dt = replicas.max_over_ranks((time.perf_counter() - t0) / args.steps, pg, device="cuda")
-        g.unregister_wf(hn)
         e2e = {"value": replicas.whole_job_rate(1.0, world, dt), "unit": "iter/s", "h2d_bytes_per_step": ML * MB * 8,
                "d2h_bytes_per_step": ML * MB * 8 + 2 * MB * 8}
 

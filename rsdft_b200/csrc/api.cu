@@ -179,6 +179,8 @@ int rsdft_gpu_init(int device) {
     RS_CUDA(cudaDeviceGetAttribute(&c.num_sms, cudaDevAttrMultiProcessorCount, device));
     RS_CUDA(cudaMalloc(&c.err_flag, 16));
     RS_CUDA(cudaMemset(c.err_flag, 0, 16));
+    RS_CUDA(cudaStreamCreateWithFlags(&c.copy_stream, cudaStreamNonBlocking));
+    for (int i = 0; i < Context::NEV; ++i) RS_CUDA(cudaEventCreateWithFlags(&c.ev[i], cudaEventDisableTiming));
     c.device = device;
     c.init = true;
     return RSDFT_OK;
@@ -188,6 +190,16 @@ int rsdft_gpu_finalize(void) {
     Context& c = g_ctx;
     if (!c.init) return RSDFT_OK;
     cudaStreamSynchronize(c.stream);
+    if (c.copy_stream) {
+        cudaStreamSynchronize(c.copy_stream);
+        cudaStreamDestroy(c.copy_stream);
+        c.copy_stream = nullptr;
+    }
+    for (int i = 0; i < Context::NEV; ++i)
+        if (c.ev[i]) {
+            cudaEventDestroy(c.ev[i]);
+            c.ev[i] = nullptr;
+        }
     for (auto& kv : c.ws)
         if (kv.second.p) cudaFree(kv.second.p);
     c.ws.clear();

@@ -645,6 +645,55 @@ int cg_device_f32(const double* unk, long ld, int mb, int spin, double* esp, dou
     return RSDFT_OK;
 }
 
+__global__ void k_or_flag(int* __restrict__ dst, const int* __restrict__ src) {
+    if (*src) *dst = 1;
+}
+
+int cg_device_f32_staged(const double* unk_host, double* unk_dev, long ld, int mb, int spin, double* esp,
+                         double* res, int ncg, int mloop, int ipc, int nchunk, float** x32_out,
+                         const float** hx_out) {
+    Context& c = ctx();
+    nchunk = std::max(1, std::min(nchunk, std::min(mb, Context::NEV)));
+    const int per = div_up(mb, nchunk);
+    float *x32 = nullptr, *hx_all = nullptr;
+    int* rej = nullptr;
+    RS_CHECK(workspace_t("cg_x32", (size_t)ld * mb, &x32));
+    RS_CHECK(workspace_t("sweep_hx", (size_t)ld * mb, &hx_all));
+    RS_CHECK(workspace_t("sweep_rej", 1, &rej));
+    RS_CUDA(cudaMemsetAsync(rej, 0, sizeof(int), c.stream));
+    // every band block's upload on the copy stream, each followed by an event
+    for (int k = 0, b0 = 0; b0 < mb; ++k, b0 += per) {
+        const int nb = std::min(per, mb - b0);
+        RS_CUDA(cudaMemcpyAsync(unk_dev + (size_t)b0 * ld, unk_host + (size_t)b0 * ld,
+                                sizeof(double) * (size_t)ld * nb, cudaMemcpyHostToDevice, c.copy_stream));
+        RS_CUDA(cudaEventRecord(c.ev[k], c.copy_stream));
+    }
+    for (int k = 0, b0 = 0; b0 < mb; ++k, b0 += per) {
+        const int nb = std::min(per, mb - b0);
+        const long n = ld * (long)nb;
+        RS_CUDA(cudaStreamWaitEvent(c.stream, c.ev[k], 0));
+        float* xb = x32 + (size_t)b0 * ld;
+        launch(k_convert<float>, 4 * c.num_sms, 256, 0, c.stream, (const double*)(unk_dev + (size_t)b0 * ld), xb, n);
+        RS_LAUNCH();
+        RS_CHECK(cg_run<float>(xb, ld, nb, spin, esp + b0, res + b0, ncg, mloop, ipc));
+        // this block's H x out of the CG workspace, and its rejection flag
+        float* hx = nullptr;
+        int* flags = nullptr;
+        RS_CHECK(workspace_t("cg_vec", (size_t)ld * nb * 7, &hx));
+        RS_CHECK(workspace_t("cg_flags", (size_t)nb * 4 + 1, &flags));
+        RS_CUDA(cudaMemcpyAsync(hx_all + (size_t)b0 * ld, hx, sizeof(float) * (size_t)n, cudaMemcpyDeviceToDevice,
+                                c.stream));
+        launch(k_or_flag, 1, 1, 0, c.stream, rej, (const int*)(flags + 4 * nb));
+        RS_LAUNCH();
+    }
+    *x32_out = x32;
+    int h = 1;
+    RS_CUDA(cudaMemcpyAsync(&h, rej, sizeof(int), cudaMemcpyDeviceToHost, c.stream));
+    RS_CUDA(cudaStreamSynchronize(c.stream));
+    *hx_out = h == 0 ? hx_all : nullptr;
+    return RSDFT_OK;
+}
+
 int cg_device(double* unk, long ld, int mb, int spin, double* esp, double* res, int ncg, int mloop, int ipc,
               int mode) {
     if (mode == RSDFT_MODE_FP64) return cg_run<double>(unk, ld, mb, spin, esp, res, ncg, mloop, ipc);

@@ -47,6 +47,9 @@ struct Context {
     int device = -1;
     cudaStream_t stream = nullptr;
     bool own_stream = false;
+    cudaStream_t copy_stream = nullptr;  // host<->device staging that overlaps compute
+    static constexpr int NEV = 16;
+    cudaEvent_t ev[NEV] = {};
     cublasHandle_t blas = nullptr;
     cusolverDnHandle_t solver = nullptr;
     int num_sms = 0;

@@ -485,7 +485,13 @@ int rsdft_gpu_eigensolver_sweep(int k, int s, double* unk, long ld, int mb, doub
     }
     double *d, *W, *R;
     bool st;
-    RS_CHECK(wf_acquire(unk, ld, mb, "sweep_unk", &d, &st));
+    // a host array in the mixed forms is uploaded band block by band block
+    // below, overlapped with the CG; every other case copies it in here
+    const int nchunk = mb >= 96 ? 8 : 1;
+    const bool overlap = mode != RSDFT_MODE_FP64 && nchunk > 1;
+    RS_CHECK(wf_acquire(unk, ld, mb, "sweep_unk", &d, &st, !overlap));
+    // the copy stream writes the staging buffer: earlier work on it first
+    if (st && overlap) RS_CUDA(cudaStreamSynchronize(c.stream));
     RS_CHECK(workspace_t("sweep_W", (size_t)mb, &W));
     RS_CHECK(workspace_t("sweep_R", (size_t)mb, &R));
     if (mode == RSDFT_MODE_FP64) {
@@ -494,7 +500,10 @@ int rsdft_gpu_eigensolver_sweep(int k, int s, double* unk, long ld, int mb, doub
     } else {
         float* x32 = nullptr;
         const float* hx = nullptr;
-        RS_CHECK(cg_device_f32(d, ld, mb, s, W, R, ncg, mloop, ipc, &x32, &hx));
+        if (st && overlap)
+            RS_CHECK(cg_device_f32_staged(unk, d, ld, mb, s, W, R, ncg, mloop, ipc, nchunk, &x32, &hx));
+        else
+            RS_CHECK(cg_device_f32(d, ld, mb, s, W, R, ncg, mloop, ipc, &x32, &hx));
         RS_CHECK(orth_subspace_diag_f32(x32, hx, d, ld, mb, s, W, mode));
     }
     RS_CHECK(stage_out(esp, W, sizeof(double) * mb));

@@ -69,6 +69,14 @@ int orth_subspace_diag_device(double* psi, long ld, int mb, int spin, double* es
 int cg_device_f32(const double* unk, long ld, int mb, int spin, double* esp, double* res, int ncg, int mloop,
                   int ipc, float** x32_out, const float** hx_out = nullptr);
 
+// The same sweep on a host array: unk_host is uploaded to unk_dev in nchunk
+// band blocks on the copy stream, and the CG of each block starts as soon as
+// its upload lands (the bands' CG steps are independent), so the upload of
+// later blocks overlaps the CG of earlier ones.
+int cg_device_f32_staged(const double* unk_host, double* unk_dev, long ld, int mb, int spin, double* esp,
+                         double* res, int ncg, int mloop, int ipc, int nchunk, float** x32_out,
+                         const float** hx_out);
+
 // Gram-Schmidt + Rayleigh-Ritz of FP32 bands x32 (h32 = H x32 if already
 // known, else null); the rotated bands are written to psi (FP64).  Mixed
 // forms only.

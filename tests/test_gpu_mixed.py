@@ -155,3 +155,25 @@ def test_mixed_general_shapes(gpu, cells, mode, tol):
     torch.cuda.synchronize()
     # FP32 CG sweep: eigenvalue estimates to ~1e-5 of the FP64 sequence
     assert np.abs(host(eb) - w).max() <= max(1e-5, tol) * max(1.0, np.abs(w).max())
+
+
+def test_mixed_sweep_host_array_overlapped_upload(gpu, cells):
+    """A host array in the mixed sweep is uploaded in band blocks on a copy
+    stream, each block's CG starting when its upload lands; the bands' CG
+    steps are independent, so the result equals the sweep on a device array."""
+    c, o = prepare(gpu, cells, "si64")
+    nb = 160
+    q = np.asfortranarray(o.gram_schmidt_t(np.asfortranarray(c.psi0()[:, :nb])))
+    ud = dev(q)
+    ed = torch.zeros(nb, dtype=torch.float64, device="cuda")
+    rd = torch.zeros_like(ed)
+    gpu.eigensolver_sweep(1, 1, ud, ed, rd, ncg=4, mloop=3, mode=api.MODE_MIXED_BF16)
+    host_pinned = torch.empty((nb, c.ML), dtype=torch.float64, pin_memory=True)
+    host_pinned.copy_(torch.from_numpy(np.ascontiguousarray(q.T)))
+    uh = host_pinned.numpy().T  # (ML, nb) Fortran view of pinned memory
+    eh = np.zeros(nb)
+    rh = np.zeros(nb)
+    gpu.eigensolver_sweep(1, 1, uh, eh, rh, ncg=4, mloop=3, mode=api.MODE_MIXED_BF16)
+    torch.cuda.synchronize()
+    assert np.array_equal(host(ed), eh) and np.array_equal(host(rd), rh)
+    assert np.array_equal(host(ud), uh)
