@@ -29,11 +29,12 @@ __device__ __forceinline__ int pwrap(int i, int n) {
 
 // ------------------------------------------------------------ projection
 // A CTA takes one sphere group (up to 4 projectors sharing a point list) and
-// 32 bands, 4 per warp.  The group's point indices and projector values are
+// PJ_WARPS x PJ_BW bands (16: two per warp, measured faster than four at
+// Si216 480 bands, where more CTAs hide the gather latency better).  The group's point indices and projector values are
 // staged in shared memory a chunk at a time; each lane strides the points
 // and issues the 4 bands' gathers together.  Per (band, projector) the lanes
 // sum points lane, lane+32, ... in order, then a fixed xor-shuffle tree.
-constexpr int PJ_BW = 4;    // bands per warp
+constexpr int PJ_BW = 2;    // bands per warp
 constexpr int PJ_WARPS = 8;
 constexpr int PJ_CH = 512;  // sphere points staged per pass (multiple of 32)
 
@@ -518,9 +519,10 @@ __global__ void __launch_bounds__(384, 1) k_stencil_tma(const __grid_constant__ 
 // Nonlocal scatter after the stencil: hpsi(p, b) += sum over the sphere
 // groups g covering p of sum_q uV(p, g, q) uVunk(g + q, b)
 // (ps_nloc2_op_module.f90:255-263), one thread per covered point and a chunk
-// of bands, SC_BU bands in flight at once.  A point's entries are taken in
-// projector order, so every sum has a fixed order.
-constexpr int SC_BU = 8;
+// of bands, SC_BU bands in flight at once (2: measured faster than 4 and 8).
+// A point's entries are taken in projector order, so every sum has a fixed
+// order.
+constexpr int SC_BU = 2;
 
 template <typename T>
 __global__ void __launch_bounds__(128) k_nl_scatter(T* __restrict__ hpsi, long ld, int nb, int bchunk,
