@@ -30,10 +30,11 @@ __device__ __forceinline__ int pwrap(int i, int n) {
 // ------------------------------------------------------------ projection
 // A CTA takes one sphere group (up to 4 projectors sharing a point list) and
 // PJ_WARPS x PJ_BW bands (16: two per warp, measured faster than four at
-// Si216 480 bands, where more CTAs hide the gather latency better).  The group's point indices and projector values are
-// staged in shared memory a chunk at a time; each lane strides the points
-// and issues the 4 bands' gathers together.  Per (band, projector) the lanes
-// sum points lane, lane+32, ... in order, then a fixed xor-shuffle tree.
+// Si216 480 bands, where more CTAs hide the gather latency better).  The
+// group's point indices and projector values are staged in shared memory a
+// chunk at a time; each lane strides the points and issues its warp's bands'
+// gathers together.  Per (band, projector) the lanes sum points lane,
+// lane+32, ... in order, then a fixed xor-shuffle tree.
 constexpr int PJ_BW = 2;    // bands per warp
 constexpr int PJ_WARPS = 8;
 constexpr int PJ_CH = 512;  // sphere points staged per pass (multiple of 32)
