@@ -1,5 +1,5 @@
 // Symmetric eigensolver for the small dense matrices of the subspace steps
-// (the Rayleigh-Ritz matrix, n = number of bands, up to ~620): the same
+// (the Rayleigh-Ritz matrix, n = number of bands, up to ~590): the same
 // result as LAPACK dsyevd / cuSOLVER syevd (eigenvalues ascending, an
 // orthonormal eigenvector basis), in three steps:
 //
@@ -38,6 +38,7 @@
 
 #include "common.cuh"
 #include "kernels.cuh"
+#include "tma.cuh"
 
 namespace rsdft {
 
@@ -90,30 +91,52 @@ __device__ __forceinline__ double rcp_nr(double q) {
     return fma(r, fma(-q, r, 1.0), r);
 }
 
-// Shared-memory layout of k_sytrd (doubles): own rows R x n, the current
-// reflector v, p / w, the look-ahead row, the published p pieces, row and
-// partial dot (double-buffered), the pulled partial dots, reduction slots and
-// scalars.
+// Shared-memory layout of k_sytrd (doubles; every array an even count, so
+// each starts 16-byte aligned for the bulk copies): own rows R x np, the
+// reflectors v_j / v_{j+1}, w, p, the look-ahead row, and the exchange
+// buffers: per parity what each CTA sent, px[16][PR], and this CTA's
+// outgoing block sb[PR] = [its R pieces of p, its part of p^T v, its rows'
+// entries of the look-ahead column, padding]; reduction slots, scalars, and
+// the two receive mbarriers.
 struct TdLayout {
-    int R, np;
-    size_t rows, vl, pf, wf, rr, pb, rb, kb, kr, red, sc, total;
+    int R, np, PR;
+    size_t rows, vl, wf, pf, rr, px, sb, red, sc, bar, total;
     __host__ __device__ TdLayout(int n) {
         R = (n + TD_C - 1) / TD_C;
         np = (n + 1) & ~1;
+        PR = (2 * R + 2) & ~1;
         rows = 0;
-        vl = rows + (size_t)R * n;  // [2][np]: v_j and v_{j+1}
-        pf = vl + 2 * (size_t)np;
-        wf = pf + np;
-        rr = wf + np;
-        pb = rr + np;
-        rb = pb + 2 * (size_t)np;
-        kb = rb + 2 * (size_t)np;
-        kr = kb + 2;
-        red = kr + TD_C;
+        vl = rows + (size_t)R * np;  // [2][np]
+        wf = vl + 2 * (size_t)np;
+        pf = wf + np;
+        rr = pf + np;
+        px = rr + np;                       // [2][TD_C][PR]
+        sb = px + 2 * (size_t)TD_C * PR;    // [2][PR]
+        red = sb + 2 * (size_t)PR;
         sc = red + TD_W;
-        total = sc + 8;
+        bar = sc + 8;  // 2 x uint64_t
+        total = bar + 2;
     }
 };
+
+__device__ __forceinline__ uint32_t cl_addr(const void* p, uint32_t rank) {
+    uint32_t r;
+    asm volatile("mapa.shared::cluster.u32 %0, %1, %2;" : "=r"(r) : "r"((uint32_t)__cvta_generic_to_shared(p)), "r"(rank));
+    return r;
+}
+
+// Bulk copy (TMA engine, point to point, no multicast) of `bytes` from this
+// CTA's shared memory to the buffer at the same offset as `dst` in CTA
+// `rank`, completion counted on that CTA's mbarrier at the offset of `bar`.
+// Addresses 16-byte aligned, bytes a multiple of 16.
+__device__ __forceinline__ void bulk_to_peer(const void* dst, const void* src, uint32_t bytes, const uint64_t* bar,
+                                             uint32_t rank) {
+    asm volatile(
+        "cp.async.bulk.shared::cluster.shared::cta.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+            cl_addr(dst, rank)),
+        "r"((uint32_t)__cvta_generic_to_shared(src)), "r"(bytes), "r"(cl_addr(bar, rank))
+        : "memory");
+}
 
 // dlarfg on x[0..len): v (v_0 = 1) into vl, sc[0] = tau, sc[1] = beta.  All
 // threads of the CTA; fixed reduction order, so every CTA that runs it on
@@ -151,44 +174,68 @@ __device__ __forceinline__ void td_reflector(const double* x, int len, double* v
 // tau (n-1) and the reflectors in the strict lower part of Q (n x n, ld n;
 // Q(j+1+k, j) = v_k for k >= 1, dsytrd's 'L' storage).
 //
-// Column j with one cluster barrier.  Before it every CTA has published p_j
-// = tau_j A v_j on its own rows and its part of p_j^T v_j, and the owner of
-// row j+1 that row as it stands.  After it every CTA pulls them, forms w_j,
-// brings its copy of row j+1 up to date and runs dlarfg on it for v_{j+1}
-// (the same bits in every CTA), then makes one pass over its own rows that
-// applies A -= v_j w_j^T + w_j v_j^T and, on the updated values, forms
-// p_{j+1} and publishes it (and row j+2, if it owns it) for the next
-// barrier.
+// Column j: every CTA holds v_j and has pushed, with bulk copies into every
+// CTA of the cluster, its pieces of p_j = tau_j A v_j and of p_j^T v_j and
+// its rows' entries of column j+1 as they stand (the look-ahead row, by
+// symmetry; gathered from all CTAs, so no SM serves a one-to-all broadcast).
+// After one cluster barrier each
+// CTA waits on its own mbarrier for those bytes, forms w_j, brings its copy of
+// row j+1 up to date and runs dlarfg on it for v_{j+1} (the same bits in
+// every CTA), then makes one pass over its own rows that applies
+// A -= v_j w_j^T + w_j v_j^T and, on the updated values, forms p_{j+1}; the
+// next pushes follow.  The barrier only guards the exchange buffers against
+// reuse (each is double-buffered by column parity); the data itself arrives
+// through the copy engine while the CTAs compute.
 __global__ void __launch_bounds__(TD_T, 1) k_sytrd(const double* __restrict__ A, int lda, int n, int upper,
                                                   double* __restrict__ Q, double* __restrict__ d,
-                                                  double* __restrict__ e, double* __restrict__ tau) {
+                                                  double* __restrict__ e, double* __restrict__ tau,
+                                                  int* __restrict__ err) {
     extern __shared__ __align__(16) double sm[];
     const TdLayout L(n);
-    const int R = L.R, np = L.np;
+    const int R = L.R, np = L.np, PR = L.PR;
     double* rows = sm + L.rows;
     double* vb = sm + L.vl;  // [2][np]
-    double* pf = sm + L.pf;
     double* wf = sm + L.wf;
+    double* pf = sm + L.pf;
     double* rr = sm + L.rr;
-    double* pb = sm + L.pb;
-    double* rb = sm + L.rb;
-    double* kb = sm + L.kb;
-    double* kr = sm + L.kr;
+    double* px = sm + L.px;
+    double* sb = sm + L.sb;
     double* red = sm + L.red;
     double* sc = sm + L.sc;
+    uint64_t* bar = reinterpret_cast<uint64_t*>(sm + L.bar);
     const int cr = (int)cluster_rank();
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    bool ok = true;
 
     for (int l = 0; l < R; ++l) {
         const int i = l * TD_C + cr;
         if (i >= n) break;
         for (int k = tid; k < n; k += TD_T) {
             const int a = i < k ? i : k, b = i < k ? k : i;  // (min, max)
-            rows[(size_t)l * n + k] = upper ? A[a + (size_t)b * lda] : A[b + (size_t)a * lda];
+            rows[(size_t)l * np + k] = upper ? A[a + (size_t)b * lda] : A[b + (size_t)a * lda];
         }
     }
+    if (tid == 0) {
+        mbar_init(&bar[0], 1);
+        mbar_init(&bar[1], 1);
+        mbar_fence_init();
+    }
     __syncthreads();
-    cluster_sync();
+    cluster_sync();  // rows loaded and receive barriers initialised everywhere
+
+    // push this CTA's block for column jn from sb[buf] into every CTA; arm
+    // this CTA's own barrier for the 16 blocks it will receive
+    auto send = [&](int buf) {
+        fence_proxy_async_smem();
+        __syncthreads();
+        if (tid == 0) {
+            const uint32_t pb = (uint32_t)(PR * sizeof(double));
+            mbar_arrive_expect_tx(&bar[buf], TD_C * pb);
+            for (int dst = 0; dst < TD_C; ++dst)
+                bulk_to_peer(px + ((size_t)buf * TD_C + cr) * PR, sb + (size_t)buf * PR, pb, &bar[buf], (uint32_t)dst);
+        }
+    };
+
     // v_0 from row 0 (CTA 0, local row 0)
     for (int k = tid; k < n; k += TD_T) rr[k] = dsmem_ld(rows + k, 0);
     __syncthreads();
@@ -203,31 +250,33 @@ __global__ void __launch_bounds__(TD_T, 1) k_sytrd(const double* __restrict__ A,
     if (cr == 0)
         for (int k = 1 + tid; k < n - 1; k += TD_T) Q[(size_t)(1 + k)] = vb[k];
     double tcur = sc[0];  // tau of the current column
-    // p_0 on own rows i > 0, and row 1 published by its owner
+    // p_0 on own rows i > 0
     {
         const double t = tcur;
         const int m = n - 1;
         double kacc = 0.0;
         for (int l = warp; l < R; l += TD_W) {
             const int i = l * TD_C + cr;
-            if (i < 1 || i >= n) continue;
-            const double* a = rows + (size_t)l * n + 1;
-            double s0 = 0.0;
-            for (int k = lane; k < m; k += 32) s0 = fma(a[k], vb[k], s0);
-            const double pv = t * warp_sum_d(s0);
-            if (lane == 0) {
-                pb[i - 1] = pv;
-                kacc = fma(pv, vb[i - 1], kacc);
+            double pv = 0.0;
+            if (i >= 1 && i < n) {
+                const double* a = rows + (size_t)l * np + 1;
+                double s0 = 0.0;
+                for (int k = lane; k < m; k += 32) s0 = fma(a[k], vb[k], s0);
+                pv = t * warp_sum_d(s0);
+                if (lane == 0) kacc = fma(pv, vb[i - 1], kacc);
             }
-            if (i == 1)
-                for (int k = lane; k < m; k += 32) rb[k] = a[k];
+            if (lane == 0) {
+                sb[l] = pv;
+                sb[R + 1 + l] = i >= 1 && i < n ? rows[(size_t)l * np + 1] : 0.0;  // A(i, 1)
+            }
         }
         if (lane == 0) red[warp] = kacc;
         __syncthreads();
         if (warp == 0) {
             const double s1 = warp_sum_d(lane < TD_W ? red[lane] : 0.0);
-            if (lane == 0) kb[0] = s1;
+            if (lane == 0) sb[R] = s1;
         }
+        send(0);
     }
 
     for (int j = 0; j <= n - 2; ++j) {
@@ -236,27 +285,36 @@ __global__ void __launch_bounds__(TD_T, 1) k_sytrd(const double* __restrict__ A,
         const double* vj = vb + par * np;
         double* vn = vb + nxt * np;
         const double t = tcur;
-        cluster_sync();  // p_j pieces, partial dots and row j+1 visible
-        for (int k = tid; k < m; k += TD_T) {
-            pf[k] = dsmem_ld(pb + par * np + k, (uint32_t)((j + 1 + k) % TD_C));
-            rr[k] = dsmem_ld(rb + par * np + k, (uint32_t)((j + 1) % TD_C));
+        cluster_sync();  // exchange buffers of the other parity are free
+        if (!mbar_wait(&bar[par], (uint32_t)((j >> 1) & 1))) ok = false;
+        {
+            // p_j and the look-ahead row j+1 (= column j+1: A(i, j+1) from the
+            // owner of row i), both spread over the 16 blocks
+            const double* xp = px + (size_t)par * TD_C * PR;
+            for (int k = tid; k < m; k += TD_T) {
+                const int i = j + 1 + k;
+                const double* blk = xp + (size_t)(i % TD_C) * PR;
+                pf[k] = blk[i / TD_C];
+                rr[k] = blk[R + 1 + i / TD_C];
+            }
         }
-        if (tid < TD_C) kr[tid] = dsmem_ld(kb + par, (uint32_t)tid);
-        __syncthreads();
         // w = p + alpha v (into wf), row j+1 up to date; its columns j+3..
         // give sigma of v_{j+1}
         double sg = 0.0;
         {
+            const double* xp = px + (size_t)par * TD_C * PR;
             double kp[TD_C / 2];  // pairwise sum of the 16 partial dots (fixed order)
 #pragma unroll
-            for (int c = 0; c < TD_C / 2; ++c) kp[c] = kr[2 * c] + kr[2 * c + 1];
+            for (int c = 0; c < TD_C / 2; ++c) kp[c] = xp[(size_t)(2 * c) * PR + R] + xp[(size_t)(2 * c + 1) * PR + R];
 #pragma unroll
             for (int h = TD_C / 4; h >= 1; h >>= 1)
 #pragma unroll
                 for (int c = 0; c < h; ++c) kp[c] = kp[2 * c] + kp[2 * c + 1];
             const double al = -0.5 * t * kp[0];
-            const double vi = vj[0], wi = fma(al, vi, pf[0]);
-            for (int k = tid; k < m; k += TD_T) {
+            const int j1 = j + 1;
+            const double p0 = xp[(size_t)(j1 % TD_C) * PR + j1 / TD_C];
+            const double vi = vj[0], wi = fma(al, vi, p0);
+            for (int k = tid; k < m; k += TD_T) {  // each thread its own k of pf, rr
                 const double wk = fma(al, vj[k], pf[k]);
                 wf[k] = wk;
                 const double r = fma(-wi, vj[k], fma(-vi, wk, rr[k]));
@@ -291,7 +349,6 @@ __global__ void __launch_bounds__(TD_T, 1) k_sytrd(const double* __restrict__ A,
             scal = sl;
             nontriv = sig > 0.0;
             if (cr == 0 && tid == 0) {
-                sc[0] = tt;
                 d[j + 1] = rr[0];
                 e[j + 1] = beta;
                 tau[j + 1] = tt;
@@ -307,53 +364,60 @@ __global__ void __launch_bounds__(TD_T, 1) k_sytrd(const double* __restrict__ A,
         __syncthreads();
         // one pass over own rows i > j: the step-j update, then p_{j+1} on rows i > j+1
         double kacc = 0.0;
+        double* sbn = sb + (size_t)nxt * PR;
         for (int l = warp; l < R; l += TD_W) {
             const int i = l * TD_C + cr;
-            if (i <= j || i >= n) continue;
-            const int ii = i - j - 1;
-            const double vi = vj[ii], wi = wf[ii];
-            double* a = rows + (size_t)l * n + j + 1;
-            const bool pub = i == j + 2;  // the next look-ahead row
-            double* rbn = rb + nxt * np - 1;
-            double s0 = 0.0, s1 = 0.0;
-            // two elements per lane per trip, loads first (vn[-1] is never used:
-            // column j+1 of the update does not enter p_{j+1})
-            for (int k0 = lane; k0 < m; k0 += 64) {
-                const int k1 = k0 + 32;
-                const bool h1 = k1 < m;
-                const double a0 = a[k0], v0 = vj[k0], w0 = wf[k0], n0 = k0 >= 1 ? vn[k0 - 1] : 0.0;
-                const double a1 = h1 ? a[k1] : 0.0, v1 = h1 ? vj[k1] : 0.0, w1 = h1 ? wf[k1] : 0.0;
-                const double n1 = h1 ? vn[k1 - 1] : 0.0;
-                const double x0 = fma(-wi, v0, fma(-vi, w0, a0));
-                const double x1 = fma(-wi, v1, fma(-vi, w1, a1));
-                a[k0] = x0;
-                s0 = fma(x0, n0, s0);
-                if (h1) {
-                    a[k1] = x1;
-                    s1 = fma(x1, n1, s1);
+            double pv = 0.0;
+            if (i > j && i < n) {
+                const int ii = i - j - 1;
+                const double vi = vj[ii], wi = wf[ii];
+                double* a = rows + (size_t)l * np + j + 1;
+                double s0 = 0.0, s1 = 0.0;
+                // two elements per lane per trip, loads first (vn[-1] is never
+                // used: column j+1 of the update does not enter p_{j+1})
+                for (int k0 = lane; k0 < m; k0 += 64) {
+                    const int k1 = k0 + 32;
+                    const bool h1 = k1 < m;
+                    const double a0 = a[k0], v0 = vj[k0], w0 = wf[k0], n0 = k0 >= 1 ? vn[k0 - 1] : 0.0;
+                    const double a1 = h1 ? a[k1] : 0.0, v1 = h1 ? vj[k1] : 0.0, w1 = h1 ? wf[k1] : 0.0;
+                    const double n1 = h1 ? vn[k1 - 1] : 0.0;
+                    const double x0 = fma(-wi, v0, fma(-vi, w0, a0));
+                    const double x1 = fma(-wi, v1, fma(-vi, w1, a1));
+                    a[k0] = x0;
+                    s0 = fma(x0, n0, s0);
+                    if (h1) {
+                        a[k1] = x1;
+                        s1 = fma(x1, n1, s1);
+                    }
                 }
-                if (pub) {
-                    if (k0 >= 1) rbn[k0] = x0;
-                    if (h1) rbn[k1] = x1;
+                if (i >= j + 2) {
+                    pv = tn * warp_sum_d(s0 + s1);
+                    if (lane == 0) kacc = fma(pv, vn[i - j - 2], kacc);
                 }
             }
-            if (i >= j + 2) {
-                const double pv = tn * warp_sum_d(s0 + s1);
-                if (lane == 0) {
-                    pb[nxt * np + (i - j - 2)] = pv;
-                    kacc = fma(pv, vn[i - j - 2], kacc);
-                }
+            __syncwarp();  // column j+2 of this row was updated by another lane
+            if (lane == 0) {
+                sbn[l] = pv;
+                // A(i, j+2) after this column's update, for the next look-ahead row
+                sbn[R + 1 + l] = i >= j + 2 && i < n ? rows[(size_t)l * np + j + 2] : 0.0;
             }
         }
         if (lane == 0) red[warp] = kacc;
         __syncthreads();
         if (warp == 0) {
             const double s1 = warp_sum_d(lane < TD_W ? red[lane] : 0.0);
-            if (lane == 0) kb[nxt] = s1;
+            if (lane == 0) sbn[R] = s1;
         }
+        send(nxt);
         tcur = tn;
     }
-    cluster_sync();  // no CTA leaves while another may still read its shared memory
+    if (!ok) {
+        // a receive that never completed: give the last column's copies one
+        // more bounded wait before leaving, and report
+        (void)mbar_wait(&bar[(n - 2) & 1], (uint32_t)(((n - 2) >> 1) & 1));
+        atomicExch(err, 4);
+    }
+    cluster_sync();  // no CTA leaves while another may still read or copy into its shared memory
 }
 
 // Sturm count: eigenvalues of T below x (dlaebz's recurrence and guard)
@@ -677,7 +741,7 @@ int syevd_fast(double* A, int n, double* W, cublasFillMode_t uplo) {
     double* aux = dd + 3 * n;
     ++g_kernel_launches;
     RS_CUDA(cudaLaunchKernelEx(&cfg, k_sytrd, (const double*)A, n, n, uplo == CUBLAS_FILL_MODE_UPPER ? 1 : 0, Q, d,
-                               e, tau));
+                               e, tau, c.err_flag));
     RS_LAUNCH();
     launch(k_tri_bisect, div_up(n, BS_WARPS), 32 * BS_WARPS, (size_t)2 * n * sizeof(double), c.stream,
            (const double*)d, (const double*)e, n, W, aux);

@@ -1,7 +1,8 @@
 // Bulk-copy (TMA) and mbarrier helpers for sm_100a, inline PTX.
 //
-// Only plain (non-multicast) bulk copies from this GPU's global memory into
-// the issuing CTA's own shared memory are used.  Every wait is bounded: a
+// Only plain (non-multicast) bulk copies are used: from this GPU's global
+// memory into the issuing CTA's own shared memory, and (eigen.cu) from a
+// CTA's shared memory into one CTA of its cluster.  Every wait is bounded: a
 // wait that runs out reports failure and the caller aborts the CTA cleanly.
 #pragma once
 
