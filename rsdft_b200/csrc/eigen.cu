@@ -121,7 +121,9 @@ struct TdLayout {
 
 __device__ __forceinline__ uint32_t cl_addr(const void* p, uint32_t rank) {
     uint32_t r;
-    asm volatile("mapa.shared::cluster.u32 %0, %1, %2;" : "=r"(r) : "r"((uint32_t)__cvta_generic_to_shared(p)), "r"(rank));
+    asm volatile("mapa.shared::cluster.u32 %0, %1, %2;"
+                 : "=r"(r)
+                 : "r"((uint32_t)__cvta_generic_to_shared(p)), "r"(rank));
     return r;
 }
 
@@ -178,14 +180,14 @@ __device__ __forceinline__ void td_reflector(const double* x, int len, double* v
 // CTA of the cluster, its pieces of p_j = tau_j A v_j and of p_j^T v_j and
 // its rows' entries of column j+1 as they stand (the look-ahead row, by
 // symmetry; gathered from all CTAs, so no SM serves a one-to-all broadcast).
-// After one cluster barrier each
-// CTA waits on its own mbarrier for those bytes, forms w_j, brings its copy of
-// row j+1 up to date and runs dlarfg on it for v_{j+1} (the same bits in
-// every CTA), then makes one pass over its own rows that applies
+// Each CTA waits on its own mbarrier for those bytes, forms w_j, brings its
+// copy of row j+1 up to date and runs dlarfg on it for v_{j+1} (the same bits
+// in every CTA), then makes one pass over its own rows that applies
 // A -= v_j w_j^T + w_j v_j^T and, on the updated values, forms p_{j+1}; the
-// next pushes follow.  The barrier only guards the exchange buffers against
-// reuse (each is double-buffered by column parity); the data itself arrives
-// through the copy engine while the CTAs compute.
+// next pushes follow.  The receive barriers carry both the data and the
+// ordering: exchange buffers are double-buffered by column parity, and the
+// block a CTA must hold before reusing a buffer was sent after that buffer's
+// previous use, so no cluster barrier is needed per column.
 __global__ void __launch_bounds__(TD_T, 1) k_sytrd(const double* __restrict__ A, int lda, int n, int upper,
                                                   double* __restrict__ Q, double* __restrict__ d,
                                                   double* __restrict__ e, double* __restrict__ tau,
@@ -232,7 +234,8 @@ __global__ void __launch_bounds__(TD_T, 1) k_sytrd(const double* __restrict__ A,
             const uint32_t pb = (uint32_t)(PR * sizeof(double));
             mbar_arrive_expect_tx(&bar[buf], TD_C * pb);
             for (int dst = 0; dst < TD_C; ++dst)
-                bulk_to_peer(px + ((size_t)buf * TD_C + cr) * PR, sb + (size_t)buf * PR, pb, &bar[buf], (uint32_t)dst);
+                bulk_to_peer(px + ((size_t)buf * TD_C + cr) * PR, sb + (size_t)buf * PR, pb, &bar[buf],
+                             (uint32_t)dst);
         }
     };
 
@@ -285,7 +288,12 @@ __global__ void __launch_bounds__(TD_T, 1) k_sytrd(const double* __restrict__ A,
         const double* vj = vb + par * np;
         double* vn = vb + nxt * np;
         const double t = tcur;
-        cluster_sync();  // exchange buffers of the other parity are free
+        // no cluster barrier: a CTA copies into px[par] of a peer for column
+        // j+2 only after it has received that peer's block for column j+1,
+        // which the peer sends after its reads of px[par] for column j; and a
+        // peer's copies out of sb[par] for column j have all landed once this
+        // CTA holds every block for column j+1 (each sender waited for its
+        // column-j blocks before sending those)
         if (!mbar_wait(&bar[par], (uint32_t)((j >> 1) & 1))) ok = false;
         {
             // p_j and the look-ahead row j+1 (= column j+1: A(i, j+1) from the
@@ -746,8 +754,8 @@ int syevd_fast(double* A, int n, double* W, cublasFillMode_t uplo) {
     launch(k_tri_bisect, div_up(n, BS_WARPS), 32 * BS_WARPS, (size_t)2 * n * sizeof(double), c.stream,
            (const double*)d, (const double*)e, n, W, aux);
     RS_LAUNCH();
-    launch(k_tri_invit, div_up(n, IV_WARPS), 32 * IV_WARPS, (size_t)2 * n * sizeof(double), c.stream, (const double*)d, (const double*)e,
-           (const double*)W, (const double*)aux, n, A, n);
+    launch(k_tri_invit, div_up(n, IV_WARPS), 32 * IV_WARPS, (size_t)2 * n * sizeof(double), c.stream,
+           (const double*)d, (const double*)e, (const double*)W, (const double*)aux, n, A, n);
     RS_LAUNCH();
     // two Newton-Schulz steps on Z (in A), through Z2 (in ws)
     {

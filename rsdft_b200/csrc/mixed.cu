@@ -424,7 +424,8 @@ __global__ void k_reduce_tiles(const double* __restrict__ P, int nsplit, int npa
         }
         const int pair = sym ? tn * (tn + 1) / 2 + tm : tm + tn * ntm;
         double s = 0.0;
-        for (int k = 0; k < nsplit; ++k) s += P[((size_t)k * npairs + pair) * (size_t)(bn * UB_M) + (size_t)cc * UB_M + rr];
+        for (int k = 0; k < nsplit; ++k)
+            s += P[((size_t)k * npairs + pair) * (size_t)(bn * UB_M) + (size_t)cc * UB_M + rr];
         return s;
     };
     double v = fetch(i, j);
