@@ -370,44 +370,47 @@ __global__ void __launch_bounds__(TD_T, 1) k_sytrd(const double* __restrict__ A,
             if (cr == 0 && k > 0) Q[(size_t)(j + 2 + k) + (size_t)(j + 1) * n] = v;
         }
         __syncthreads();
-        // one pass over own rows i > j: the step-j update, then p_{j+1} on rows i > j+1
+        // one pass over own rows i > j: the step-j update, then p_{j+1} on rows
+        // i > j+1.  A warp takes its rows two at a time, sharing the loads of
+        // v_j, w_j and v_{j+1} between them (vn[-1] is never used: column j+1
+        // of the update does not enter p_{j+1})
         double kacc = 0.0;
         double* sbn = sb + (size_t)nxt * PR;
-        for (int l = warp; l < R; l += TD_W) {
-            const int i = l * TD_C + cr;
-            double pv = 0.0;
-            if (i > j && i < n) {
-                const int ii = i - j - 1;
-                const double vi = vj[ii], wi = wf[ii];
-                double* a = rows + (size_t)l * np + j + 1;
-                double s0 = 0.0, s1 = 0.0;
-                // two elements per lane per trip, loads first (vn[-1] is never
-                // used: column j+1 of the update does not enter p_{j+1})
-                for (int k0 = lane; k0 < m; k0 += 64) {
-                    const int k1 = k0 + 32;
-                    const bool h1 = k1 < m;
-                    const double a0 = a[k0], v0 = vj[k0], w0 = wf[k0], n0 = k0 >= 1 ? vn[k0 - 1] : 0.0;
-                    const double a1 = h1 ? a[k1] : 0.0, v1 = h1 ? vj[k1] : 0.0, w1 = h1 ? wf[k1] : 0.0;
-                    const double n1 = h1 ? vn[k1 - 1] : 0.0;
-                    const double x0 = fma(-wi, v0, fma(-vi, w0, a0));
-                    const double x1 = fma(-wi, v1, fma(-vi, w1, a1));
-                    a[k0] = x0;
-                    s0 = fma(x0, n0, s0);
-                    if (h1) {
-                        a[k1] = x1;
-                        s1 = fma(x1, n1, s1);
-                    }
+        for (int l0 = warp; l0 < R; l0 += 2 * TD_W) {
+            const int l1 = l0 + TD_W;
+            const int i0 = l0 * TD_C + cr, i1 = l1 * TD_C + cr;
+            const bool h0 = i0 > j && i0 < n, h1 = l1 < R && i1 > j && i1 < n;  // warp-uniform
+            const double vi0 = h0 ? vj[i0 - j - 1] : 0.0, wi0 = h0 ? wf[i0 - j - 1] : 0.0;
+            const double vi1 = h1 ? vj[i1 - j - 1] : 0.0, wi1 = h1 ? wf[i1 - j - 1] : 0.0;
+            double* a0 = rows + (size_t)l0 * np + j + 1;
+            double* a1 = rows + (size_t)(h1 ? l1 : l0) * np + j + 1;
+            double s0 = 0.0, s1 = 0.0;
+            for (int k = lane; k < m; k += 32) {
+                const double v = vj[k], w = wf[k], nv = k >= 1 ? vn[k - 1] : 0.0;
+                if (h0) {
+                    const double x = fma(-wi0, v, fma(-vi0, w, a0[k]));
+                    a0[k] = x;
+                    s0 = fma(x, nv, s0);
                 }
-                if (i >= j + 2) {
-                    pv = tn * warp_sum_d(s0 + s1);
-                    if (lane == 0) kacc = fma(pv, vn[i - j - 2], kacc);
+                if (h1) {
+                    const double x = fma(-wi1, v, fma(-vi1, w, a1[k]));
+                    a1[k] = x;
+                    s1 = fma(x, nv, s1);
                 }
             }
-            __syncwarp();  // column j+2 of this row was updated by another lane
+            const double pv0 = (h0 && i0 >= j + 2) ? tn * warp_sum_d(s0) : 0.0;
+            const double pv1 = (h1 && i1 >= j + 2) ? tn * warp_sum_d(s1) : 0.0;
+            __syncwarp();  // column j+2 of these rows was updated by other lanes
             if (lane == 0) {
-                sbn[l] = pv;
+                if (h0 && i0 >= j + 2) kacc = fma(pv0, vn[i0 - j - 2], kacc);
+                if (h1 && i1 >= j + 2) kacc = fma(pv1, vn[i1 - j - 2], kacc);
                 // A(i, j+2) after this column's update, for the next look-ahead row
-                sbn[R + 1 + l] = i >= j + 2 && i < n ? rows[(size_t)l * np + j + 2] : 0.0;
+                sbn[l0] = pv0;
+                sbn[R + 1 + l0] = i0 >= j + 2 && i0 < n ? rows[(size_t)l0 * np + j + 2] : 0.0;
+                if (l1 < R) {
+                    sbn[l1] = pv1;
+                    sbn[R + 1 + l1] = i1 >= j + 2 && i1 < n ? rows[(size_t)l1 * np + j + 2] : 0.0;
+                }
             }
         }
         if (lane == 0) red[warp] = kacc;
