@@ -431,24 +431,13 @@ __global__ void __launch_bounds__(TD_T, 1) k_sytrd(const double* __restrict__ A,
     cluster_sync();  // no CTA leaves while another may still read or copy into its shared memory
 }
 
-// Sturm count: eigenvalues of T below x (dlaebz's recurrence and guard)
-__device__ __forceinline__ int sturm_count(const double* sd, const double* se2, int n, double x, double pivmin) {
-    double q = sd[0] - x;
-    if (fabs(q) <= pivmin) q = -pivmin;
-    int c = q < 0.0 ? 1 : 0;
-    for (int i = 1; i < n; ++i) {
-        q = sd[i] - x - se2[i - 1] * rcp_nr(q);  // |q| > pivmin >= DBL_MIN: normal
-        if (fabs(q) <= pivmin) q = -pivmin;
-        c += q < 0.0 ? 1 : 0;
-    }
-    return c;
-}
-
 constexpr int BS_WARPS = 2;  // small blocks: the 480-odd warps spread over all SMs
 constexpr int BS_PTS = 4;  // trial points per lane (independent Sturm chains)
 
 // w[k] = k-th smallest eigenvalue of T (d, e), one warp per k, 32 x BS_PTS
-// trial points per round; aux[0] = |T|_1
+// trial points per round, each counted with dlaebz's Sturm recurrence
+// q_i = d_i - x - e_{i-1}^2 / q_{i-1} (eigenvalues below x = negative q,
+// |q| <= pivmin replaced by -pivmin); aux[0] = |T|_1
 __global__ void __launch_bounds__(32 * BS_WARPS) k_tri_bisect(const double* __restrict__ d,
                                                              const double* __restrict__ e, int n,
                                                              double* __restrict__ w, double* __restrict__ aux) {
@@ -628,7 +617,7 @@ __global__ void __launch_bounds__(32 * IV_WARPS) k_tri_invit(const double* __res
             }
             // last row
             if (fabs(D) < tol) D = copysign(tol, D);
-            const int ln = (n - 1) / IV_RPL, rn = (n - 1) - ln * IV_RPL;
+            const int ln = (n - 1) / IV_RPL;  // lane holding the last row
             // back substitution in reverse lane order, carrying y(i+1), y(i+2)
             double y1 = R * rcp_nr(D), y2 = 0.0;  // |D| >= tol
             for (int l = ln; l >= 0; --l) {
@@ -650,7 +639,6 @@ __global__ void __launch_bounds__(32 * IV_WARPS) k_tri_invit(const double* __res
                 y1 = __shfl_sync(0xffffffffu, y1, l);
                 y2 = __shfl_sync(0xffffffffu, y2, l);
             }
-            (void)rn;
             // Gram-Schmidt against the group's earlier vectors
             for (int p = k; p < j; ++p) {
                 double dot = 0.0;
