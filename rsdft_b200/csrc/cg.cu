@@ -563,7 +563,7 @@ static int cg_run(T* x, long ld, int mb, int spin, double* esp, double* res, int
             // in mloop + 2 passes (s-step form; w_j in r, q, Pg, hp, which
             // are free until hpsi(p))
             const SSVec<T> sv{{v.r, v.q, v.Pg, v.hp}};
-            RS_CHECK(sstep_precond<T>(v.g, sv, v.p, x, v.hx, ld, mb, mloop, icg == 1, s, ss, cz, part, pa, dV));
+            RS_CHECK(sstep_precond<T>(v.g, sv, v.p, x, ld, mb, mloop, icg == 1, s, ss, cz, part, pa, dV));
         } else {
             // --- preconditioning (Pgk = gk on entry)
             if (ipc == 4 && mloop > 0) {
@@ -596,13 +596,8 @@ static int cg_run(T* x, long ld, int mb, int spin, double* esp, double* res, int
             RS_LAUNCH();
         }
         RS_CHECK(hpsi_device<T>(v.p, v.hp, ld, mb, spin, s.active));
-        // --- six dots: <x|x>, <p|x>, <p|p>, <x|Hx>, <p|Hx>, <p|Hp> (the s-step
-        // search-direction pass has formed the first five)
-        if (sstep) {
-            launch(k_multidot<T, 2, DotsXY>, vg, VT, 0, st, v.p, v.hp, nullptr, nullptr, ld, n, part, s.active, gv);
-            launch(k_finish_strided, div_up((long)mb, 128), 128, 0, st, (const double*)part, nchunk, 1, mb, dV,
-                   s.dots + 5, 6, (const int*)s.active);
-        } else {
+        // --- six dots: <x|x>, <p|x>, <p|p>, <x|Hx>, <p|Hx>, <p|Hp>
+        {
             launch(k_multidot<T, 4, DotsCG6>, vg, VT, 0, st, x, v.p, v.hx, v.hp, ld, n, part, s.active, gv);
             finish(6, dV, s.dots, s.active);
         }

@@ -142,18 +142,11 @@ __device__ __forceinline__ T pc_offdiag(const T* __restrict__ f, long i, int i1,
 }
 
 // Preconditioner + search direction of one CG step in the s-step form:
-// p = Pg (first) or Pg + bk p, with rb = dV <Pg|g> and gkgk updated in s,
-// the pending x update applied, and s.dots[0..4] = dV (<x|x>, <p|x>, <p|p>,
-// <x|Hx>, <p|Hx>) of each active band formed from the new x, p and hx.
+// p = Pg (first) or Pg + bk p, with rb = dV <Pg|g> and gkgk updated in s.
 // ss and cz hold SS_STRIDE and SS_MAXM doubles per band, part the per-CTA
 // partial sums (mb x nchunk x 8 doubles).
 template <typename T>
-int sstep_precond(const T* g, const SSVec<T>& sv, T* p, T* x, const T* hx, long ld, int mb, int mloop, int first,
-                  const CGScal& s, double* ss, double* cz, double* part, const PcArgs& pa, double dV);
-
-// out[b * ostride + k] = scale * sum over the nchunk partial sums in part
-// (K values per band and chunk), for the active bands
-__global__ void k_finish_strided(const double* __restrict__ part, int nchunk, int K, int nb, double scale,
-                                 double* __restrict__ out, int ostride, const int* __restrict__ active);
+int sstep_precond(const T* g, const SSVec<T>& sv, T* p, T* x, long ld, int mb, int mloop, int first, const CGScal& s,
+                  double* ss, double* cz, double* part, const PcArgs& pa, double dV);
 
 }  // namespace rsdft

@@ -139,41 +139,34 @@ __global__ void s_sstep(CGScal s, const double* __restrict__ ss, double* __restr
 }
 
 // p = g + sum_j cz_j w_j (+ bk p after the first step)
-// The search direction p = g + sum_j c_j w_j + bk p of every active band
-// (and, for a band with a pending update, x = u11 x + u21 p_old first); when
-// part5 is given, also the first five of the CG step's six dot products with
-// the new p and the current x, Hx (<x|x>, <p|x>, <p|p>, <x|Hx>, <p|Hx>,
-// cg_module.f90:236-282), so the pass after H p only needs <p|Hp>.
 template <typename T>
 __global__ void __launch_bounds__(VT) k_ss_p(const T* __restrict__ g, SSVec<T> sv, T* __restrict__ p,
-                                             T* __restrict__ x, const T* __restrict__ hx, long ld, long n,
-                                             const double* __restrict__ cz, const double* __restrict__ bk_, int m,
-                                             int first, const int* __restrict__ active, const int* __restrict__ pend,
+                                             T* __restrict__ x, long ld, long n, const double* __restrict__ cz,
+                                             const double* __restrict__ bk_, int m, int first,
+                                             const int* __restrict__ active, const int* __restrict__ pend,
                                              const double* __restrict__ u11_, const double* __restrict__ u21_,
-                                             double* __restrict__ part5, int vec) {
+                                             int vec) {
     using G = Grp16<T>;
     constexpr int W = G::W;
-    __shared__ double sh[5 * (VT / 32)];
     const int b = blockIdx.y;
     const bool act = !active || active[b];
     const bool upd = pend && pend[b];  // the previous step's x update, which needs the old p
     if (!act && !upd) return;
-    const bool dots = part5 && act;  // uniform per CTA
     const long off = (long)b * ld, base = (long)blockIdx.x * VCHUNK;
     T c[SS_MAXM];
 #pragma unroll
     for (int j = 0; j < SS_MAXM; ++j) c[j] = (T)cz[(long)b * SS_MAXM + j];
     const T bk = (T)bk_[b];
     const T u11 = upd ? (T)u11_[b] : (T)0, u21 = upd ? (T)u21_[b] : (T)0;
-    double acc[5] = {0.0, 0.0, 0.0, 0.0, 0.0};
 #pragma unroll 2
     for (int it = 0; it < VITEMS / W; ++it) {
         const long i = base + ((long)it * VT + threadIdx.x) * W;
         if (vec && i + W <= n) {
-            T pg[W], t[W], xv[W];
+            T pg[W], t[W];
             if (upd || !first) G::load(p + off + i, t);
-            if (upd || dots) G::load(x + off + i, xv);
             if (upd) {
+                T xv[W];
+                G::load(x + off + i, xv);
 #pragma unroll
                 for (int q = 0; q < W; ++q) xv[q] = cg_upd2_elem(xv[q], t[q], u11, u21);
                 G::store(x + off + i, xv);
@@ -196,65 +189,20 @@ __global__ void __launch_bounds__(VT) k_ss_p(const T* __restrict__ g, SSVec<T> s
                 for (int q = 0; q < W; ++q) pg[q] += bk * pn[q];
             }
             G::store(p + off + i, pg);
-            if (dots) {
-                T h[W];
-                G::load(hx + off + i, h);
-#pragma unroll
-                for (int q = 0; q < W; ++q) {
-                    const double xd = (double)xv[q], pd = (double)pg[q], hd = (double)h[q];
-                    acc[0] = fma(xd, xd, acc[0]);
-                    acc[1] = fma(pd, xd, acc[1]);
-                    acc[2] = fma(pd, pd, acc[2]);
-                    acc[3] = fma(xd, hd, acc[3]);
-                    acc[4] = fma(pd, hd, acc[4]);
-                }
-            }
         } else {
             for (int q = 0; q < W && i + q < n; ++q) {
                 const long k = off + i + q;
                 const T po = (upd || !first) ? p[k] : (T)0;
-                T xk = (upd || dots) ? x[k] : (T)0;
-                if (upd) {
-                    xk = cg_upd2_elem(xk, po, u11, u21);
-                    x[k] = xk;
-                }
+                if (upd) x[k] = cg_upd2_elem(x[k], po, u11, u21);
                 if (!act) continue;
                 T pg = g[k];
 #pragma unroll
                 for (int j = 0; j < SS_MAXM; ++j)
                     if (j < m) pg += c[j] * sv.w[j][k];
-                pg = first ? pg : pg + bk * po;
-                p[k] = pg;
-                if (dots) {
-                    const double xd = (double)xk, pd = (double)pg, hd = (double)hx[k];
-                    acc[0] = fma(xd, xd, acc[0]);
-                    acc[1] = fma(pd, xd, acc[1]);
-                    acc[2] = fma(pd, pd, acc[2]);
-                    acc[3] = fma(xd, hd, acc[3]);
-                    acc[4] = fma(pd, hd, acc[4]);
-                }
+                p[k] = first ? pg : pg + bk * po;
             }
         }
     }
-    if (dots) {
-        block_sum_n<VT, 5>(acc, sh);
-        if (threadIdx.x == 0) {
-#pragma unroll
-            for (int k = 0; k < 5; ++k) part5[((long)b * gridDim.x + blockIdx.x) * 5 + k] = acc[k];
-        }
-    }
-}
-
-__global__ void k_finish_strided(const double* __restrict__ part, int nchunk, int K, int nb, double scale,
-                                 double* __restrict__ out, int ostride, const int* __restrict__ active) {
-    int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= nb * K) return;
-    int b = i / K, k = i - b * K;
-    if (active && !active[b]) return;
-    const double* q = part + (long)b * nchunk * K + k;
-    double s = 0.0;
-    for (int c = 0; c < nchunk; ++c) s += q[(long)c * K];
-    out[(long)b * ostride + k] = s * scale;
 }
 
 template <typename T>
@@ -684,8 +632,8 @@ static int pc_tma_dispatch(int K, bool store, const T* g, const SSVec<T>& sv, co
 }
 
 template <typename T>
-int sstep_precond(const T* g, const SSVec<T>& sv, T* p, T* x, const T* hx, long ld, int mb, int mloop, int first,
-                  const CGScal& s, double* ss, double* cz, double* part, const PcArgs& pa, double dV) {
+int sstep_precond(const T* g, const SSVec<T>& sv, T* p, T* x, long ld, int mb, int mloop, int first, const CGScal& s,
+                  double* ss, double* cz, double* part, const PcArgs& pa, double dV) {
     const Context& c = ctx();
     cudaStream_t st = c.stream;
     const long n = c.ml;
@@ -715,19 +663,16 @@ int sstep_precond(const T* g, const SSVec<T>& sv, T* p, T* x, const T* hx, long 
         finish_to(D, out, nch);
     }
     launch(s_sstep, sb, 128, 0, st, s, ss, cz, mb, mloop, pa.d, dV, first);
-    const int gv = grp16_ok<T>(ld, {g, p, x, hx, sv.w[0], sv.w[1], sv.w[2], sv.w[3]}) ? 1 : 0;
-    launch(k_ss_p<T>, vg, VT, 0, st, g, sv, p, x, hx, ld, n, cz, s.bk, mloop, first, s.active,
-           (const int*)(first ? nullptr : s.pend), (const double*)s.u11, (const double*)s.u21, part, gv);
-    // <x|x>, <p|x>, <p|p>, <x|Hx>, <p|Hx> into dots[0..4] of each band (dots[5] = <p|Hp> after H p)
-    launch(k_finish_strided, div_up((long)mb * 5, 128), 128, 0, st, (const double*)part, nchunk, 5, mb, dV, s.dots,
-           6, (const int*)s.active);
+    const int gv = grp16_ok<T>(ld, {g, p, x, sv.w[0], sv.w[1], sv.w[2], sv.w[3]}) ? 1 : 0;
+    launch(k_ss_p<T>, vg, VT, 0, st, g, sv, p, x, ld, n, cz, s.bk, mloop, first, s.active,
+           (const int*)(first ? nullptr : s.pend), (const double*)s.u11, (const double*)s.u21, gv);
     RS_LAUNCH();
     return RSDFT_OK;
 }
 
-template int sstep_precond<double>(const double*, const SSVec<double>&, double*, double*, const double*, long, int,
-                                   int, int, const CGScal&, double*, double*, double*, const PcArgs&, double);
-template int sstep_precond<float>(const float*, const SSVec<float>&, float*, float*, const float*, long, int, int,
-                                  int, const CGScal&, double*, double*, double*, const PcArgs&, double);
+template int sstep_precond<double>(const double*, const SSVec<double>&, double*, double*, long, int, int, int,
+                                   const CGScal&, double*, double*, double*, const PcArgs&, double);
+template int sstep_precond<float>(const float*, const SSVec<float>&, float*, float*, long, int, int, int,
+                                  const CGScal&, double*, double*, double*, const PcArgs&, double);
 
 }  // namespace rsdft
