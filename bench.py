@@ -42,7 +42,7 @@ MODES = {"fp64": 0, "mixed-bf16": 1, "mixed-bf16x3": 2}
 def parse():
     p = argparse.ArgumentParser()
     p.add_argument("--gpus", type=int, default=1)
-    p.add_argument("--steps", type=int, default=5)
+    p.add_argument("--steps", type=int, default=20)
     p.add_argument("--warmup", type=int, default=3)
     p.add_argument("--impl", default="ours", choices=["ours", "reference"])
     p.add_argument("--workload", default="si216")
@@ -58,9 +58,15 @@ def parse():
 
 # ------------------------------------------------------------------ clocks
 class ClockSampler:
-    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+    """nvidia-smi clock / throttle samples (every 100 ms), each stamped by
+    nvidia-smi itself, so the ones inside a timed window can be picked out.
+    Started well before the window (nvidia-smi takes a few hundred ms to
+    print its first sample)."""
+
+    FIELDS = ("timestamp,index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
               "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
               "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+    REASONS = ("hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap")
 
     def __init__(self, gpu_index: int):
         self.idx = gpu_index
@@ -71,7 +77,7 @@ class ClockSampler:
         try:
             self.proc = subprocess.Popen(
                 ["nvidia-smi", "-i", str(self.idx), f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
-                 "-lms", "200"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+                 "-lms", "100"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
             self.t = threading.Thread(target=self._read, daemon=True)
             self.t.start()
         except (OSError, FileNotFoundError):
@@ -83,29 +89,49 @@ class ClockSampler:
 
     def stop(self):
         if self.proc is None:
-            return None
+            return
         self.proc.terminate()
         try:
             self.proc.wait(timeout=5)
         except subprocess.TimeoutExpired:
             self.proc.kill()
-        sm, mx, reasons = [], None, set()
-        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        for ln in self.lines:
+        self.t.join(timeout=2)  # the reader has taken every line once the pipe closes
+
+    @classmethod
+    def parse(cls, lines):
+        """(epoch seconds, sm MHz, max sm MHz, set of active reasons) per sample."""
+        out = []
+        for ln in lines:
             f = [x.strip() for x in ln.split(",")]
-            if len(f) < 9:
+            if len(f) < 10:
                 continue
             try:
-                sm.append(float(f[1]))
-                mx = float(f[2])
+                ts = time.mktime(time.strptime(f[0].split(".")[0], "%Y/%m/%d %H:%M:%S"))
+                ts += float("0." + f[0].split(".")[1]) if "." in f[0] else 0.0
+                sm, mx = float(f[2]), float(f[3])
             except ValueError:
                 continue
-            for n, v in zip(names, f[5:9]):
-                if v.lower().startswith("active"):
-                    reasons.add(n)
-        if not sm:
+            reasons = {n for n, v in zip(cls.REASONS, f[6:10]) if v.lower().startswith("active")}
+            out.append((ts, sm, mx, reasons))
+        return out
+
+    @classmethod
+    def summarize(cls, samples, t0, t1):
+        """Samples inside [t0, t1] (host wall clock); when the window is
+        shorter than the sampling period, the nearest sample on each side
+        (within 0.3 s: the GPU is busy with warm-up before and the next
+        phase after)."""
+        inside = [s for s in samples if t0 <= s[0] <= t1]
+        if not inside:
+            before = [s for s in samples if t0 - 0.3 <= s[0] < t0]
+            after = [s for s in samples if t1 < s[0] <= t1 + 0.3]
+            inside = before[-1:] + after[:1]
+        if not inside:
             return None
-        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": mx, "reasons": sorted(reasons), "samples": len(sm)}
+        reasons = set().union(*(s[3] for s in inside))
+        return {"sm_mhz": statistics.median(s[1] for s in inside), "sm_max_mhz": inside[-1][2],
+                "reasons": sorted(reasons), "samples": len(inside),
+                "window_s": round(t1 - t0, 3)}
 
 
 # ------------------------------------------------------------ CPU baseline
@@ -269,24 +295,26 @@ def main():
     results = {}
     clocks = None
     launches = 0
+    window = None
+    sampler = ClockSampler(local)
+    sampler.start()
     for mode in modes:
         u = start.t().contiguous().t()
         for _ in range(args.warmup):
             iterate(u, mode)
         barrier()
-        sampler = ClockSampler(local) if mode == head else None
-        if sampler:
-            sampler.start()
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         n0 = _lib.load().rsdft_gpu_kernel_launches()
+        w0 = time.time()
         e0.record(stream)
         for _ in range(args.steps):
             iterate(u, mode)
         e1.record(stream)
         barrier()
+        w1 = time.time()
         n1 = _lib.load().rsdft_gpu_kernel_launches()
-        if sampler:
-            clocks = sampler.stop()
+        if mode == head:
+            window = (w0, w1)
             launches = int(n1 - n0)
         ms = replicas.max_over_ranks(e0.elapsed_time(e1) / args.steps, pg, device="cuda")
         results[mode] = {"ms": ms, "esp": esp.cpu().numpy().copy()}
@@ -368,6 +396,13 @@ def main():
         dt = replicas.max_over_ranks((time.perf_counter() - t0) / args.steps, pg, device="cuda")
         e2e = {"value": replicas.whole_job_rate(1.0, world, dt), "unit": "iter/s", "h2d_bytes_per_step": ML * MB * 8,
                "d2h_bytes_per_step": ML * MB * 8 + 2 * MB * 8}
+
+    # clocks during the headline form's timed window (the sampler has run
+    # since before the first form's warm-up)
+    if window is not None and time.time() < window[1] + 0.35:
+        time.sleep(window[1] + 0.35 - time.time())
+    sampler.stop()
+    clocks = ClockSampler.summarize(ClockSampler.parse(sampler.lines), *window) if window else None
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
