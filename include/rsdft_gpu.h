@@ -206,6 +206,42 @@ int rsdft_gpu_force_nloc(int mi, const double *unk, long ld, int mb, const doubl
 int rsdft_gpu_hpsi_adjoint(const double *psi, const double *chi, long ld, int nb, const double *occ,
                            double *dl_dv, double *dl_dr);
 
+/* ------------------------------------------------------ wavefunction file */
+
+/* Write unk(ML, mb, mk, ms) (band stride ld, k stride ld*mb, spin stride
+ * ld*mb*mk; real Gamma data) to the wavefunction file of RSDFT, record for
+ * record: Fortran sequential unformatted records with 4-byte length markers;
+ * header, LL2(3,ML) grid map (x fastest), occ(mb,mk,ms), aa(3,3), bb(3,3),
+ * kbb(3,mmbz), the single-process layout records, then one record per band
+ * n = mbwr1..mbwr2 for every k and spin.  oc = 4 or 5 stores the bands in
+ * FP32, oc >= 10 writes the old format (no lattice or layout records), any
+ * other oc FP64.  io_ctrl = 0 puts everything in path; io_ctrl = 3 puts the
+ * band records in path.00000.  mbwr1/mbwr2 outside 1..mb are replaced by
+ * 1 and mb as the reference does.  occ, aa, bb and kbb may be NULL (zeros).
+ * unk may be a plain host array, a registered one (its device mirror is
+ * written) or device memory (both copied band by band through pinned
+ * buffers while the previous band is written).
+ * (replaces simple_wf_io_write(file_wf,IO_ctrl,OC,SYStype=0,MBwr1,MBwr2),
+ * io_write_module.f90:19-264, for one process) */
+int rsdft_gpu_write_wf(const char *path, const double *unk, long ld, int mb, int mk, int ms, int mbwr1, int mbwr2,
+                       int oc, int io_ctrl, const int *ngrid, const double *occ, const double *aa,
+                       const double *bb, int mmbz, const double *kbb);
+
+/* Read a wavefunction file written by RSDFT (new or old format, FP64 or
+ * FP32 bands, io_ctrl 0 or 3 as for the writer) into unk(ML, mb, mk, ms):
+ * the grid must match ngrid; grid points are placed through the file's
+ * LL2 map; bands, k points and spins beyond mb, mk, ms are skipped.
+ * occ(mb,mk,ms), if not NULL, receives the file's occupations over the
+ * common ranges.  info[13], if not NULL, receives the header: ML, ML1, ML2,
+ * ML3, MB, MB1, MB2, MK, MS, MMBZ, IO_ctrl, OC, TYPE_WF (the old format has
+ * no MK..TYPE_WF: mk, ms, 0, 0, 0, 0 are reported).  unk as for the writer:
+ * a registered array's device mirror, or device memory, is filled band by
+ * band through pinned buffers.
+ * (replaces simple_wf_io_read(file_wf,SYStype=0,IO_ctrl,...),
+ * io_read_module.f90:15-521, for one process) */
+int rsdft_gpu_read_wf(const char *path, double *unk, long ld, int mb, int mk, int ms, int io_ctrl,
+                      const int *ngrid, double *occ, int *info);
+
 #ifdef __cplusplus
 }
 #endif

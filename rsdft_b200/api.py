@@ -15,6 +15,8 @@ replace (j-iwata/RSDFT v1.3.0, src/):
 ``subspace_rotv_sl(k,s,unk,vsub)``    subspace_rotv_sl_module.f90:24
 ``calc_force_ps_nloc2(MI,force2,..)`` ps_nloc2_module.f90:1281
 ``hpsi_adjoint(psi, ...)``            (adjoint of op_localpot + op_ps_nloc2_hp)
+``write_wf(path, unk, ngrid, ...)``   io_write_module.f90:19 (simple_wf_io_write)
+``read_wf(path, unk, ngrid, ...)``    io_read_module.f90:15 (simple_wf_io_read)
 ====================================  ==========================================
 
 The reference routines read module state (``unk``, ``Vloc``, the projector
@@ -25,6 +27,8 @@ with strides ``(1, ML)`` (``fortran_empty`` makes one).  Every call raises
 ``RsdftError`` on a non-zero status; nothing falls back to the CPU.
 """
 from __future__ import annotations
+
+import os
 
 import numpy as np
 
@@ -76,6 +80,67 @@ def _ld(a) -> int:
     if _is_torch(a):
         return int(a.stride(1)) if a.dim() == 2 else int(a.shape[0])
     return int(a.strides[1] // a.itemsize) if a.ndim == 2 else int(a.shape[0])
+
+
+HEADER_FIELDS = ("ML", "ML1", "ML2", "ML3", "MB", "MB1", "MB2", "MK", "MS", "MMBZ", "IO_ctrl", "OC", "TYPE_WF")
+
+
+def _wf_dims(unk, mk, ms):
+    """(ld, mb, mk, ms) of a Fortran-ordered unk(ML, MB) or unk(ML, MB, MK, MS)."""
+    if unk.ndim == 4:
+        return int(unk.shape[0]), int(unk.shape[1]), int(unk.shape[2]), int(unk.shape[3])
+    if unk.ndim == 2:
+        nb = int(unk.shape[1])
+        if nb % (mk * ms) != 0:
+            raise ValueError(f"unk has {nb} columns, not a multiple of mk * ms = {mk * ms}")
+        return _ld(unk), nb // (mk * ms), mk, ms
+    raise ValueError("unk must be (ML, MB) or (ML, MB, MK, MS)")
+
+
+def _f64(a, shape, name):
+    if a is None:
+        return None
+    a = np.asfortranarray(a, dtype=np.float64)
+    if a.size != int(np.prod(shape)):
+        raise ValueError(f"{name}: {a.size} values, expected {shape}")
+    return a
+
+
+def write_wf(path, unk, ngrid, *, mk=1, ms=1, mbwr1=1, mbwr2=None, oc=0, io_ctrl=0, occ=None, aa=None, bb=None,
+             kbb=None) -> None:
+    """simple_wf_io_write (io_write_module.f90:19-264) for one process.
+
+    unk is Fortran-ordered (ML, MB) -- columns band-major over (k, spin) when
+    mk * ms > 1 -- or (ML, MB, MK, MS); a host array, a registered one, or a
+    device tensor.  oc = 4 or 5 writes FP32 bands, oc >= 10 the old format;
+    io_ctrl 3 writes the bands to path + ".00000".  Needs no device for host
+    arrays."""
+    ld, mb, mk, ms = _wf_dims(unk, mk, ms)
+    ng = np.ascontiguousarray(ngrid, dtype=np.int32)
+    occ = _f64(occ, (mb, mk, ms), "occ")
+    aa = _f64(aa, (3, 3), "aa")
+    bb = _f64(bb, (3, 3), "bb")
+    kbb = None if kbb is None else np.asfortranarray(np.asarray(kbb, dtype=np.float64).reshape(3, -1))
+    mmbz = 0 if kbb is None else kbb.shape[1]
+    _lib.call("rsdft_gpu_write_wf", os.fsencode(path), _ptr(unk, name="unk"), ld, mb, mk, ms, mbwr1,
+              mb if mbwr2 is None else mbwr2, oc, io_ctrl, ng.ctypes.data,
+              None if occ is None else occ.ctypes.data, None if aa is None else aa.ctypes.data,
+              None if bb is None else bb.ctypes.data, mmbz, None if kbb is None else kbb.ctypes.data)
+
+
+def read_wf(path, unk, ngrid, *, mk=1, ms=1, io_ctrl=0, occ=None) -> dict:
+    """simple_wf_io_read (io_read_module.f90:15-521) for one process: fills
+    unk (as for write_wf) and occ(MB, MK, MS) if given; returns the file's
+    header fields."""
+    ld, mb, mk, ms = _wf_dims(unk, mk, ms)
+    ng = np.ascontiguousarray(ngrid, dtype=np.int32)
+    if occ is not None and (not isinstance(occ, np.ndarray) or occ.dtype != np.float64 or not occ.flags.f_contiguous
+                            or occ.size != mb * mk * ms):
+        raise ValueError("occ must be a Fortran-ordered float64 array of MB * MK * MS values")
+    info = np.zeros(13, dtype=np.int32)
+    _lib.call("rsdft_gpu_read_wf", os.fsencode(path), _ptr(unk, name="unk"), ld, mb, mk, ms, io_ctrl, ng.ctypes.data,
+              None if occ is None else occ.ctypes.data, info.ctypes.data)
+    return dict(zip(HEADER_FIELDS, (int(v) for v in info)))
 
 
 class RsdftGpu:
@@ -185,6 +250,17 @@ class RsdftGpu:
     def hpsi_adjoint(self, psi, *, chi=None, occ=None, dl_dv=None, dl_dr=None) -> None:
         _lib.call("rsdft_gpu_hpsi_adjoint", _ptr(psi, name="psi"), _ptr(chi, name="chi"), _ld(psi), psi.shape[1],
                   _ptr(occ, name="occ"), _ptr(dl_dv, name="dl_dv"), _ptr(dl_dr, name="dl_dr"))
+
+    # ------------------------------------------------ wavefunction file
+    def write_wf(self, path, unk, *, mbwr1=1, mbwr2=None, oc=0, io_ctrl=0, occ=None, aa=None, bb=None,
+                 kbb=None, mk=1, ms=1) -> None:
+        """write_wf on this context's grid (see the module function)."""
+        write_wf(path, unk, self.cell.ngrid, mk=mk, ms=ms, mbwr1=mbwr1, mbwr2=mbwr2, oc=oc, io_ctrl=io_ctrl, occ=occ,
+                 aa=aa, bb=bb, kbb=kbb)
+
+    def read_wf(self, path, unk, *, io_ctrl=0, occ=None, mk=1, ms=1) -> dict:
+        """read_wf on this context's grid (see the module function)."""
+        return read_wf(path, unk, self.cell.ngrid, mk=mk, ms=ms, io_ctrl=io_ctrl, occ=occ)
 
     # --------------------------------------------------------- composite
     def finalize_fp64(self, unk, esp, res) -> None:

@@ -1,0 +1,422 @@
+// RSDFT's wavefunction file (wf.dat1), written and read for one process.
+//
+// Format (simple_wf_io_write, io_write_module.f90:19-264; read back by
+// simple_wf_io_read, io_read_module.f90:15-521): Fortran sequential
+// unformatted records, each framed by a 4-byte little-endian length marker
+// before and after it (the default of the Fortran compilers RSDFT builds
+// with; records above 2^31 - 9 bytes, which need split records, are
+// refused).  New format (OC < 10):
+//   -1 | ML, ML1, ML2, ML3 | MB, MBwr1, MBwr2 | MK, MS, MMBZ |
+//   IO_ctrl, OC, TYPE_WF | LL2(3, ML) | occ(MB, MK, MS) | aa, bb, kbb(3, MMBZ) |
+//   np(0:7) | grid id, ir | band id, ir | bzsm id, ir | spin id, ir |
+//   then unk(:, n, k, s) for s = 1..MS, k = 1..MK, n = MBwr1..MBwr2,
+//   real(8) or, for OC = 4 and 5, real(4).
+// Old format (OC >= 10): ML.. | MB.. | LL2 | occ | bands (real(8)).
+// TYPE_WF = 1 marks real (Gamma) data.  With one process the layout records
+// are np = 1 and id = 0, ir = the full count in each dimension, and LL2 lists
+// the grid points x fastest (SYStype = 0 over the whole grid).
+//
+// Device-resident arrays (a registered host array's mirror, or device
+// memory) move band by band through two pinned buffers: the copy of the
+// next band runs while the current one is written (or, reading, the copy of
+// the current band while the next one is read).
+#include <algorithm>
+#include <cstdint>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "common.cuh"
+
+namespace rsdft {
+namespace {
+
+constexpr size_t kMaxRecord = 2147483639;  // one pair of 4-byte markers
+
+struct File {
+    FILE* f = nullptr;
+    std::vector<char> vbuf;
+    std::string path;
+    ~File() {
+        if (f) fclose(f);
+    }
+    int open(const std::string& p, const char* mode) {
+        path = p;
+        f = fopen(p.c_str(), mode);
+        if (!f) {
+            set_error("cannot open '%s' (mode %s)", p.c_str(), mode);
+            return RSDFT_EINVAL;
+        }
+        vbuf.resize((size_t)8 << 20);
+        setvbuf(f, vbuf.data(), _IOFBF, vbuf.size());
+        return RSDFT_OK;
+    }
+    int close() {
+        const int rc = fclose(f);
+        f = nullptr;
+        if (rc != 0) {
+            set_error("error closing '%s'", path.c_str());
+            return RSDFT_EINVAL;
+        }
+        return RSDFT_OK;
+    }
+};
+
+struct Part {
+    const void* p;
+    size_t n;
+};
+
+int write_record(File& fh, std::initializer_list<Part> parts) {
+    size_t len = 0;
+    for (const Part& q : parts) len += q.n;
+    if (len > kMaxRecord) {
+        set_error("'%s': record of %zu bytes exceeds one 4-byte-marker record", fh.path.c_str(), len);
+        return RSDFT_EUNSUP;
+    }
+    const int32_t m = (int32_t)len;
+    bool ok = fwrite(&m, 4, 1, fh.f) == 1;
+    for (const Part& q : parts) ok = ok && (q.n == 0 || fwrite(q.p, 1, q.n, fh.f) == q.n);
+    ok = ok && fwrite(&m, 4, 1, fh.f) == 1;
+    if (!ok) {
+        set_error("write to '%s' failed", fh.path.c_str());
+        return RSDFT_EINVAL;
+    }
+    return RSDFT_OK;
+}
+
+template <typename T>
+int write_values(File& fh, const std::vector<T>& v) {
+    return write_record(fh, {{v.data(), v.size() * sizeof(T)}});
+}
+
+// Leading marker of the next record; *len = its length in bytes.
+int record_head(File& fh, size_t* len, const char* what) {
+    int32_t m = 0;
+    if (fread(&m, 4, 1, fh.f) != 1) {
+        set_error("'%s': file ends before the %s record", fh.path.c_str(), what);
+        return RSDFT_EINVAL;
+    }
+    if (m < 0) {
+        set_error("'%s': the %s record is split (over 2 GiB); not supported", fh.path.c_str(), what);
+        return RSDFT_EUNSUP;
+    }
+    *len = (size_t)m;
+    return RSDFT_OK;
+}
+
+int record_tail(File& fh, size_t len, const char* what) {
+    int32_t m = 0;
+    if (fread(&m, 4, 1, fh.f) != 1 || (size_t)m != len) {
+        set_error("'%s': bad length marker after the %s record", fh.path.c_str(), what);
+        return RSDFT_EINVAL;
+    }
+    return RSDFT_OK;
+}
+
+// Read a record of at least `bytes` bytes into dst (a Fortran read may take
+// fewer items than the record holds; the rest is skipped).
+int read_record(File& fh, void* dst, size_t bytes, const char* what) {
+    size_t len = 0;
+    RS_CHECK(record_head(fh, &len, what));
+    if (len < bytes) {
+        set_error("'%s': the %s record holds %zu bytes, %zu expected", fh.path.c_str(), what, len, bytes);
+        return RSDFT_EINVAL;
+    }
+    if (bytes && fread(dst, 1, bytes, fh.f) != bytes) {
+        set_error("'%s': file ends inside the %s record", fh.path.c_str(), what);
+        return RSDFT_EINVAL;
+    }
+    if (len > bytes && fseek(fh.f, (long)(len - bytes), SEEK_CUR) != 0) {
+        set_error("'%s': seek failed in the %s record", fh.path.c_str(), what);
+        return RSDFT_EINVAL;
+    }
+    return record_tail(fh, len, what);
+}
+
+int skip_record(File& fh, const char* what) { return read_record(fh, nullptr, 0, what); }
+
+// Where the bands live: a host array, or device memory (a registered array's
+// mirror, or a device pointer), moved through two pinned band buffers.
+struct Bands {
+    double* host = nullptr;  // plain host array
+    double* dev = nullptr;   // device-resident
+    double* pin[2] = {nullptr, nullptr};
+    cudaEvent_t ev[2] = {nullptr, nullptr};
+    ~Bands() {
+        for (int i = 0; i < 2; ++i) {
+            if (pin[i]) cudaFreeHost(pin[i]);
+            if (ev[i]) cudaEventDestroy(ev[i]);
+        }
+    }
+};
+
+// Resolve unk; for device-resident data check the extent against a
+// registration and set up the pinned buffers.
+int bands_open(Bands& b, const double* unk, size_t span, long ml) {
+    void* d = nullptr;
+    if (!resolve(unk, &d)) {
+        b.host = const_cast<double*>(unk);
+        return RSDFT_OK;
+    }
+    RS_CHECK(require_init());
+    const char* c = reinterpret_cast<const char*>(unk);
+    for (const auto& r : ctx().regs) {
+        if (c >= r.host && c < r.host + r.bytes && c + span * sizeof(double) > r.host + r.bytes) {
+            set_error("wavefunction file: the array extends past its registered range");
+            return RSDFT_EINVAL;
+        }
+    }
+    b.dev = static_cast<double*>(d);
+    for (int i = 0; i < 2; ++i) {
+        RS_CUDA(cudaMallocHost(&b.pin[i], sizeof(double) * (size_t)ml));
+        RS_CUDA(cudaEventCreateWithFlags(&b.ev[i], cudaEventDisableTiming));
+    }
+    return RSDFT_OK;
+}
+
+bool oc_single(int oc) { return oc == 4 || oc == 5; }
+
+std::string split_name(const char* path) { return std::string(path) + ".00000"; }
+
+}  // namespace
+}  // namespace rsdft
+
+using namespace rsdft;
+
+extern "C" int rsdft_gpu_write_wf(const char* path, const double* unk, long ld, int mb, int mk, int ms, int mbwr1,
+                                  int mbwr2, int oc, int io_ctrl, const int* ngrid, const double* occ,
+                                  const double* aa, const double* bb, int mmbz, const double* kbb) {
+    if (!path || !unk || !ngrid || mb < 1 || mk < 1 || ms < 1 || mmbz < 0) {
+        set_error("write_wf: NULL path/unk/ngrid or bad counts");
+        return RSDFT_EINVAL;
+    }
+    if (io_ctrl != 0 && io_ctrl != 3) {
+        set_error("write_wf: io_ctrl %d (only 0 and 3 are written)", io_ctrl);
+        return RSDFT_EUNSUP;
+    }
+    const int n1 = ngrid[0], n2 = ngrid[1], n3 = ngrid[2];
+    if (n1 < 1 || n2 < 1 || n3 < 1) {
+        set_error("write_wf: bad grid %d x %d x %d", n1, n2, n3);
+        return RSDFT_EINVAL;
+    }
+    const long ml = (long)n1 * n2 * n3;
+    if (ld < ml) {
+        set_error("write_wf: ld %ld < ML %ld", ld, ml);
+        return RSDFT_EINVAL;
+    }
+    // the reference's own correction of the band range (io_write_module.f90:80-81)
+    if (mbwr1 < 1 || mbwr2 < mbwr1 || mb < mbwr1) mbwr1 = 1;
+    if (mbwr2 < 1 || mbwr2 < mbwr1 || mb < mbwr2) mbwr2 = mb;
+    const bool single = oc_single(oc), oldfmt = oc >= 10;
+
+    Bands b;
+    const size_t span = (size_t)ld * ((size_t)mb * mk * ms - 1) + (size_t)ml;
+    RS_CHECK(bands_open(b, unk, span, ml));
+
+    File fh;
+    RS_CHECK(fh.open(path, "wb"));
+    // ---- header
+    std::vector<int32_t> ll2((size_t)3 * ml);
+    for (long i = 0; i < ml; ++i) {
+        ll2[3 * i] = (int32_t)(i % n1);
+        ll2[3 * i + 1] = (int32_t)((i / n1) % n2);
+        ll2[3 * i + 2] = (int32_t)(i / ((long)n1 * n2));
+    }
+    std::vector<double> occv((size_t)mb * mk * ms, 0.0);
+    if (occ) std::memcpy(occv.data(), occ, occv.size() * sizeof(double));
+    const std::vector<int32_t> dims{(int32_t)ml, n1, n2, n3}, bands{mb, mbwr1, mbwr2};
+    if (!oldfmt) {
+        RS_CHECK(write_values(fh, std::vector<int32_t>{-1}));
+        RS_CHECK(write_values(fh, dims));
+        RS_CHECK(write_values(fh, bands));
+        RS_CHECK(write_values(fh, std::vector<int32_t>{mk, ms, mmbz}));
+        RS_CHECK(write_values(fh, std::vector<int32_t>{io_ctrl, oc, 1}));
+        RS_CHECK(write_values(fh, ll2));
+        RS_CHECK(write_values(fh, occv));
+        std::vector<double> lat(18 + (size_t)3 * mmbz, 0.0);
+        if (aa) std::memcpy(lat.data(), aa, 9 * sizeof(double));
+        if (bb) std::memcpy(lat.data() + 9, bb, 9 * sizeof(double));
+        if (kbb && mmbz > 0) std::memcpy(lat.data() + 18, kbb, (size_t)3 * mmbz * sizeof(double));
+        RS_CHECK(write_values(fh, lat));
+        RS_CHECK(write_values(fh, std::vector<int32_t>(8, 1)));  // np(0:7) of one process
+        for (int32_t count : {(int32_t)ml, mb, mk, ms}) RS_CHECK(write_values(fh, std::vector<int32_t>{0, count}));
+    } else {
+        RS_CHECK(write_values(fh, dims));
+        RS_CHECK(write_values(fh, bands));
+        RS_CHECK(write_values(fh, ll2));
+        RS_CHECK(write_values(fh, occv));
+    }
+    File split;
+    File* out = &fh;
+    if (io_ctrl == 3) {
+        RS_CHECK(fh.close());
+        RS_CHECK(split.open(split_name(path), "wb"));
+        out = &split;
+    }
+    // ---- bands: s, k, n = mbwr1..mbwr2
+    std::vector<long> offs;
+    for (int s = 0; s < ms; ++s)
+        for (int k = 0; k < mk; ++k)
+            for (int n = mbwr1 - 1; n < mbwr2; ++n) offs.push_back(ld * ((long)n + (long)mb * (k + (long)mk * s)));
+    std::vector<float> sp(single ? (size_t)ml : 0);
+    cudaStream_t st = b.dev ? ctx().stream : nullptr;
+    auto issue = [&](size_t i) -> int {
+        RS_CUDA(cudaMemcpyAsync(b.pin[i & 1], b.dev + offs[i], sizeof(double) * (size_t)ml, cudaMemcpyDeviceToHost,
+                                st));
+        RS_CUDA(cudaEventRecord(b.ev[i & 1], st));
+        return RSDFT_OK;
+    };
+    if (b.dev && !offs.empty()) RS_CHECK(issue(0));
+    for (size_t i = 0; i < offs.size(); ++i) {
+        const double* src = b.host ? b.host + offs[i] : b.pin[i & 1];
+        if (b.dev) {
+            RS_CUDA(cudaEventSynchronize(b.ev[i & 1]));
+            if (i + 1 < offs.size()) RS_CHECK(issue(i + 1));  // into the buffer written out last round
+        }
+        if (single) {
+            for (long j = 0; j < ml; ++j) sp[j] = (float)src[j];
+            RS_CHECK(write_values(*out, sp));
+        } else {
+            RS_CHECK(write_record(*out, {{src, sizeof(double) * (size_t)ml}}));
+        }
+    }
+    return out->close();
+}
+
+extern "C" int rsdft_gpu_read_wf(const char* path, double* unk, long ld, int mb, int mk, int ms, int io_ctrl,
+                                 const int* ngrid, double* occ, int* info) {
+    if (!path || !unk || !ngrid || mb < 1 || mk < 1 || ms < 1) {
+        set_error("read_wf: NULL path/unk/ngrid or bad counts");
+        return RSDFT_EINVAL;
+    }
+    if (io_ctrl != 0 && io_ctrl != 3) {
+        set_error("read_wf: io_ctrl %d (only 0 and 3 are read)", io_ctrl);
+        return RSDFT_EUNSUP;
+    }
+    const int n1 = ngrid[0], n2 = ngrid[1], n3 = ngrid[2];
+    if (n1 < 1 || n2 < 1 || n3 < 1) {
+        set_error("read_wf: bad grid %d x %d x %d", n1, n2, n3);
+        return RSDFT_EINVAL;
+    }
+    const long ml = (long)n1 * n2 * n3;
+    if (ld < ml) {
+        set_error("read_wf: ld %ld < ML %ld", ld, ml);
+        return RSDFT_EINVAL;
+    }
+    File fh;
+    RS_CHECK(fh.open(path, "rb"));
+    // ---- header (io_read_module.f90:126-150)
+    int32_t first = 0;
+    size_t len = 0;
+    RS_CHECK(record_head(fh, &len, "first"));
+    const bool newfmt = len >= 4 && fread(&first, 4, 1, fh.f) == 1 && first < 0;
+    if (newfmt) {
+        if (len > 4) fseek(fh.f, (long)(len - 4), SEEK_CUR);
+        RS_CHECK(record_tail(fh, len, "first"));
+    } else {
+        rewind(fh.f);
+    }
+    int32_t h[13] = {0};
+    RS_CHECK(read_record(fh, h, 4 * sizeof(int32_t), "grid size"));
+    RS_CHECK(read_record(fh, h + 4, 3 * sizeof(int32_t), "band range"));
+    if (newfmt) {
+        RS_CHECK(read_record(fh, h + 7, 3 * sizeof(int32_t), "k/spin count"));
+        RS_CHECK(read_record(fh, h + 10, 3 * sizeof(int32_t), "io/precision flags"));
+    } else {
+        h[7] = mk;  // the old format has no k / spin counts: the caller's (io_read_module.f90:146-147)
+        h[8] = ms;
+    }
+    if (info) std::memcpy(info, h, sizeof(h));
+    if (h[0] != ml || h[1] != n1 || h[2] != n2 || h[3] != n3) {
+        set_error("read_wf: file grid %d (%d x %d x %d), expected %ld (%d x %d x %d)", h[0], h[1], h[2], h[3], ml,
+                  n1, n2, n3);
+        return RSDFT_EINVAL;
+    }
+    const int fmb = h[4], fmb1 = h[5], fmb2 = h[6], fmk = h[7], fms = h[8], fmmbz = h[9], foc = h[11];
+    if (fmb < 1 || fmb1 < 1 || fmb2 < fmb1 || fmk < 1 || fms < 1 || fmmbz < 0) {
+        set_error("read_wf: bad counts in the header (MB %d, %d..%d, MK %d, MS %d)", fmb, fmb1, fmb2, fmk, fms);
+        return RSDFT_EINVAL;
+    }
+    if (newfmt && h[12] != 1) {
+        set_error("read_wf: TYPE_WF %d (complex data) in a real Gamma-point read", h[12]);
+        return RSDFT_EUNSUP;
+    }
+    const bool single = newfmt && oc_single(foc);
+    // ---- grid map: file point i -> grid index
+    std::vector<int32_t> ll2((size_t)3 * ml);
+    RS_CHECK(read_record(fh, ll2.data(), ll2.size() * sizeof(int32_t), "LL2"));
+    std::vector<long> perm((size_t)ml);
+    std::vector<char> seen((size_t)ml, 0);
+    bool identity = true;
+    for (long i = 0; i < ml; ++i) {
+        const int a = ll2[3 * i], b2 = ll2[3 * i + 1], c = ll2[3 * i + 2];
+        if (a < 0 || a >= n1 || b2 < 0 || b2 >= n2 || c < 0 || c >= n3) {
+            set_error("read_wf: LL2 point %ld = (%d, %d, %d) outside the grid", i + 1, a, b2, c);
+            return RSDFT_EINVAL;
+        }
+        const long j = a + (long)n1 * (b2 + (long)n2 * c);
+        if (seen[j]++) {
+            set_error("read_wf: LL2 lists grid point (%d, %d, %d) twice", a, b2, c);
+            return RSDFT_EINVAL;
+        }
+        perm[i] = j;
+        identity = identity && j == i;
+    }
+    // ---- occupations over the common ranges (io_read_module.f90:218-237)
+    std::vector<double> focc((size_t)fmb * fmk * fms);
+    RS_CHECK(read_record(fh, focc.data(), focc.size() * sizeof(double), "occ"));
+    if (occ) {
+        for (int s = 0; s < std::min(ms, fms); ++s)
+            for (int k = 0; k < std::min(mk, fmk); ++k)
+                for (int n = 0; n < std::min(mb, fmb); ++n)
+                    occ[n + (long)mb * (k + (long)mk * s)] = focc[n + (long)fmb * (k + (long)fmk * s)];
+    }
+    if (newfmt) {
+        RS_CHECK(skip_record(fh, "lattice"));
+        for (const char* w : {"np", "grid layout", "band layout", "k layout", "spin layout"})
+            RS_CHECK(skip_record(fh, w));
+    }
+    File split;
+    File* in = &fh;
+    if (io_ctrl == 3) {
+        RS_CHECK(split.open(split_name(path), "rb"));
+        in = &split;
+    }
+    // ---- bands
+    Bands b;
+    const size_t span = (size_t)ld * ((size_t)mb * mk * ms - 1) + (size_t)ml;
+    RS_CHECK(bands_open(b, unk, span, ml));
+    cudaStream_t st = b.dev ? ctx().stream : nullptr;
+    std::vector<float> sp(single ? (size_t)ml : 0);
+    std::vector<double> tmp(identity ? 0 : (size_t)ml);
+    size_t used = 0;  // bands copied to the device so far (pinned buffer use count)
+    for (int s = 0; s < fms; ++s)
+        for (int k = 0; k < fmk; ++k)
+            for (int n = fmb1 - 1; n < fmb2; ++n) {
+                if (n >= mb || k >= mk || s >= ms) {
+                    RS_CHECK(skip_record(*in, "band"));
+                    continue;
+                }
+                const long off = ld * ((long)n + (long)mb * (k + (long)mk * s));
+                double* dst = b.host ? b.host + off : b.pin[used & 1];
+                if (b.dev && used >= 2) RS_CUDA(cudaEventSynchronize(b.ev[used & 1]));  // its last copy is done
+                double* land = identity ? dst : tmp.data();
+                if (single) {
+                    RS_CHECK(read_record(*in, sp.data(), sp.size() * sizeof(float), "band"));
+                    for (long j = 0; j < ml; ++j) land[j] = (double)sp[j];
+                } else {
+                    RS_CHECK(read_record(*in, land, sizeof(double) * (size_t)ml, "band"));
+                }
+                if (!identity)
+                    for (long j = 0; j < ml; ++j) dst[perm[j]] = tmp[j];
+                if (b.dev) {
+                    RS_CUDA(cudaMemcpyAsync(b.dev + off, dst, sizeof(double) * (size_t)ml, cudaMemcpyHostToDevice, st));
+                    RS_CUDA(cudaEventRecord(b.ev[used & 1], st));
+                    ++used;
+                }
+            }
+    if (b.dev) RS_CUDA(cudaStreamSynchronize(st));
+    return RSDFT_OK;
+}

@@ -13,6 +13,8 @@
 ! gpu_subspace_rotv_sl          subspace_rotv_sl       subspace_rotv_sl_module.f90:24
 ! gpu_esp_calc                  esp_calc               esp_calc_module.f90:15
 ! gpu_calc_force_ps_nloc2       calc_force_ps_nloc2    ps_nloc2_module.f90:1281
+! gpu_wf_io_write               simple_wf_io_write     io_write_module.f90:19
+! gpu_wf_io_read                simple_wf_io_read      io_read_module.f90:15
 !
 ! Real Gamma-point build only (-D_DRSDFT_), one MPI rank per GPU.  Arrays are
 ! passed by address (c_loc); a non-zero status stops the program with the
@@ -27,7 +29,8 @@ MODULE rsdft_gpu_mod
   PRIVATE
   PUBLIC :: gpu_init, gpu_setup_grid, gpu_setup_vloc, gpu_setup_nonlocal, gpu_register_wf, gpu_sync_to_host, &
             gpu_sync_to_device, gpu_hamiltonian, gpu_conjugate_gradient, gpu_gram_schmidt, gpu_subspace_diag, &
-            gpu_subspace_mate_sl, gpu_subspace_solv_sl, gpu_subspace_rotv_sl, gpu_esp_calc, gpu_calc_force_ps_nloc2
+            gpu_subspace_mate_sl, gpu_subspace_solv_sl, gpu_subspace_rotv_sl, gpu_esp_calc, gpu_calc_force_ps_nloc2, &
+            gpu_wf_io_write, gpu_wf_io_read
 
   integer(c_int), parameter, PUBLIC :: RSDFT_MODE_FP64 = 0, RSDFT_MODE_MIXED_BF16 = 1, RSDFT_MODE_MIXED_BF16X3 = 2
 
@@ -143,6 +146,20 @@ MODULE rsdft_gpu_mod
        type(c_ptr), value :: unk, occ, force2
        integer(c_long), value :: ld
      end function rsdft_gpu_force_nloc
+     integer(c_int) function rsdft_gpu_write_wf(path, unk, ld, mb, mk, ms, mbwr1, mbwr2, oc, io_ctrl, ngrid, occ, &
+          aa, bb, mmbz, kbb) bind(C, name="rsdft_gpu_write_wf")
+       import :: c_int, c_long, c_ptr
+       type(c_ptr), value :: path, unk, ngrid, occ, aa, bb, kbb
+       integer(c_long), value :: ld
+       integer(c_int), value :: mb, mk, ms, mbwr1, mbwr2, oc, io_ctrl, mmbz
+     end function rsdft_gpu_write_wf
+     integer(c_int) function rsdft_gpu_read_wf(path, unk, ld, mb, mk, ms, io_ctrl, ngrid, occ, info) &
+          bind(C, name="rsdft_gpu_read_wf")
+       import :: c_int, c_long, c_ptr
+       type(c_ptr), value :: path, unk, ngrid, occ, info
+       integer(c_long), value :: ld
+       integer(c_int), value :: mb, mk, ms, io_ctrl
+     end function rsdft_gpu_read_wf
   end interface
 
 CONTAINS
@@ -329,5 +346,54 @@ CONTAINS
     call check(rsdft_gpu_force_nloc(int(mi, c_int), c_loc(unk), int(size(unk, 1), c_long), &
                int(size(unk, 2), c_int), c_loc(occ), c_loc(force2)), "calc_force_ps_nloc2")
   END SUBROUTINE gpu_calc_force_ps_nloc2
+
+  ! file name as a NUL-terminated C string
+  SUBROUTINE c_path(file, buf)
+    character(*), intent(IN) :: file
+    character(kind=c_char), allocatable, intent(OUT) :: buf(:)
+    integer :: i, n
+    n = len_trim(file)
+    allocate( buf(n + 1) )
+    do i = 1, n
+       buf(i) = file(i:i)
+    end do
+    buf(n + 1) = c_null_char
+  END SUBROUTINE c_path
+
+  ! simple_wf_io_write(file_wf, IO_ctrl, OC, SYStype=0, MBwr1, MBwr2, ...)
+  ! (io_write_module.f90:19) for one process, from the device mirror of a
+  ! registered unk; Ngrid(1:3), occ, aa, bb, kbb(3,MMBZ) as in the modules
+  ! the reference writer reads.
+  SUBROUTINE gpu_wf_io_write(file_wf, io_ctrl, oc, mbwr1, mbwr2, unk, ngrid, occ, aa, bb, kbb)
+    character(*), intent(IN) :: file_wf
+    integer, intent(IN) :: io_ctrl, oc, mbwr1, mbwr2, ngrid(3)
+    real(8), intent(IN), target :: unk(:, :, :, :), occ(:, :, :), aa(3, 3), bb(3, 3), kbb(:, :)
+    character(kind=c_char), allocatable, target :: cpath(:)
+    integer(c_int), target :: ng(3)
+    real(c_double), target :: a(3, 3), b(3, 3)
+    ng = ngrid
+    a = aa
+    b = bb
+    call c_path(file_wf, cpath)
+    call check(rsdft_gpu_write_wf(c_loc(cpath), c_loc(unk), int(size(unk, 1), c_long), int(size(unk, 2), c_int), &
+               int(size(unk, 3), c_int), int(size(unk, 4), c_int), int(mbwr1, c_int), int(mbwr2, c_int), &
+               int(oc, c_int), int(io_ctrl, c_int), c_loc(ng), c_loc(occ), c_loc(a), c_loc(b), &
+               int(size(kbb, 2), c_int), c_loc(kbb)), "wf_io_write")
+  END SUBROUTINE gpu_wf_io_write
+
+  ! simple_wf_io_read(file_wf, SYStype=0, IO_ctrl, ...) (io_read_module.f90:15)
+  ! for one process, into the device mirror of a registered unk and occ.
+  SUBROUTINE gpu_wf_io_read(file_wf, io_ctrl, unk, ngrid, occ)
+    character(*), intent(IN) :: file_wf
+    integer, intent(IN) :: io_ctrl, ngrid(3)
+    real(8), intent(INOUT), target :: unk(:, :, :, :), occ(:, :, :)
+    character(kind=c_char), allocatable, target :: cpath(:)
+    integer(c_int), target :: ng(3), info(13)
+    ng = ngrid
+    call c_path(file_wf, cpath)
+    call check(rsdft_gpu_read_wf(c_loc(cpath), c_loc(unk), int(size(unk, 1), c_long), int(size(unk, 2), c_int), &
+               int(size(unk, 3), c_int), int(size(unk, 4), c_int), int(io_ctrl, c_int), c_loc(ng), c_loc(occ), &
+               c_loc(info)), "wf_io_read")
+  END SUBROUTINE gpu_wf_io_read
 
 END MODULE rsdft_gpu_mod
