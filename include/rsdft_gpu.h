@@ -206,6 +206,13 @@ int rsdft_gpu_force_nloc(int mi, const double *unk, long ld, int mb, const doubl
 int rsdft_gpu_hpsi_adjoint(const double *psi, const double *chi, long ld, int nb, const double *occ,
                            double *dl_dv, double *dl_dr);
 
+/* Electron density of one (k, spin) block: rho(r) = sum_n occ(n) unk(r,n)^2
+ * over the mb bands (occ(n) = 0 skipped), rho(ML) overwritten; a caller with
+ * several k points or spins adds the blocks.  (replaces the NCPP branch of
+ * calc_density, density_module.f90:115-138, for one block; no symmetry
+ * operations) */
+int rsdft_gpu_calc_density(const double *unk, long ld, int mb, const double *occ, double *rho);
+
 /* ------------------------------------------------------ wavefunction file */
 
 /* Write unk(ML, mb, mk, ms) (band stride ld, k stride ld*mb, spin stride

@@ -45,6 +45,7 @@ SIGNATURES = {
     "rsdft_gpu_residual": (_c_int, [_c_int, _c_int, _vp, _c_long, _c_int, _vp, _vp]),
     "rsdft_gpu_force_nloc": (_c_int, [_c_int, _vp, _c_long, _c_int, _vp, _vp]),
     "rsdft_gpu_hpsi_adjoint": (_c_int, [_vp, _vp, _c_long, _c_int, _vp, _vp, _vp]),
+    "rsdft_gpu_calc_density": (_c_int, [_vp, _c_long, _c_int, _vp, _vp]),
     "rsdft_gpu_write_wf": (_c_int, [ctypes.c_char_p, _vp, _c_long, _c_int, _c_int, _c_int, _c_int, _c_int, _c_int,
                                     _c_int, _vp, _vp, _vp, _vp, _c_int, _vp]),
     "rsdft_gpu_read_wf": (_c_int, [ctypes.c_char_p, _vp, _c_long, _c_int, _c_int, _c_int, _c_int, _vp, _vp, _vp]),

@@ -15,6 +15,7 @@ replace (j-iwata/RSDFT v1.3.0, src/):
 ``subspace_rotv_sl(k,s,unk,vsub)``    subspace_rotv_sl_module.f90:24
 ``calc_force_ps_nloc2(MI,force2,..)`` ps_nloc2_module.f90:1281
 ``hpsi_adjoint(psi, ...)``            (adjoint of op_localpot + op_ps_nloc2_hp)
+``calc_density(unk, occ, rho)``      density_module.f90:115 (calc_density, NCPP)
 ``write_wf(path, unk, ngrid, ...)``   io_write_module.f90:19 (simple_wf_io_write)
 ``read_wf(path, unk, ngrid, ...)``    io_read_module.f90:15 (simple_wf_io_read)
 ====================================  ==========================================
@@ -250,6 +251,12 @@ class RsdftGpu:
     def hpsi_adjoint(self, psi, *, chi=None, occ=None, dl_dv=None, dl_dr=None) -> None:
         _lib.call("rsdft_gpu_hpsi_adjoint", _ptr(psi, name="psi"), _ptr(chi, name="chi"), _ld(psi), psi.shape[1],
                   _ptr(occ, name="occ"), _ptr(dl_dv, name="dl_dv"), _ptr(dl_dr, name="dl_dr"))
+
+    def calc_density(self, unk, occ, rho) -> None:
+        """rho(ML) = sum_n occ(n) unk(:, n)^2 (calc_density's NCPP branch,
+        density_module.f90:129-136, for one k / spin block)."""
+        _lib.call("rsdft_gpu_calc_density", _ptr(unk, name="unk"), _ld(unk), unk.shape[1], _ptr(occ, name="occ"),
+                  _ptr(rho, name="rho"))
 
     # ------------------------------------------------ wavefunction file
     def write_wf(self, path, unk, *, mbwr1=1, mbwr2=None, oc=0, io_ctrl=0, occ=None, aa=None, bb=None,

@@ -258,4 +258,25 @@ int rsdft_gpu_hpsi_adjoint(const double* psi, const double* chi, long ld, int nb
     return RSDFT_OK;
 }
 
+int rsdft_gpu_calc_density(const double* unk, long ld, int mb, const double* occ, double* rho) {
+    RS_CHECK(require_grid());
+    Context& c = ctx();
+    if (ld < c.ml || mb < 1 || !occ || !rho) {
+        set_error("calc_density: bad arguments");
+        return RSDFT_EINVAL;
+    }
+    double *dp, *docc = nullptr, *dr = nullptr;
+    bool sp;
+    RS_CHECK(wf_acquire(unk, ld, mb, "adj_psi", &dp, &sp));
+    RS_CHECK(stage_in(occ, sizeof(double) * mb, "adj_occ", (void**)&docc));
+    RS_CHECK(workspace_t("adj_dv", (size_t)c.ml, &dr));
+    // the V-part adjoint with unit volume element: sum_n occ_n psi_n^2
+    launch(k_vloc_adjoint, div_up(c.ml, 256), 256, 0, c.stream, dp, (const double*)nullptr, ld, mb,
+           (const double*)docc, 1.0, c.ml, dr);
+    RS_LAUNCH();
+    RS_CHECK(stage_out(rho, dr, sizeof(double) * c.ml));
+    (void)sp;
+    return RSDFT_OK;
+}
+
 }  // extern "C"

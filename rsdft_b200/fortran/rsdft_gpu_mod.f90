@@ -13,6 +13,7 @@
 ! gpu_subspace_rotv_sl          subspace_rotv_sl       subspace_rotv_sl_module.f90:24
 ! gpu_esp_calc                  esp_calc               esp_calc_module.f90:15
 ! gpu_calc_force_ps_nloc2       calc_force_ps_nloc2    ps_nloc2_module.f90:1281
+! gpu_calc_density              calc_density (NCPP)    density_module.f90:115
 ! gpu_wf_io_write               simple_wf_io_write     io_write_module.f90:19
 ! gpu_wf_io_read                simple_wf_io_read      io_read_module.f90:15
 !
@@ -30,7 +31,7 @@ MODULE rsdft_gpu_mod
   PUBLIC :: gpu_init, gpu_setup_grid, gpu_setup_vloc, gpu_setup_nonlocal, gpu_register_wf, gpu_sync_to_host, &
             gpu_sync_to_device, gpu_hamiltonian, gpu_conjugate_gradient, gpu_gram_schmidt, gpu_subspace_diag, &
             gpu_subspace_mate_sl, gpu_subspace_solv_sl, gpu_subspace_rotv_sl, gpu_esp_calc, gpu_calc_force_ps_nloc2, &
-            gpu_wf_io_write, gpu_wf_io_read
+            gpu_calc_density, gpu_wf_io_write, gpu_wf_io_read
 
   integer(c_int), parameter, PUBLIC :: RSDFT_MODE_FP64 = 0, RSDFT_MODE_MIXED_BF16 = 1, RSDFT_MODE_MIXED_BF16X3 = 2
 
@@ -146,6 +147,12 @@ MODULE rsdft_gpu_mod
        type(c_ptr), value :: unk, occ, force2
        integer(c_long), value :: ld
      end function rsdft_gpu_force_nloc
+     integer(c_int) function rsdft_gpu_calc_density(unk, ld, mb, occ, rho) bind(C, name="rsdft_gpu_calc_density")
+       import :: c_int, c_long, c_ptr
+       type(c_ptr), value :: unk, occ, rho
+       integer(c_long), value :: ld
+       integer(c_int), value :: mb
+     end function rsdft_gpu_calc_density
      integer(c_int) function rsdft_gpu_write_wf(path, unk, ld, mb, mk, ms, mbwr1, mbwr2, oc, io_ctrl, ngrid, occ, &
           aa, bb, mmbz, kbb) bind(C, name="rsdft_gpu_write_wf")
        import :: c_int, c_long, c_ptr
@@ -346,6 +353,15 @@ CONTAINS
     call check(rsdft_gpu_force_nloc(int(mi, c_int), c_loc(unk), int(size(unk, 1), c_long), &
                int(size(unk, 2), c_int), c_loc(occ), c_loc(force2)), "calc_force_ps_nloc2")
   END SUBROUTINE gpu_calc_force_ps_nloc2
+
+  ! calc_density's NCPP branch (density_module.f90:129-136) for one (k, s)
+  ! block: rho(:) = sum_n occ(n) unk(:, n)**2
+  SUBROUTINE gpu_calc_density(unk, occ, rho)
+    real(8), intent(IN), target :: unk(:, :), occ(:)
+    real(8), intent(OUT), target :: rho(:)
+    call check(rsdft_gpu_calc_density(c_loc(unk), int(size(unk, 1), c_long), int(size(unk, 2), c_int), &
+               c_loc(occ), c_loc(rho)), "calc_density")
+  END SUBROUTINE gpu_calc_density
 
   ! file name as a NUL-terminated C string
   SUBROUTINE c_path(file, buf)

@@ -2,7 +2,9 @@
 registered host array (whose device mirror is what counts) are written band
 by band through pinned buffers and must give the same bytes as the host
 array; reading fills the device memory.  The file format itself is checked
-against the reference's records on the CPU (tests/test_wfio.py)."""
+against the reference's records on the CPU (tests/test_wfio.py).  The
+session `gpu` fixture puts torch and the library on one stream, so torch's
+copies and the library's transfers are ordered."""
 import numpy as np
 import pytest
 
@@ -12,11 +14,6 @@ pytestmark = pytest.mark.gpu
 
 NG = (8, 6, 4)
 ML = 8 * 6 * 4
-
-
-@pytest.fixture(scope="module")
-def gpu():
-    return api.RsdftGpu(0)
 
 
 @pytest.mark.parametrize("oc", [0, 4])
