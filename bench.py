@@ -179,6 +179,13 @@ def cpu_iteration_rate(cell, sample_bands: int, ncg: int, mloop: int):
     }
 
 
+def metric_name(cell, ncg):
+    """The headline metric's label for a workload ("Si216 72^3, 480 bands" by default)."""
+    n1 = cell.ngrid[0]
+    return (f"eigensolver iter/s ({cell.name.split('_')[0].capitalize()} {n1}^3, {cell.nband} bands, "
+            f"CG Ncg={ncg} + GS + subspace)")
+
+
 def run_reference(args, rank, world):
     if rank != 0:
         return
@@ -198,7 +205,7 @@ def run_reference(args, rank, world):
     v = statistics.median(x["value"] for x in rates)
     out = {
         "impl": "reference",
-        "metric": "eigensolver iter/s (Si216 72^3, 480 bands, CG Ncg=4 + GS + subspace)",
+        "metric": metric_name(cell, args.ncg),
         "value": v,
         "unit": "iter/s",
         "n_gpus": world,
@@ -411,7 +418,7 @@ def main():
     if rank == 0:
         ms = results[head]["ms"]
         line = {
-            "metric": "eigensolver iter/s (Si216 72^3, 480 bands, CG Ncg=4 + GS + subspace)",
+            "metric": metric_name(cell, args.ncg),
             "value": replicas.whole_job_rate(1000.0, world, ms),
             "unit": "iter/s",
             "n_gpus": world,
