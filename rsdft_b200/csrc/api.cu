@@ -159,6 +159,7 @@ using namespace rsdft;
 extern "C" {
 
 int rsdft_gpu_init(int device) {
+    RS_ENTRY();
     Context& c = g_ctx;
     if (c.init && c.device == device) return RSDFT_OK;
     if (c.init) rsdft_gpu_finalize();
@@ -187,6 +188,7 @@ int rsdft_gpu_init(int device) {
 }
 
 int rsdft_gpu_finalize(void) {
+    RS_ENTRY();
     Context& c = g_ctx;
     if (!c.init) return RSDFT_OK;
     cudaStreamSynchronize(c.stream);
@@ -222,6 +224,7 @@ const char* rsdft_gpu_last_error(void) { return get_error(); }
 long long rsdft_gpu_kernel_launches(void) { return g_kernel_launches; }
 
 int rsdft_gpu_set_stream(void* stream) {
+    RS_ENTRY();
     RS_CHECK(require_init());
     Context& c = g_ctx;
     if (c.own_stream && c.stream) {
@@ -241,6 +244,7 @@ int rsdft_gpu_set_stream(void* stream) {
 }
 
 int rsdft_gpu_synchronize(void) {
+    RS_ENTRY();
     RS_CHECK(require_init());
     RS_CUDA(cudaStreamSynchronize(g_ctx.stream));
     int flag = 0;
@@ -255,6 +259,7 @@ int rsdft_gpu_synchronize(void) {
 
 int rsdft_gpu_set_grid(const int* ngrid, int md, double coef_lap0, const double* coef_lap,
                        const double* hgrid, const double* ggg, double dv) {
+    RS_ENTRY();
     RS_CHECK(require_init());
     Context& c = g_ctx;
     if (!ngrid || !coef_lap || !hgrid) {
@@ -304,6 +309,7 @@ int rsdft_gpu_set_grid(const int* ngrid, int md, double coef_lap0, const double*
 }
 
 int rsdft_gpu_set_vloc(const double* vloc, long ml, int nspin) {
+    RS_ENTRY();
     RS_CHECK(require_grid());
     Context& c = g_ctx;
     if (!vloc || ml != c.ml || nspin < 1) {
@@ -322,6 +328,7 @@ int rsdft_gpu_set_vloc(const double* vloc, long ml, int nspin) {
 
 int rsdft_gpu_set_nonlocal(int nzlma, const int* lma_ptr, const int* jjp, const double* uv,
                            const int* iuv, const int* amap, int natom, const double* duvdr) {
+    RS_ENTRY();
     RS_CHECK(require_grid());
     Context& c = g_ctx;
     if (nzlma < 0 || (nzlma > 0 && (!lma_ptr || !jjp || !uv || !iuv || !amap))) {
@@ -441,6 +448,7 @@ int rsdft_gpu_set_nonlocal(int nzlma, const int* lma_ptr, const int* jjp, const 
 }
 
 int rsdft_gpu_register_wf(double* unk, long ml, int mb) {
+    RS_ENTRY();
     RS_CHECK(require_init());
     if (!unk || ml <= 0 || mb <= 0) {
         set_error("register_wf: bad arguments");
@@ -475,6 +483,7 @@ static WfReg* find_reg(double* unk) {
 }
 
 int rsdft_gpu_unregister_wf(double* unk) {
+    RS_ENTRY();
     RS_CHECK(require_init());
     Context& c = g_ctx;
     for (size_t i = 0; i < c.regs.size(); ++i)
@@ -489,6 +498,7 @@ int rsdft_gpu_unregister_wf(double* unk) {
 }
 
 int rsdft_gpu_sync_to_host(double* unk) {
+    RS_ENTRY();
     RS_CHECK(require_init());
     WfReg* r = find_reg(unk);
     if (!r) {
@@ -501,6 +511,7 @@ int rsdft_gpu_sync_to_host(double* unk) {
 }
 
 int rsdft_gpu_sync_to_device(double* unk) {
+    RS_ENTRY();
     RS_CHECK(require_init());
     WfReg* r = find_reg(unk);
     if (!r) {

@@ -714,6 +714,7 @@ int cg_device(double* unk, long ld, int mb, int spin, double* esp, double* res, 
 using namespace rsdft;
 
 extern "C" int rsdft_gpu_esp_calc(int k, int s, const double* wf, int n1, int n2, int ns, int ne, double* e) {
+    RS_ENTRY();
     RS_CHECK(require_grid());
     Context& c = ctx();
     if (k != 1) {
@@ -740,6 +741,7 @@ extern "C" int rsdft_gpu_esp_calc(int k, int s, const double* wf, int n1, int n2
 }
 
 extern "C" int rsdft_gpu_residual(int k, int s, const double* wf, long ld, int nb, double* e, double* res) {
+    RS_ENTRY();
     RS_CHECK(require_grid());
     Context& c = ctx();
     if (k != 1 || s < 1 || s > c.nspin || ld < c.ml || nb < 1 || nb > 65535 || !e || !res) {
@@ -758,6 +760,7 @@ extern "C" int rsdft_gpu_residual(int k, int s, const double* wf, long ld, int n
 
 extern "C" int rsdft_gpu_conjugate_gradient(int n1, int n2, int mb, int k, int s, double* unk, double* esp,
                                             double* res, int ncg, int mloop, int ipc, int mode) {
+    RS_ENTRY();
     RS_CHECK(require_grid());
     Context& c = ctx();
     if (k != 1) {

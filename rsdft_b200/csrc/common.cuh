@@ -14,9 +14,23 @@
 #include <utility>
 #include <vector>
 
+#include <nvtx3/nvToolsExt.h>
+
 #include "../../include/rsdft_gpu.h"
 
 namespace rsdft {
+
+// A named NVTX range over one C-ABI call (the entry's name), so profiler
+// timelines group the kernels by the reference routine they replace (the
+// role of the reference's watchb timers, watch_module.f90:89-219).  Without
+// a profiler attached the NVTX calls do nothing.
+struct NvtxRange {
+    explicit NvtxRange(const char* name) { nvtxRangePushA(name); }
+    ~NvtxRange() { nvtxRangePop(); }
+    NvtxRange(const NvtxRange&) = delete;
+    NvtxRange& operator=(const NvtxRange&) = delete;
+};
+#define RS_ENTRY() const ::rsdft::NvtxRange rs_entry_range_(__func__)
 
 constexpr int MAXMD = 8;
 

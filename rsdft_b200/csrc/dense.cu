@@ -379,6 +379,7 @@ static int check_k_s(int k, int s, const char* who) {
 extern "C" {
 
 int rsdft_gpu_gram_schmidt(int n0, int n1, int k, int s, double* unk, long ld, int nblk, int nblk1, int mode) {
+    RS_ENTRY();
     RS_CHECK(require_grid());
     (void)nblk;
     (void)nblk1;
@@ -407,6 +408,7 @@ int rsdft_gpu_gram_schmidt(int n0, int n1, int k, int s, double* unk, long ld, i
 }
 
 int rsdft_gpu_subspace_mate(int k, int s, const double* unk, long ld, int mb, double* hsub, int ldh) {
+    RS_ENTRY();
     RS_CHECK(require_grid());
     RS_CHECK(check_k_s(k, s, "subspace_mate"));
     Context& c = ctx();
@@ -430,6 +432,7 @@ int rsdft_gpu_subspace_mate(int k, int s, const double* unk, long ld, int mb, do
 }
 
 int rsdft_gpu_subspace_solv(int mb, const double* hsub, int ldh, double* esp, double* vsub, int ldv) {
+    RS_ENTRY();
     RS_CHECK(require_init());
     Context& c = ctx();
     if (mb < 1 || ldh < mb || ldv < mb || !hsub || !esp || !vsub) {
@@ -450,6 +453,7 @@ int rsdft_gpu_subspace_solv(int mb, const double* hsub, int ldh, double* esp, do
 }
 
 int rsdft_gpu_subspace_rotv(int k, int s, double* unk, long ld, int mb, const double* vsub, int ldv) {
+    RS_ENTRY();
     RS_CHECK(require_grid());
     RS_CHECK(check_k_s(k, s, "subspace_rotv"));
     Context& c = ctx();
@@ -475,6 +479,7 @@ int rsdft_gpu_subspace_rotv(int k, int s, double* unk, long ld, int mb, const do
 
 int rsdft_gpu_eigensolver_sweep(int k, int s, double* unk, long ld, int mb, double* esp, double* res, int ncg,
                                 int mloop, int ipc, int mode) {
+    RS_ENTRY();
     RS_CHECK(require_grid());
     RS_CHECK(check_k_s(k, s, "eigensolver_sweep"));
     Context& c = ctx();
@@ -513,6 +518,7 @@ int rsdft_gpu_eigensolver_sweep(int k, int s, double* unk, long ld, int mb, doub
 }
 
 int rsdft_gpu_orth_subspace_diag(int k, int s, double* unk, long ld, int mb, double* esp, int mode) {
+    RS_ENTRY();
     RS_CHECK(require_grid());
     RS_CHECK(check_k_s(k, s, "orth_subspace_diag"));
     Context& c = ctx();
@@ -531,6 +537,7 @@ int rsdft_gpu_orth_subspace_diag(int k, int s, double* unk, long ld, int mb, dou
 }
 
 int rsdft_gpu_subspace_diag(int k, int s, double* unk, long ld, int mb, double* esp, int mode) {
+    RS_ENTRY();
     RS_CHECK(require_grid());
     RS_CHECK(check_k_s(k, s, "subspace_diag"));
     Context& c = ctx();

@@ -195,6 +195,7 @@ using namespace rsdft;
 extern "C" {
 
 int rsdft_gpu_force_nloc(int mi, const double* unk, long ld, int mb, const double* occ, double* force2) {
+    RS_ENTRY();
     RS_CHECK(require_grid());
     Context& c = ctx();
     if (!c.nl_set || !c.duv) {
@@ -222,6 +223,7 @@ int rsdft_gpu_force_nloc(int mi, const double* unk, long ld, int mb, const doubl
 
 int rsdft_gpu_hpsi_adjoint(const double* psi, const double* chi, long ld, int nb, const double* occ, double* dl_dv,
                            double* dl_dr) {
+    RS_ENTRY();
     RS_CHECK(require_grid());
     Context& c = ctx();
     if (ld < c.ml || nb < 1 || (!chi && !occ) || (!dl_dv && !dl_dr)) {
@@ -259,6 +261,7 @@ int rsdft_gpu_hpsi_adjoint(const double* psi, const double* chi, long ld, int nb
 }
 
 int rsdft_gpu_calc_density(const double* unk, long ld, int mb, const double* occ, double* rho) {
+    RS_ENTRY();
     RS_CHECK(require_grid());
     Context& c = ctx();
     if (ld < c.ml || mb < 1 || !occ || !rho) {

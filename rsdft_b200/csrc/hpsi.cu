@@ -769,6 +769,7 @@ using namespace rsdft;
 
 extern "C" int rsdft_gpu_hamiltonian(int k, int s, const double* tpsi, double* htpsi, int n1, int n2, int ib1,
                                      int ib2) {
+    RS_ENTRY();
     RS_CHECK(require_grid());
     Context& c = ctx();
     if (k != 1) {
@@ -877,6 +878,7 @@ int hpsi_static_scratch(const double* psi, double* hpsi, long ld, int nb, int sp
 
 extern "C" int rsdft_gpu_hamiltonian_noalloc(int k, int s, const double* tpsi, double* htpsi, int n1, int n2,
                                              int ib1, int ib2) {
+    RS_ENTRY();
     RS_CHECK(require_grid());
     Context& c = ctx();
     if (k != 1) {

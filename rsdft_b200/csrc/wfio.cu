@@ -188,6 +188,7 @@ using namespace rsdft;
 extern "C" int rsdft_gpu_write_wf(const char* path, const double* unk, long ld, int mb, int mk, int ms, int mbwr1,
                                   int mbwr2, int oc, int io_ctrl, const int* ngrid, const double* occ,
                                   const double* aa, const double* bb, int mmbz, const double* kbb) {
+    RS_ENTRY();
     if (!path || !unk || !ngrid || mb < 1 || mk < 1 || ms < 1 || mmbz < 0) {
         set_error("write_wf: NULL path/unk/ngrid or bad counts");
         return RSDFT_EINVAL;
@@ -287,6 +288,7 @@ extern "C" int rsdft_gpu_write_wf(const char* path, const double* unk, long ld, 
 
 extern "C" int rsdft_gpu_read_wf(const char* path, double* unk, long ld, int mb, int mk, int ms, int io_ctrl,
                                  const int* ngrid, double* occ, int* info) {
+    RS_ENTRY();
     if (!path || !unk || !ngrid || mb < 1 || mk < 1 || ms < 1) {
         set_error("read_wf: NULL path/unk/ngrid or bad counts");
         return RSDFT_EINVAL;

@@ -58,3 +58,18 @@ def test_init_reports_missing_device(lib):
     rc = L.rsdft_gpu_init(0)
     assert rc in (-1, -3)
     assert len(L.rsdft_gpu_last_error()) > 0
+
+
+def test_every_entry_is_defined_once_and_opens_a_trace_range():
+    """Each C-ABI entry is defined once in csrc and starts with RS_ENTRY() (an
+    NVTX range named after it), except the two plain getters."""
+    import glob
+
+    src = "".join(open(f).read() for f in sorted(glob.glob(os.path.join(ROOT, "rsdft_b200", "csrc", "*.cu"))))
+    defs = re.findall(r'(?m)^(?:extern "C" )?(?:int|long long|const char\*) (rsdft_gpu_\w+)\([^)]*\)\s*\{\s*(\S+)', src)
+    names = [n for n, _ in defs]
+    assert sorted(names) == declared()
+    getters = {"rsdft_gpu_last_error", "rsdft_gpu_kernel_launches"}
+    for name, first in defs:
+        if name not in getters:
+            assert first == "RS_ENTRY();", f"{name} does not open with RS_ENTRY()"
