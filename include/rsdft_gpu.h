@@ -59,6 +59,12 @@ int rsdft_gpu_synchronize(void);
  * (diagnostics; library calls such as cuBLAS are not counted).  (no
  * reference counterpart; the reference's timers are watch_module.f90) */
 long long rsdft_gpu_kernel_launches(void);
+/* Failure-path self test: launch one kernel whose mbarrier wait can never
+ * complete, bounded by `cycles` SM clock cycles (1 .. 2^34), after which it
+ * sets the error flag exactly as a library kernel whose wait ran out does;
+ * the next rsdft_gpu_synchronize returns RSDFT_ETIMEOUT, later calls work.
+ * (no reference counterpart: the reference stops the program on errors) */
+int rsdft_gpu_selftest_timeout(long long cycles);
 
 /* Grid and FD kinetic coefficients: Ngrid(1:3), Md, coef_lap0, coef_lap(3,Md)
  * (axis-major: coef_lap[axis*Md + m-1]), Hgrid(1:3), ggg(1:3), dV.
