@@ -36,7 +36,7 @@ import numpy as np
 ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
-MODES = {"fp64": 0, "mixed-bf16": 1, "mixed-bf16x3": 2}
+MODES = {"fp64": 0, "mixed-bf16x3": 1, "mixed-tf32": 2, "mixed-bf16x2": 3}
 
 
 def parse():
@@ -46,7 +46,7 @@ def parse():
     p.add_argument("--warmup", type=int, default=3)
     p.add_argument("--impl", default="ours", choices=["ours", "reference"])
     p.add_argument("--workload", default="si216")
-    p.add_argument("--mode", default="auto", choices=["auto", "fp64", "mixed-bf16", "mixed-bf16x3"])
+    p.add_argument("--mode", default="auto", choices=["auto", "fp64", "mixed-bf16x3", "mixed-bf16x2"])
     p.add_argument("--ncg", type=int, default=4)
     p.add_argument("--mloop", type=int, default=3)
     p.add_argument("--no-cpu-baseline", action="store_true")
@@ -281,7 +281,7 @@ def main():
 
     modes = ["fp64"]
     if args.mode == "auto":
-        for m in ("mixed-bf16",):
+        for m in ("mixed-bf16x3",):
             if supported(MODES[m]):
                 modes.append(m)
                 break
@@ -428,7 +428,7 @@ def main():
             "higher_is_better": True,
             "scaling": "weak",
             "vs_baseline": None,
-            "dtype": "f64" if head == "fp64" else ("bf16(3-term)+f32+f64" if head == "mixed-bf16" else "bf16(2-term)+f32+f64"),
+            "dtype": "f64" if head == "fp64" else ("bf16(3-term)+f32+f64" if head == "mixed-bf16x3" else "bf16(2-term)+f32+f64"),
             "data": "synthetic (seeded Si cell, random start bands)",
             "config": {"workload": args.workload, "grid": list(cell.ngrid), "bands": MB, "Md": cell.md,
                        "ncg": args.ncg, "mloop": args.mloop, "form": head,

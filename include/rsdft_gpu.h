@@ -38,10 +38,14 @@ extern "C" {
 #define RSDFT_EUNSUP (-6)    /* unsupported option (k != 1, Md > 8, ...) */
 #define RSDFT_ETIMEOUT (-7)  /* a kernel's bounded wait ran out (reported at the next sync) */
 
-/* precision modes of the eigensolver entries */
-#define RSDFT_MODE_FP64 0        /* plain all-FP64 form */
-#define RSDFT_MODE_MIXED_BF16 1    /* 3-term split-BF16 tensor-core contractions (6 products), FP32 CG */
-#define RSDFT_MODE_MIXED_BF16X3 2  /* 2-term split-BF16 tensor-core contractions (3 products), FP32 CG */
+/* precision modes of the eigensolver entries; the name gives the operand
+ * split of the tensor-core contractions (CG sweeps run in FP32 in every
+ * mixed mode; Cholesky, the subspace eigensolve and the closing residuals
+ * stay FP64) */
+#define RSDFT_MODE_FP64 0          /* plain all-FP64 form */
+#define RSDFT_MODE_MIXED_BF16X3 1  /* 3-term split-BF16 (6 products, 24 significant bits) */
+#define RSDFT_MODE_MIXED_TF32 2    /* 2-term split-TF32, kind::tf32 (3 products, ~22 bits: FP32 accuracy) */
+#define RSDFT_MODE_MIXED_BF16X2 3  /* 2-term split-BF16 (3 products, 16 bits) */
 
 /* ---------------------------------------------------------------- set-up */
 
@@ -59,6 +63,10 @@ int rsdft_gpu_synchronize(void);
  * (diagnostics; library calls such as cuBLAS are not counted).  (no
  * reference counterpart; the reference's timers are watch_module.f90) */
 long long rsdft_gpu_kernel_launches(void);
+/* Bytes of device workspace the library holds (its named, grow-only
+ * buffers; registered wavefunction mirrors and set-up tables not counted).
+ * (diagnostics; no reference counterpart) */
+long long rsdft_gpu_workspace_bytes(void);
 /* Failure-path self test: launch one kernel whose mbarrier wait can never
  * complete, bounded by `cycles` SM clock cycles (1 .. 2^34), after which it
  * sets the error flag exactly as a library kernel whose wait ran out does;
@@ -117,8 +125,11 @@ int rsdft_gpu_hamiltonian(int k, int s, const double *tpsi, double *htpsi, int n
  *    (ib2-ib1+1) * nzlma above that returns RSDFT_EINVAL; split the bands.
  *  - tpsi and htpsi must be device memory or lie in a registered
  *    wavefunction: nothing is staged.
- *  - The first call on a device looks up the array's device address; make
- *    that first call before any stream capture.
+ *  - rsdft_gpu_init looks up the array's device address for its device.  The
+ *    first launch of a kernel can still make the CUDA driver load that
+ *    kernel's code (lazy module loading), which the driver allocates: make
+ *    one call at set-up, before the caller's own pool takes the memory and
+ *    before any stream capture.
  *  - All calls share the one array: calls that overlap on the GPU (other
  *    streams, other host threads) race.  Each call overwrites every value it
  *    reads, so no clearing is needed between calls. */

@@ -22,6 +22,7 @@ SIGNATURES = {
     "rsdft_gpu_set_stream": (_c_int, [_vp]),
     "rsdft_gpu_synchronize": (_c_int, []),
     "rsdft_gpu_kernel_launches": (ctypes.c_longlong, []),
+    "rsdft_gpu_workspace_bytes": (ctypes.c_longlong, []),
     "rsdft_gpu_selftest_timeout": (_c_int, [ctypes.c_longlong]),
     "rsdft_gpu_set_grid": (_c_int, [_vp, _c_int, _c_double, _vp, _vp, _vp, _c_double]),
     "rsdft_gpu_set_vloc": (_c_int, [_vp, _c_long, _c_int]),

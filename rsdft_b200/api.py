@@ -37,8 +37,9 @@ from . import _lib
 from ._lib import RsdftError  # noqa: F401  (re-export)
 
 MODE_FP64 = 0
-MODE_MIXED_BF16 = 1
-MODE_MIXED_BF16X3 = 2
+MODE_MIXED_BF16X3 = 1  # 3-term split-BF16 contractions (6 products)
+MODE_MIXED_TF32 = 2    # 2-term split-TF32 contractions (3 products)
+MODE_MIXED_BF16X2 = 3  # 2-term split-BF16 contractions (3 products)
 
 
 def _is_torch(a) -> bool:

@@ -4,6 +4,8 @@
 #include <cstring>
 #include <numeric>
 
+#include <cuda.h>
+
 #include "common.cuh"
 
 namespace rsdft {
@@ -13,6 +15,8 @@ long long g_kernel_launches = 0;
 static thread_local char g_err[1024] = "";
 
 Context& ctx() { return g_ctx; }
+
+int noalloc_bind_scratch();  // hpsi.cu
 
 void set_error(const char* fmt, ...) {
     va_list ap;
@@ -40,6 +44,20 @@ int require_grid() {
     return RSDFT_OK;
 }
 
+int set_smem_optin(const void* kernel, int bytes) {
+    int& have = g_ctx.smem_optin[kernel];
+    if (bytes > have) {
+        RS_CUDA(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes));
+        have = bytes;
+    }
+    return RSDFT_OK;
+}
+
+char* host_workspace(size_t bytes) {
+    if (g_ctx.host_ws.size() < bytes) g_ctx.host_ws.resize(bytes);
+    return g_ctx.host_ws.data();
+}
+
 int workspace(const char* name, size_t bytes, void** out) {
     Buf& b = g_ctx.ws[name];
     if (b.bytes < bytes) {
@@ -61,7 +79,27 @@ int workspace(const char* name, size_t bytes, void** out) {
     return RSDFT_OK;
 }
 
-int resolve(const void* p, void** dev) {
+// cuMemGetAddressRange through the driver entry point (no link-time libcuda):
+// the allocation that holds a device address, to check a span against it.
+using AddressRangeFn = CUresult (*)(CUdeviceptr*, size_t*, CUdeviceptr);
+
+static AddressRangeFn address_range_fn() {
+    static AddressRangeFn fn = nullptr;
+    static bool tried = false;
+    if (!tried) {
+        tried = true;
+        void* f = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPoint("cuMemGetAddressRange", &f, cudaEnableDefault, &q) == cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            fn = reinterpret_cast<AddressRangeFn>(f);
+        else
+            cudaGetLastError();
+    }
+    return fn;
+}
+
+int resolve(const void* p, size_t bytes, void** dev) {
     if (!p) return 0;
     cudaPointerAttributes at;
     cudaError_t e = cudaPointerGetAttributes(&at, p);
@@ -69,13 +107,37 @@ int resolve(const void* p, void** dev) {
         cudaGetLastError();
         at.type = cudaMemoryTypeUnregistered;
     }
+    const char* c = static_cast<const char*>(p);
     if (at.type == cudaMemoryTypeDevice || at.type == cudaMemoryTypeManaged) {
+        if (at.type == cudaMemoryTypeDevice && g_ctx.init && at.device != g_ctx.device) {
+            set_error("device pointer %p belongs to device %d, the library is bound to device %d", p, at.device,
+                      g_ctx.device);
+            return RSDFT_EINVAL;
+        }
+        if (at.type == cudaMemoryTypeDevice && bytes > 0) {
+            if (AddressRangeFn fn = address_range_fn()) {
+                CUdeviceptr base = 0;
+                size_t size = 0;
+                if (fn(&base, &size, reinterpret_cast<CUdeviceptr>(p)) == CUDA_SUCCESS) {
+                    const size_t off = (size_t)(reinterpret_cast<CUdeviceptr>(p) - base);
+                    if (off + bytes > size) {
+                        set_error("device array at %p: %zu bytes requested, %zu left in its allocation", p, bytes,
+                                  size - off);
+                        return RSDFT_EINVAL;
+                    }
+                }
+            }
+        }
         *dev = const_cast<void*>(p);
         return 1;
     }
-    const char* c = static_cast<const char*>(p);
     for (auto& r : g_ctx.regs) {
         if (c >= r.host && c < r.host + r.bytes) {
+            if ((size_t)(c - r.host) + bytes > r.bytes) {
+                set_error("array at %p: %zu bytes requested, %zu left in its registered wavefunction", p, bytes,
+                          (size_t)(r.host + r.bytes - c));
+                return RSDFT_EINVAL;
+            }
             *dev = r.dev + (c - r.host);
             return 1;
         }
@@ -84,7 +146,9 @@ int resolve(const void* p, void** dev) {
 }
 
 int stage_in(const void* p, size_t bytes, const char* wsname, void** dev) {
-    if (resolve(p, dev)) return RSDFT_OK;
+    const int r = resolve(p, bytes, dev);
+    if (r < 0) return r;
+    if (r) return RSDFT_OK;
     RS_CHECK(workspace(wsname, bytes, dev));
     RS_CUDA(cudaMemcpyAsync(*dev, p, bytes, cudaMemcpyHostToDevice, g_ctx.stream));
     return RSDFT_OK;
@@ -92,7 +156,9 @@ int stage_in(const void* p, size_t bytes, const char* wsname, void** dev) {
 
 int stage_out(void* p, const void* dev, size_t bytes) {
     void* d = nullptr;
-    if (resolve(p, &d)) {
+    const int r = resolve(p, bytes, &d);
+    if (r < 0) return r;
+    if (r) {
         if (d != dev) RS_CUDA(cudaMemcpyAsync(d, dev, bytes, cudaMemcpyDeviceToDevice, g_ctx.stream));
         return RSDFT_OK;
     }
@@ -109,11 +175,13 @@ int wf_acquire(const double* p, long ld, int nb, const char* wsname, double** de
         set_error("NULL wavefunction pointer");
         return RSDFT_EINVAL;
     }
-    if (resolve(p, &d)) {
+    size_t bytes = sizeof(double) * (size_t)ld * (size_t)nb;
+    const int r = resolve(p, bytes, &d);
+    if (r < 0) return r;
+    if (r) {
         *dev = static_cast<double*>(d);
         return RSDFT_OK;
     }
-    size_t bytes = sizeof(double) * (size_t)ld * (size_t)nb;
     RS_CHECK(workspace(wsname, bytes, &d));
     if (copy_in) RS_CUDA(cudaMemcpyAsync(d, p, bytes, cudaMemcpyHostToDevice, g_ctx.stream));
     *dev = static_cast<double*>(d);
@@ -183,6 +251,9 @@ int rsdft_gpu_init(int device) {
     RS_CUDA(cudaStreamCreateWithFlags(&c.copy_stream, cudaStreamNonBlocking));
     for (int i = 0; i < Context::NEV; ++i) RS_CUDA(cudaEventCreateWithFlags(&c.ev[i], cudaEventDisableTiming));
     c.device = device;
+    // the device address of rsdft_gpu_hamiltonian_noalloc's static scratch,
+    // looked up now so that entry never loads a module or allocates
+    RS_CHECK(noalloc_bind_scratch());
     c.init = true;
     return RSDFT_OK;
 }
@@ -222,6 +293,12 @@ int rsdft_gpu_finalize(void) {
 const char* rsdft_gpu_last_error(void) { return get_error(); }
 
 long long rsdft_gpu_kernel_launches(void) { return g_kernel_launches; }
+
+long long rsdft_gpu_workspace_bytes(void) {
+    long long n = 0;
+    for (const auto& kv : g_ctx.ws) n += (long long)kv.second.bytes;
+    return n;
+}
 
 int rsdft_gpu_set_stream(void* stream) {
     RS_ENTRY();

@@ -780,7 +780,7 @@ extern "C" int rsdft_gpu_conjugate_gradient(int n1, int n2, int mb, int k, int s
         set_error("conjugate_gradient: ipc=%d unsupported (0 or 4)", ipc);
         return RSDFT_EUNSUP;
     }
-    if (mode < 0 || mode > 2) {
+    if (!mode_valid(mode)) {
         set_error("conjugate_gradient: mode=%d unknown", mode);
         return RSDFT_EINVAL;
     }

@@ -114,6 +114,11 @@ struct Context {
     // workspace
     std::map<std::string, Buf> ws;
     std::vector<WfReg> regs;
+    std::vector<char> host_ws;               // host scratch of cuSOLVER calls
+    std::map<const void*, int> smem_optin;   // dynamic shared memory opted in, per kernel
+    int max_smem_optin = -1;                 // device limit (cudaDevAttrMaxSharedMemoryPerBlockOptin)
+    int sytrd_clusters = -1;                 // active 16-CTA clusters of the eigensolver kernel
+    double* noalloc_scratch = nullptr;       // device address of the static scratch array
 };
 
 Context& ctx();
@@ -181,6 +186,14 @@ inline void launch(void (*kernel)(KArgs...), dim3 grid, dim3 block, size_t smem,
 int require_init();
 int require_grid();
 
+// Opt `kernel` in to `bytes` of dynamic shared memory on the bound device.
+// The record lives in the context, so a context on another device sets the
+// attribute again; a size no larger than the one set already does nothing.
+int set_smem_optin(const void* kernel, int bytes);
+
+// Host scratch owned by the context (grow-only; contents undefined).
+char* host_workspace(size_t bytes);
+
 // ------------------------------------------------------------ workspace
 // Named device buffer, grown (never shrunk) on demand; contents undefined.
 int workspace(const char* name, size_t bytes, void** out);
@@ -190,10 +203,13 @@ inline int workspace_t(const char* name, size_t count, T** out) {
 }
 
 // ------------------------------------------------- pointer resolution
-// Classify a caller pointer: device memory is used directly; a host pointer
-// inside a registered wavefunction range maps onto its device mirror.
-// Returns 1 if *dev was set (device-visible), 0 if p is plain host memory.
-int resolve(const void* p, void** dev);
+// Classify a caller pointer and the `bytes` that follow it: device memory of
+// the bound device is used directly; a host pointer inside a registered
+// wavefunction range maps onto its device mirror.  Returns 1 if *dev was set
+// (device-visible), 0 if p is plain host memory, RSDFT_EINVAL (error set) if
+// the span runs past the end of its registration or device allocation, or if
+// p is device memory of another device.
+int resolve(const void* p, size_t bytes, void** dev);
 
 // Stage a small caller array onto the device (copy if host), and back.
 int stage_in(const void* host_or_dev, size_t bytes, const char* wsname, void** dev);
@@ -205,6 +221,8 @@ int stage_out(void* host_or_dev, const void* dev, size_t bytes);
 int wf_acquire(const double* p, long ld, int nb, const char* wsname, double** dev, bool* staged,
                bool copy_in = true);
 int wf_release(double* p, const double* dev, long ld, int nb, bool staged);
+
+inline bool mode_valid(int mode) { return mode >= RSDFT_MODE_FP64 && mode <= RSDFT_MODE_MIXED_BF16X2; }
 
 inline int div_up(long a, long b) { return (int)((a + b - 1) / b); }
 

@@ -118,10 +118,9 @@ static int cholqr_pass(const double* psi, double* out, long ld, int nb, double* 
                                           nb, &dws, &hws));
     void* dw = nullptr;
     RS_CHECK(workspace("gs_trtri", dws + 16, &dw));
-    static std::vector<char> hw;
-    if (hw.size() < hws + 16) hw.resize(hws + 16);
+    char* hw = host_workspace(hws + 16);
     RS_SOLVER(cusolverDnXtrtri(c.solver, CUBLAS_FILL_MODE_UPPER, CUBLAS_DIAG_NON_UNIT, nb, CUDA_R_64F, S, nb, dw,
-                               dws, hw.data(), hws, dinfo));
+                               dws, hw, hws, dinfo));
     RS_CHECK(check_info(dinfo, "gram_schmidt: triangular inverse"));
     launch(k_zero_lower, dim3(div_up(nb, 128), nb), 128, 0, c.stream, S, nb, nb);
     RS_LAUNCH();
@@ -223,7 +222,7 @@ __global__ void k_diag_minmax(const double* __restrict__ a, int n, int lda, doub
 // condition 2.4e3 gave 6.5e-4 relative eigenvalue error in the 2-term form,
 // 3e-6 in the 3-term form).
 static double fused_rr_kappa_max(int mode) {
-    return mode == RSDFT_MODE_FP64 ? 1e3 : (mode == RSDFT_MODE_MIXED_BF16 ? 1e2 : 1e1);
+    return mode == RSDFT_MODE_FP64 ? 1e3 : (mode == RSDFT_MODE_MIXED_BF16X2 ? 1e1 : 1e2);
 }
 
 // Gram-Schmidt followed by subspace_diag (the pair calc_sweep calls,
@@ -276,10 +275,9 @@ int orth_subspace_diag_device(double* psi, long ld, int mb, int spin, double* es
                                           mb, &dws, &hws));
     void* dw = nullptr;
     RS_CHECK(workspace("gs_trtri", dws + 16, &dw));
-    static std::vector<char> hw;
-    if (hw.size() < hws + 16) hw.resize(hws + 16);
+    char* hw = host_workspace(hws + 16);
     RS_SOLVER(cusolverDnXtrtri(c.solver, CUBLAS_FILL_MODE_UPPER, CUBLAS_DIAG_NON_UNIT, mb, CUDA_R_64F, S, mb, dw,
-                               dws, hw.data(), hws, dinfo));
+                               dws, hw, hws, dinfo));
     RS_CHECK(check_info(dinfo, "orth_subspace_diag: triangular inverse"));
     launch(k_zero_lower, dim3(div_up(mb, 128), mb), 128, 0, c.stream, S, mb, mb);
     RS_LAUNCH();
@@ -346,10 +344,9 @@ int orth_subspace_diag_f32(const float* x32, const float* hx, double* psi, long 
                                           mb, &dws, &hws));
     void* dw = nullptr;
     RS_CHECK(workspace("gs_trtri", dws + 16, &dw));
-    static std::vector<char> hw;
-    if (hw.size() < hws + 16) hw.resize(hws + 16);
+    char* hw = host_workspace(hws + 16);
     RS_SOLVER(cusolverDnXtrtri(c.solver, CUBLAS_FILL_MODE_UPPER, CUBLAS_DIAG_NON_UNIT, mb, CUDA_R_64F, S, mb, dw,
-                               dws, hw.data(), hws, dinfo));
+                               dws, hw, hws, dinfo));
     RS_CHECK(check_info(dinfo, "eigensolver_sweep: triangular inverse"));
     launch(k_zero_lower, dim3(div_up(mb, 128), mb), 128, 0, c.stream, S, mb, mb);
     RS_LAUNCH();
@@ -390,7 +387,7 @@ int rsdft_gpu_gram_schmidt(int n0, int n1, int k, int s, double* unk, long ld, i
         return RSDFT_EUNSUP;
     }
     const int nb = n1 - n0 + 1;
-    if (n0 < 1 || nb < 1 || ld < c.ml || !unk || mode < 0 || mode > 2) {
+    if (n0 < 1 || nb < 1 || ld < c.ml || !unk || !mode_valid(mode)) {
         set_error("gram_schmidt: bad arguments (n0=%d n1=%d ld=%ld)", n0, n1, ld);
         return RSDFT_EINVAL;
     }
@@ -484,7 +481,7 @@ int rsdft_gpu_eigensolver_sweep(int k, int s, double* unk, long ld, int mb, doub
     RS_CHECK(check_k_s(k, s, "eigensolver_sweep"));
     Context& c = ctx();
     if (ld != c.ml || mb < 1 || mb > 65535 || !esp || !res || ncg < 0 || mloop < 0 || (ipc != 0 && ipc != 4) ||
-        mode < 0 || mode > 2) {
+        !mode_valid(mode)) {
         set_error("eigensolver_sweep: bad arguments");
         return RSDFT_EINVAL;
     }
@@ -522,7 +519,7 @@ int rsdft_gpu_orth_subspace_diag(int k, int s, double* unk, long ld, int mb, dou
     RS_CHECK(require_grid());
     RS_CHECK(check_k_s(k, s, "orth_subspace_diag"));
     Context& c = ctx();
-    if (ld < c.ml || mb < 1 || !esp || mode < 0 || mode > 2) {
+    if (ld < c.ml || mb < 1 || !esp || !mode_valid(mode)) {
         set_error("orth_subspace_diag: bad arguments");
         return RSDFT_EINVAL;
     }
@@ -541,7 +538,7 @@ int rsdft_gpu_subspace_diag(int k, int s, double* unk, long ld, int mb, double* 
     RS_CHECK(require_grid());
     RS_CHECK(check_k_s(k, s, "subspace_diag"));
     Context& c = ctx();
-    if (ld < c.ml || mb < 1 || !esp || mode < 0 || mode > 2) {
+    if (ld < c.ml || mb < 1 || !esp || !mode_valid(mode)) {
         set_error("subspace_diag: bad arguments");
         return RSDFT_EINVAL;
     }

@@ -694,19 +694,13 @@ int syevd_fast(double* A, int n, double* W, cublasFillMode_t uplo) {
     Context& c = ctx();
     if (n < 3 || n > 32 * IV_RPL) return RSDFT_EUNSUP;
     const size_t smem = td_smem_bytes(n);
-    static int max_optin = -1, max_clusters = -1;
-    if (max_optin < 0) {
-        int dev = 0;
-        RS_CUDA(cudaGetDevice(&dev));
-        RS_CUDA(cudaDeviceGetAttribute(&max_optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev));
-    }
-    if (smem > (size_t)max_optin) return RSDFT_EUNSUP;
-    static size_t smem_set = 0;
-    if (smem > smem_set) {
+    if (c.max_smem_optin < 0)
+        RS_CUDA(cudaDeviceGetAttribute(&c.max_smem_optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, c.device));
+    if (smem > (size_t)c.max_smem_optin) return RSDFT_EUNSUP;
+    if ((int)smem > c.smem_optin[(const void*)k_sytrd]) {
         RS_CUDA(cudaFuncSetAttribute(k_sytrd, cudaFuncAttributeNonPortableClusterSizeAllowed, 1));
-        RS_CUDA(cudaFuncSetAttribute(k_sytrd, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-        smem_set = smem;
-        max_clusters = -1;
+        RS_CHECK(set_smem_optin((const void*)k_sytrd, (int)smem));
+        c.sytrd_clusters = -1;
     }
     cudaLaunchConfig_t cfg{};
     cudaLaunchAttribute attr[1];
@@ -720,13 +714,13 @@ int syevd_fast(double* A, int n, double* W, cublasFillMode_t uplo) {
     cfg.stream = c.stream;
     cfg.attrs = attr;
     cfg.numAttrs = 1;
-    if (max_clusters < 0) {
-        if (cudaOccupancyMaxActiveClusters(&max_clusters, k_sytrd, &cfg) != cudaSuccess) {
+    if (c.sytrd_clusters < 0) {
+        if (cudaOccupancyMaxActiveClusters(&c.sytrd_clusters, k_sytrd, &cfg) != cudaSuccess) {
             cudaGetLastError();
-            max_clusters = 0;
+            c.sytrd_clusters = 0;
         }
     }
-    if (max_clusters < 1) return RSDFT_EUNSUP;
+    if (c.sytrd_clusters < 1) return RSDFT_EUNSUP;
 
     double *Q = nullptr, *dd = nullptr, *ws = nullptr, *work = nullptr;
     int* dinfo = nullptr;

@@ -12,7 +12,6 @@
 //  elements) run k_stencil, a register-queue kernel with per-plane halo
 //  loads and the scatter fused in its epilogue.
 #include <algorithm>
-#include <mutex>
 
 #include "common.cuh"
 #include "kernels.cuh"
@@ -660,12 +659,7 @@ static int launch_tma(StencilArgs<T> a, const StencilCoef& cf, int nb, cudaStrea
         encode_tmap_4d(&maps.wrap, dt, a.psi, dims, strides, bw) != RSDFT_OK ||
         encode_tmap_4d(&maps.vloc, dt, a.vloc, vdims, vstrides, bm) != RSDFT_OK)
         return RSDFT_OK;  // not usable for this shape: the caller takes the general kernel
-    static bool attr_set = false;
-    if (!attr_set) {
-        RS_CUDA(cudaFuncSetAttribute(k_stencil_tma<T, MD, BY>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                     220 * 1024 + 8 * 16));
-        attr_set = true;
-    }
+    RS_CHECK(set_smem_optin((const void*)k_stencil_tma<T, MD, BY>, 220 * 1024 + 8 * 16));
     dim3 grid(a.n2 / g.TY, (unsigned)(nb * a.nzc));
     launch(k_stencil_tma<T, MD, BY>, grid, g.threads, g.smem, st, maps, a, coef_as<T>(cf), g.TY, g.RS, g.S, g.ncw,
            c.err_flag);
@@ -801,41 +795,42 @@ extern "C" int rsdft_gpu_hamiltonian(int k, int s, const double* tpsi, double* h
 // coefficients uVunk(nzlma, nb), lives in the file-scope array below, which
 // every GPU that loads this library holds until the process exits.  In host
 // code the array's name is a host-side stand-in, not a device address, so the
-// kernel is given the address cudaGetSymbolAddress returns for the current
-// device (looked up on the first call on each device).
+// kernel is given the address cudaGetSymbolAddress returns for the bound
+// device.  rsdft_gpu_init looks it up (with that device current) and the
+// context keeps it, so a finalize / device reset / init sequence looks it up
+// again instead of reusing an address from an earlier context.
 namespace rsdft {
-namespace {
 
 static __device__ __align__(256) double g_hpsi_noalloc_uvunk[RSDFT_NOALLOC_SCRATCH_VALUES];
 
-constexpr int kMaxDevices = 64;
-std::mutex g_noalloc_mutex;
-double* g_noalloc_addr[kMaxDevices] = {};
+int noalloc_bind_scratch() {
+    Context& c = ctx();
+    void* p = nullptr;
+    const cudaError_t e = cudaGetSymbolAddress(&p, g_hpsi_noalloc_uvunk);
+    if (e != cudaSuccess || !p) {
+        set_error("cudaGetSymbolAddress of the static hamiltonian_noalloc scratch failed on device %d: %s", c.device,
+                  cudaGetErrorString(e));
+        return RSDFT_ECUDA;
+    }
+    c.noalloc_scratch = static_cast<double*>(p);
+    return RSDFT_OK;
+}
+
+namespace {
 
 int noalloc_scratch(double** out) {
     int dev = -1;
     RS_CUDA(cudaGetDevice(&dev));
-    if (dev < 0 || dev >= kMaxDevices) {
-        set_error("hamiltonian_noalloc: device ordinal %d outside 0..%d", dev, kMaxDevices - 1);
-        return RSDFT_EUNSUP;
-    }
     if (dev != ctx().device) {
         set_error("hamiltonian_noalloc: current device %d is not the device %d given to rsdft_gpu_init", dev,
                   ctx().device);
         return RSDFT_EINVAL;
     }
-    std::lock_guard<std::mutex> lock(g_noalloc_mutex);
-    if (!g_noalloc_addr[dev]) {
-        void* p = nullptr;
-        const cudaError_t e = cudaGetSymbolAddress(&p, g_hpsi_noalloc_uvunk);
-        if (e != cudaSuccess || !p) {
-            set_error("hamiltonian_noalloc: cudaGetSymbolAddress of the static scratch failed on device %d: %s", dev,
-                      cudaGetErrorString(e));
-            return RSDFT_ECUDA;
-        }
-        g_noalloc_addr[dev] = static_cast<double*>(p);
+    if (!ctx().noalloc_scratch) {
+        set_error("hamiltonian_noalloc: the static scratch has no device address (rsdft_gpu_init did not bind it)");
+        return RSDFT_ENOTINIT;
     }
-    *out = g_noalloc_addr[dev];
+    *out = ctx().noalloc_scratch;
     return RSDFT_OK;
 }
 
@@ -903,7 +898,12 @@ extern "C" int rsdft_gpu_hamiltonian_noalloc(int k, int s, const double* tpsi, d
         return RSDFT_EINVAL;
     }
     void *dpsi = nullptr, *dh = nullptr;
-    if (!resolve(tpsi, &dpsi) || !resolve(htpsi, &dh)) {
+    const size_t span = sizeof(double) * (size_t)ld * (size_t)nb;
+    const int rp = resolve(tpsi, span, &dpsi);
+    if (rp < 0) return rp;
+    const int rh = resolve(htpsi, span, &dh);
+    if (rh < 0) return rh;
+    if (!rp || !rh) {
         set_error("hamiltonian_noalloc: tpsi and htpsi must be device memory or lie in a registered wavefunction "
                   "(this entry point stages nothing)");
         return RSDFT_EINVAL;

@@ -445,12 +445,7 @@ template <int BN, int NT, int NS, bool DRAIN, bool BMN = false>
 static int launch_umma(const UmmaMaps& maps, const UmmaArgs& g, dim3 grid) {
     constexpr int STAGE = NT * (UB_M * UB_K * 2 + BN * UB_K * 2);
     const size_t smem = (size_t)NS * STAGE + 256;
-    static bool attr = false;
-    if (!attr) {
-        RS_CUDA(cudaFuncSetAttribute(k_umma<BN, NT, NS, DRAIN, BMN>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                     (int)smem));
-        attr = true;
-    }
+    RS_CHECK(set_smem_optin((const void*)k_umma<BN, NT, NS, DRAIN, BMN>, (int)smem));
     launch(k_umma<BN, NT, NS, DRAIN, BMN>, grid, U_THREADS, smem, ctx().stream, maps, g);
     RS_LAUNCH();
     return RSDFT_OK;

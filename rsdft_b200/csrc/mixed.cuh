@@ -33,6 +33,6 @@ int rotate_mixed(const double* psi, double* out, long ld, int nb, const double* 
 int rotate_mixed(const float* psi, double* out, long ld, int nb, const double* V, int ldv, int nterms,
                  const void* psi_split = nullptr);
 
-inline int mode_terms(int mode) { return mode == RSDFT_MODE_MIXED_BF16 ? 3 : 2; }
+inline int mode_terms(int mode) { return mode == RSDFT_MODE_MIXED_BF16X3 ? 3 : 2; }
 
 }  // namespace rsdft

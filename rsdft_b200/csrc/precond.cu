@@ -582,12 +582,7 @@ static int pc_tma_step(const T* src, const T* const* aux, T* wout, const PcArgs&
         return RSDFT_OK;
     for (int a = 0; a < NA; ++a)
         if (encode_tmap_4d(&maps.aux[a], dt, aux[a], dims, strides, bm) != RSDFT_OK) return RSDFT_OK;
-    static bool attr_set = false;
-    if (!attr_set) {
-        RS_CUDA(cudaFuncSetAttribute(k_pc_tma<T, K, STORE>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                     220 * 1024 + 8 * 16));
-        attr_set = true;
-    }
+    RS_CHECK(set_smem_optin((const void*)k_pc_tma<T, K, STORE>, 220 * 1024 + 8 * 16));
     // coefficients of the operator part: (A - I) for w_0, B = offdiag / d for
     // w_1, 2 B for the later steps
     StencilCoef cf{};

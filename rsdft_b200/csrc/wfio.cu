@@ -156,18 +156,13 @@ struct Bands {
 // registration and set up the pinned buffers.
 int bands_open(Bands& b, const double* unk, size_t span, long ml) {
     void* d = nullptr;
-    if (!resolve(unk, &d)) {
+    const int r = resolve(unk, span * sizeof(double), &d);
+    if (r < 0) return r;
+    if (!r) {
         b.host = const_cast<double*>(unk);
         return RSDFT_OK;
     }
     RS_CHECK(require_init());
-    const char* c = reinterpret_cast<const char*>(unk);
-    for (const auto& r : ctx().regs) {
-        if (c >= r.host && c < r.host + r.bytes && c + span * sizeof(double) > r.host + r.bytes) {
-            set_error("wavefunction file: the array extends past its registered range");
-            return RSDFT_EINVAL;
-        }
-    }
     b.dev = static_cast<double*>(d);
     for (int i = 0; i < 2; ++i) {
         RS_CUDA(cudaMallocHost(&b.pin[i], sizeof(double) * (size_t)ml));

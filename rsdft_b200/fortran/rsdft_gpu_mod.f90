@@ -33,7 +33,8 @@ MODULE rsdft_gpu_mod
             gpu_subspace_mate_sl, gpu_subspace_solv_sl, gpu_subspace_rotv_sl, gpu_esp_calc, gpu_calc_force_ps_nloc2, &
             gpu_calc_density, gpu_wf_io_write, gpu_wf_io_read
 
-  integer(c_int), parameter, PUBLIC :: RSDFT_MODE_FP64 = 0, RSDFT_MODE_MIXED_BF16 = 1, RSDFT_MODE_MIXED_BF16X3 = 2
+  integer(c_int), parameter, PUBLIC :: RSDFT_MODE_FP64 = 0, RSDFT_MODE_MIXED_BF16X3 = 1, &
+                                       RSDFT_MODE_MIXED_TF32 = 2, RSDFT_MODE_MIXED_BF16X2 = 3
 
   interface
      integer(c_int) function rsdft_gpu_init(device) bind(C, name="rsdft_gpu_init")

@@ -33,7 +33,7 @@ ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 if ROOT not in sys.path:
     sys.path.insert(0, ROOT)
 
-MODES = {"fp64": 0, "mixed-bf16": 1, "mixed-bf16x3": 2}
+MODES = {"fp64": 0, "mixed-bf16x3": 1, "mixed-tf32": 2, "mixed-bf16x2": 3}
 
 
 def _setup(workload: str, ngrid: int = 0, bands: int = 0):
@@ -127,7 +127,7 @@ def run_large(args) -> dict:
     occ[: cell.nocc] = 2.0
     out = {"what": "large", "workload": args.workload, "grid": list(cell.ngrid), "bands": MB, "steps": args.steps}
     res = {}
-    for name, mode in (("fp64", 0), ("mixed-bf16", 1)):
+    for name, mode in (("fp64", 0), ("mixed-bf16x3", 1)):
         u = start.t().contiguous().t()
         esp = torch.zeros(MB, dtype=torch.float64, device="cuda")
         r = torch.zeros_like(esp)
@@ -153,8 +153,8 @@ def run_large(args) -> dict:
                      "adjoint_force_ms": f0.elapsed_time(f1)}
         del u
     occn = cell.nocc
-    out["eig_err_max_occupied_ha"] = float(np.abs(res["fp64"][0][:occn] - res["mixed-bf16"][0][:occn]).max())
-    out["force_err_max_ha_bohr"] = float(np.abs(res["fp64"][1] - res["mixed-bf16"][1]).max())
+    out["eig_err_max_occupied_ha"] = float(np.abs(res["fp64"][0][:occn] - res["mixed-bf16x3"][0][:occn]).max())
+    out["force_err_max_ha_bohr"] = float(np.abs(res["fp64"][1] - res["mixed-bf16x3"][1]).max())
     h = api.fortran_empty(ML, MB)
     ms = _timed(torch, st, lambda: g.hamiltonian(1, 1, start, h, 1, ML, 1, MB), 2, 5)
     nbytes = MB * ML * 16 + ML * 8 + int(cell.lma_ptr[-1]) * 12
@@ -182,7 +182,7 @@ def main(argv=None) -> None:
     it.add_argument("--bands", type=int, default=0)
     rr = sub.add_parser("rr")
     rr.add_argument("--workload", default="si216")
-    rr.add_argument("--mode", default="mixed-bf16", choices=sorted(MODES))
+    rr.add_argument("--mode", default="mixed-bf16x3", choices=sorted(MODES))
     rr.add_argument("--ngrid", type=int, default=0)
     rr.add_argument("--bands", type=int, default=0)
     rr.add_argument("--warmup", type=int, default=2)

@@ -69,7 +69,7 @@ def test_every_entry_is_defined_once_and_opens_a_trace_range():
     defs = re.findall(r'(?m)^(?:extern "C" )?(?:int|long long|const char\*) (rsdft_gpu_\w+)\([^)]*\)\s*\{\s*(\S+)', src)
     names = [n for n, _ in defs]
     assert sorted(names) == declared()
-    getters = {"rsdft_gpu_last_error", "rsdft_gpu_kernel_launches"}
+    getters = {"rsdft_gpu_last_error", "rsdft_gpu_kernel_launches", "rsdft_gpu_workspace_bytes"}
     for name, first in defs:
         if name not in getters:
             assert first == "RS_ENTRY();", f"{name} does not open with RS_ENTRY()"

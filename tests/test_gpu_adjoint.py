@@ -58,7 +58,7 @@ def set_vloc(c, v):
 def converged(gpu, cells):
     c, o = prepare(gpu, cells, "si64_adjoint")
     u64, e64, r64 = converge(gpu, c, o, api.MODE_FP64)
-    umx, emx, rmx = converge(gpu, c, o, api.MODE_MIXED_BF16)
+    umx, emx, rmx = converge(gpu, c, o, api.MODE_MIXED_BF16X3)
     return c, o, (u64, e64, r64), (umx, emx, rmx)
 
 

@@ -18,7 +18,7 @@ from test_gpu_parity import dev, host, overlap_check, prepare, rel
 pytestmark = pytest.mark.gpu
 
 
-@pytest.mark.parametrize("mode,tol", [(api.MODE_MIXED_BF16, 3e-6), (api.MODE_MIXED_BF16X3, 2e-4)])
+@pytest.mark.parametrize("mode,tol", [(api.MODE_MIXED_BF16X3, 3e-6), (api.MODE_MIXED_BF16X2, 2e-4)])
 @pytest.mark.parametrize("name,nb", [("si8", 32), ("si64", 160)])
 def test_mixed_gram_schmidt(gpu, cells, mode, tol, name, nb):
     c, o = prepare(gpu, cells, name)
@@ -33,7 +33,7 @@ def test_mixed_gram_schmidt(gpu, cells, mode, tol, name, nb):
     assert rel(g, ref) <= 50 * tol
 
 
-@pytest.mark.parametrize("mode,tol", [(api.MODE_MIXED_BF16, 3e-6), (api.MODE_MIXED_BF16X3, 1e-4)])
+@pytest.mark.parametrize("mode,tol", [(api.MODE_MIXED_BF16X3, 3e-6), (api.MODE_MIXED_BF16X2, 1e-4)])
 def test_mixed_subspace_diag(gpu, cells, mode, tol):
     c, o = prepare(gpu, cells, "si64")
     nb = 160
@@ -48,7 +48,7 @@ def test_mixed_subspace_diag(gpu, cells, mode, tol):
     assert overlap_check(host(u), ref, w, c.dV, gap_tol=1e-3) <= 1e3 * tol
 
 
-@pytest.mark.parametrize("mode,tol", [(api.MODE_MIXED_BF16, 3e-6), (api.MODE_MIXED_BF16X3, 1e-4)])
+@pytest.mark.parametrize("mode,tol", [(api.MODE_MIXED_BF16X3, 3e-6), (api.MODE_MIXED_BF16X2, 1e-4)])
 def test_mixed_orth_subspace_diag(gpu, cells, mode, tol):
     c, o = prepare(gpu, cells, "si64")
     nb = 160
@@ -73,9 +73,9 @@ def test_mixed_sweep_matches_separate_calls(gpu, cells):
     ua, ub = dev(q), dev(q)
     ea = torch.zeros(nb, dtype=torch.float64, device="cuda")
     eb, ra, rb = torch.zeros_like(ea), torch.zeros_like(ea), torch.zeros_like(ea)
-    gpu.conjugate_gradient(1, c.ML, nb, 1, 1, ua, ea, ra, ncg=4, mloop=3, mode=api.MODE_MIXED_BF16)
-    gpu.orth_subspace_diag(1, 1, ua, ea, mode=api.MODE_MIXED_BF16)
-    gpu.eigensolver_sweep(1, 1, ub, eb, rb, ncg=4, mloop=3, mode=api.MODE_MIXED_BF16)
+    gpu.conjugate_gradient(1, c.ML, nb, 1, 1, ua, ea, ra, ncg=4, mloop=3, mode=api.MODE_MIXED_BF16X3)
+    gpu.orth_subspace_diag(1, 1, ua, ea, mode=api.MODE_MIXED_BF16X3)
+    gpu.eigensolver_sweep(1, 1, ub, eb, rb, ncg=4, mloop=3, mode=api.MODE_MIXED_BF16X3)
     torch.cuda.synchronize()
     assert np.abs(host(ea) - host(eb)).max() <= 3e-6 * max(1.0, np.abs(host(ea)).max())
     assert np.abs(host(ra) - host(rb)).max() <= 1e-12 * max(1.0, np.abs(host(ra)).max())
@@ -90,7 +90,7 @@ def test_mixed_cg_sweep_fp32(gpu, cells):
     u = dev(q)
     esp = torch.zeros(c.nband, dtype=torch.float64, device="cuda")
     res = torch.zeros_like(esp)
-    gpu.conjugate_gradient(1, c.ML, c.nband, 1, 1, u, esp, res, ncg=4, mloop=3, mode=api.MODE_MIXED_BF16)
+    gpu.conjugate_gradient(1, c.ML, c.nband, 1, 1, u, esp, res, ncg=4, mloop=3, mode=api.MODE_MIXED_BF16X3)
     torch.cuda.synchronize()
     # FP32 storage and arithmetic in the sweeps: eigenvalue estimates to ~1e-6
     assert np.abs(host(esp) - resp).max() <= 1e-5 * max(1.0, np.abs(resp).max())
@@ -106,7 +106,7 @@ def test_mixed_iteration_tracks_fp64(gpu, cells):
     res = torch.zeros_like(ea)
     for _ in range(3):
         gpu.eigensolver_iteration(ua, ea, res, ncg=4, mloop=3, mode=api.MODE_FP64)
-        gpu.eigensolver_iteration(ub, eb, res, ncg=4, mloop=3, mode=api.MODE_MIXED_BF16)
+        gpu.eigensolver_iteration(ub, eb, res, ncg=4, mloop=3, mode=api.MODE_MIXED_BF16X3)
     torch.cuda.synchronize()
     assert np.abs(host(ea) - host(eb)).max() <= 1e-5
 
@@ -122,7 +122,7 @@ def test_mixed_then_fp64_closing_pass(gpu, cells):
     res = torch.zeros_like(ea)
     for _ in range(4):
         gpu.eigensolver_iteration(ua, ea, res, ncg=4, mloop=3, mode=api.MODE_FP64)
-        gpu.eigensolver_iteration(ub, eb, res, ncg=4, mloop=3, mode=api.MODE_MIXED_BF16)
+        gpu.eigensolver_iteration(ub, eb, res, ncg=4, mloop=3, mode=api.MODE_MIXED_BF16X3)
     gpu.finalize_fp64(ua, ea, res)
     gpu.finalize_fp64(ub, eb, res)
     torch.cuda.synchronize()
@@ -131,7 +131,7 @@ def test_mixed_then_fp64_closing_pass(gpu, cells):
     assert np.abs(host(ea) - host(eb)).max() <= 1e-5
 
 
-@pytest.mark.parametrize("mode,tol", [(api.MODE_MIXED_BF16, 3e-6), (api.MODE_MIXED_BF16X3, 1e-4)])
+@pytest.mark.parametrize("mode,tol", [(api.MODE_MIXED_BF16X3, 3e-6), (api.MODE_MIXED_BF16X2, 1e-4)])
 def test_mixed_general_shapes(gpu, cells, mode, tol):
     """ML = 18^3 (not a multiple of 32: the rotation takes the transposed
     split; FP32 rows of 18 take the general stencil) and 36 bands (the band
@@ -167,13 +167,13 @@ def test_mixed_sweep_host_array_overlapped_upload(gpu, cells):
     ud = dev(q)
     ed = torch.zeros(nb, dtype=torch.float64, device="cuda")
     rd = torch.zeros_like(ed)
-    gpu.eigensolver_sweep(1, 1, ud, ed, rd, ncg=4, mloop=3, mode=api.MODE_MIXED_BF16)
+    gpu.eigensolver_sweep(1, 1, ud, ed, rd, ncg=4, mloop=3, mode=api.MODE_MIXED_BF16X3)
     host_pinned = torch.empty((nb, c.ML), dtype=torch.float64, pin_memory=True)
     host_pinned.copy_(torch.from_numpy(np.ascontiguousarray(q.T)))
     uh = host_pinned.numpy().T  # (ML, nb) Fortran view of pinned memory
     eh = np.zeros(nb)
     rh = np.zeros(nb)
-    gpu.eigensolver_sweep(1, 1, uh, eh, rh, ncg=4, mloop=3, mode=api.MODE_MIXED_BF16)
+    gpu.eigensolver_sweep(1, 1, uh, eh, rh, ncg=4, mloop=3, mode=api.MODE_MIXED_BF16X3)
     torch.cuda.synchronize()
     assert np.array_equal(host(ed), eh) and np.array_equal(host(rd), rh)
     assert np.array_equal(host(ud), uh)
