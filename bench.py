@@ -14,8 +14,9 @@ Printed JSON line (rank 0):
                runs the iteration and downloads it with the eigenvalues
   roofline     hpsi (projection + fused stencil/Vloc/nonlocal kernels) on all
                bands: algorithmic bytes / measured duration vs measured HBM peak
-  cpu_baseline the oracle (C/OpenMP + numpy BLAS) on the host cores, a
-               bounded sample of the same iteration (rank 0, N = 1)
+  cpu_baseline the oracle (C/OpenMP + numpy BLAS) on the host cores: one
+               whole iteration of the same workload, every band (rank 0,
+               N = 1)
 ``--impl reference`` times only that CPU implementation (the reference is
 Fortran and cannot be built in this image; the oracle restates it).
 Multi-GPU (torchrun): independent replicas, one per GPU ("scaling": "weak").
@@ -46,13 +47,12 @@ def parse():
     p.add_argument("--warmup", type=int, default=3)
     p.add_argument("--impl", default="ours", choices=["ours", "reference"])
     p.add_argument("--workload", default="si216")
-    p.add_argument("--mode", default="auto", choices=["auto", "fp64", "mixed-bf16x3", "mixed-bf16x2"])
+    p.add_argument("--mode", default="auto", choices=["auto"] + sorted(MODES))
     p.add_argument("--ncg", type=int, default=4)
     p.add_argument("--mloop", type=int, default=3)
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--no-e2e", action="store_true")
     p.add_argument("--no-accuracy", action="store_true", help="skip the 10-iteration accuracy comparison")
-    p.add_argument("--cpu-sample-bands", type=int, default=6)
     return p.parse_args()
 
 
@@ -135,47 +135,75 @@ class ClockSampler:
 
 
 # ------------------------------------------------------------ CPU baseline
-def cpu_iteration_rate(cell, sample_bands: int, ncg: int, mloop: int):
-    """Oracle timing of one eigensolver iteration on a bounded sample.
+def host_info():
+    """CPU model, logical cores and the BLAS numpy/scipy call (the oracle's
+    dense steps)."""
+    model = "unknown"
+    try:
+        for ln in open("/proc/cpuinfo"):
+            if ln.lower().startswith("model name"):
+                model = ln.split(":", 1)[1].strip()
+                break
+    except OSError:
+        pass
+    blas = "unknown"
+    try:
+        cfg = np.show_config(mode="dicts")["Build Dependencies"]["blas"]
+        blas = f"{cfg.get('name', '?')} {cfg.get('version', '')}".strip()
+    except Exception:  # noqa: BLE001 - numpy builds without the dict form
+        pass
+    return {"cpu_model": model, "logical_cores": os.cpu_count(), "blas": blas}
 
-    CG runs band by band exactly as the reference does, so its cost is
-    measured on ``sample_bands`` bands and scaled to all bands; hpsi of the
-    subspace step likewise; the BLAS-3 steps (literal recursive Gram-Schmidt,
-    dsyr2k, dsyev, rotation) are timed at full size.
-    """
+
+def cpu_iteration(o, cell, psi, ncg: int, mloop: int):
+    """One full eigensolver iteration on the oracle, as calc_sweep runs it
+    (sweep_module.f90:150-155): conjugate_gradient_1 on every band (band by
+    band, cg_module.f90:97-430), the literal recursive gram_schmidt_t
+    (gram_schmidt_t_module.f90:84-316), then subspace_diag_la with H psi of
+    every band, dsyr2k, DSYEV and the rotation (subspace_diag_la_module.f90:
+    18-232).  Returns the new bands and the seconds of each step."""
+    t0 = time.perf_counter()
+    u, _, _, _ = o.conjugate_gradient(psi, ncg, mloop)
+    t1 = time.perf_counter()
+    u = o.gram_schmidt_t(u)
+    t2 = time.perf_counter()
+    u, _, _ = o.subspace_diag_la(u)
+    t3 = time.perf_counter()
+    return np.asfortranarray(u), {"cg": t1 - t0, "gram_schmidt": t2 - t1, "subspace_diag": t3 - t2}
+
+
+def cpu_baseline_run(cell, ncg: int, mloop: int, steps: int, warmup: int):
+    """The oracle (C/OpenMP on all host threads + numpy/OpenBLAS) timed on
+    whole iterations of the full workload (every band), continuing from the
+    seeded start bands after Gram-Schmidt: `warmup` untimed iterations, then
+    `steps` timed ones; median seconds per iteration."""
     from oracle import oracle as O  # CPU baseline leg only
 
     o = O.Oracle(cell)
-    MB, ML = cell.nband, cell.ML
-    psi = np.asfortranarray(cell.psi0())
-    ns = max(1, min(sample_bands, MB))
-    t0 = time.perf_counter()
-    o.conjugate_gradient(psi[:, :ns], ncg, mloop)
-    t_cg = (time.perf_counter() - t0) * MB / ns
-    t0 = time.perf_counter()
-    o.hamiltonian(psi[:, :ns])
-    t_h = (time.perf_counter() - t0) * MB / ns
-    t0 = time.perf_counter()
-    q = o.gram_schmidt_t(psi)
-    t_gs = time.perf_counter() - t0
-    t0 = time.perf_counter()
-    hs = 0.5 * cell.dV * (q.T @ psi + psi.T @ q)  # dsyr2k-shaped contraction (psi stands in for H psi)
-    import scipy.linalg.lapack as lapack
-
-    w, v, info = lapack.dsyev(np.triu(hs), compute_v=1, lower=0)
-    _ = q @ v
-    t_sub = time.perf_counter() - t0 + t_h
-    total = t_cg + t_gs + t_sub
-    threads = O.lib().oracle_num_threads()
+    psi = o.gram_schmidt_t(np.asfortranarray(cell.psi0()))
+    for _ in range(warmup):
+        psi, _ = cpu_iteration(o, cell, psi, ncg, mloop)
+    per, parts = [], []
+    for _ in range(steps):
+        t0 = time.perf_counter()
+        psi, sec = cpu_iteration(o, cell, psi, ncg, mloop)
+        per.append(time.perf_counter() - t0)
+        parts.append(sec)
+    threads = int(O.lib().oracle_num_threads())
+    med = statistics.median(per)
+    info = host_info()
     return {
-        "value": 1.0 / total,
+        "value": 1.0 / med,
         "unit": "iter/s",
-        "cores": int(threads),
+        "cores": threads,
         "kind": "port",
-        "sample": (f"oracle (C/OpenMP {threads} threads + numpy BLAS): CG on {ns} of {MB} bands and hpsi on "
-                   f"{ns} bands scaled x{MB / ns:.0f}; literal recursive Gram-Schmidt, dsyr2k, dsyev and rotation "
-                   f"at full size ({ML} x {MB})"),
-        "seconds": {"cg": t_cg, "gram_schmidt": t_gs, "subspace": t_sub},
+        "sample": (f"oracle (C/OpenMP, {threads} threads, + numpy/{info['blas']}): {steps} whole iteration(s) of "
+                   f"{cell.nband} bands x {cell.ML} points after {warmup} untimed, median; no scaling"),
+        "steps": steps,
+        "warmup": warmup,
+        "seconds_per_iter": per,
+        "seconds": {k: statistics.median(p[k] for p in parts) for k in parts[0]},
+        "host": info,
     }
 
 
@@ -187,30 +215,31 @@ def metric_name(cell, ncg):
 
 
 def run_reference(args, rank, world):
+    """The reference arm: the reference's CPU path (its Fortran cannot be
+    built in this image, so the oracle's restatement of it) on the host
+    cores, rank 0 only.  Whole iterations of the full workload: at most 3
+    timed after at most 1 untimed (about 20-40 s each), and the line says
+    how many ran."""
     if rank != 0:
         return
     from rsdft_b200.cell import build_cell
 
     cell = build_cell(args.workload)
-    # warm-up then timed samples, each a bounded sample of the iteration
-    w = max(0, min(args.warmup, 1))
-    for _ in range(w):
-        cpu_iteration_rate(cell, 1, args.ncg, args.mloop)
-    rates = []
+    steps = max(1, min(args.steps, 3))
+    warmup = max(0, min(args.warmup, 1))
     t0 = time.perf_counter()
-    for _ in range(max(1, min(args.steps, 3))):
-        rates.append(cpu_iteration_rate(cell, args.cpu_sample_bands, args.ncg, args.mloop))
+    r = cpu_baseline_run(cell, args.ncg, args.mloop, steps, warmup)
     wall = time.perf_counter() - t0
-    r = rates[-1]
-    v = statistics.median(x["value"] for x in rates)
+    v = r["value"]
     out = {
         "impl": "reference",
         "metric": metric_name(cell, args.ncg),
         "value": v,
         "unit": "iter/s",
         "n_gpus": world,
-        "steps": len(rates),
-        "warmup": w,
+        "ranks_used": 1,
+        "steps": steps,
+        "warmup": warmup,
         "ms_per_step": 1000.0 / v,
         "higher_is_better": True,
         "scaling": "weak",
@@ -219,10 +248,12 @@ def run_reference(args, rank, world):
         "data": "synthetic (seeded Si cell, random start bands)",
         "config": {"workload": f"{args.workload}", "grid": list(cell.ngrid), "bands": cell.nband, "Md": cell.md,
                    "ncg": args.ncg, "mloop": args.mloop},
-        "cpu_baseline": {"value": v, "unit": "iter/s", "cores": r["cores"], "kind": "port", "sample": r["sample"]},
+        "cpu_baseline": {k: r[k] for k in ("value", "unit", "cores", "kind", "sample", "steps", "warmup", "host")},
         "e2e": {"value": v, "unit": "iter/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        "seconds": r["seconds"],
         "note": ("The reference is Fortran+MPI; no Fortran compiler exists in this image, so its CPU path is "
-                 "timed through the oracle's line-by-line restatement."),
+                 "timed through the oracle's line-by-line restatement, on one process (rank 0) whatever the "
+                 "number of ranks launched."),
         "wall_s": wall,
     }
     print(json.dumps(out), flush=True)
@@ -413,7 +444,7 @@ def main():
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        cpu = cpu_iteration_rate(cell, args.cpu_sample_bands, args.ncg, args.mloop)
+        cpu = cpu_baseline_run(cell, args.ncg, args.mloop, 1, 0)
 
     if rank == 0:
         ms = results[head]["ms"]

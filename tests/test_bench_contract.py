@@ -31,6 +31,9 @@ def test_reference_arm_line():
     assert d["vs_baseline"] is None and d["config"]["workload"] == "si8"
     cb = d["cpu_baseline"]
     assert cb["value"] == d["value"] and cb["kind"] in ("port", "reference") and cb["cores"] >= 1 and cb["sample"]
+    # whole iterations actually timed, no scaling; the host is described
+    assert (cb["steps"], cb["warmup"]) == (d["steps"], d["warmup"]) and "scaled" not in cb["sample"]
+    assert cb["host"]["cpu_model"] and cb["host"]["blas"] and d["ranks_used"] == 1
     e2e = d["e2e"]
     assert e2e["value"] == d["value"] and e2e["unit"] == d["unit"]
     assert e2e["h2d_bytes_per_step"] == 0 and e2e["d2h_bytes_per_step"] == 0
@@ -51,4 +54,5 @@ def test_reference_arm_under_torchrun_prints_once():
     assert out.returncode == 0, out.stderr[-2000:]
     lines = [ln for ln in out.stdout.splitlines() if ln.startswith("{")]
     assert len(lines) == 1
-    assert json.loads(lines[0])["impl"] == "reference"
+    d = json.loads(lines[0])
+    assert d["impl"] == "reference" and d["n_gpus"] == 2 and d["ranks_used"] == 1

@@ -322,6 +322,28 @@ def test_registered_host_wavefunction(gpu, cells):
         gpu.unregister_wf(unk)
 
 
+def test_span_past_registration_rejected(gpu, cells):
+    """A block that starts inside a registered array but runs past its end
+    is refused (EINVAL) before any kernel runs, by the staging and the
+    no-allocation entries alike; the same block within range works."""
+    c, o = prepare(gpu, cells, "si8")
+    unk = np.array(c.psi0(), order="F", copy=True)
+    gpu.register_wf(unk)
+    try:
+        nb = c.nband - 4 + 1  # from column 5: one band more than is left
+        out = api.fortran_empty(c.ML, nb)
+        for call in (gpu.hamiltonian, gpu.hamiltonian_noalloc):
+            with pytest.raises(api.RsdftError) as e:
+                call(1, 1, unk[:, 4:], out, 1, c.ML, 5, 4 + nb)
+            assert e.value.code == -1 and "registered" in str(e.value)
+        ok = api.fortran_empty(c.ML, c.nband - 4)
+        gpu.hamiltonian(1, 1, unk[:, 4:], ok, 1, c.ML, 5, c.nband)
+        torch.cuda.synchronize()
+        assert rel(host(ok), o.hamiltonian(unk[:, 4:])) <= TOL
+    finally:
+        gpu.unregister_wf(unk)
+
+
 def test_error_statuses(gpu, cells):
     c, o = prepare(gpu, cells, "si8_g12")
     psi = np.asfortranarray(c.psi0())

@@ -7,8 +7,11 @@ RSDFT_NOALLOC_SCRATCH_VALUES doubles shared by every call.
 Checked through the C ABI against rsdft_gpu_hamiltonian on two calls in a row
 (the second with other bands and another band count, so a stale scratch would
 show), within the 1e-12 relative tolerance of the other hpsi parity tests, and
-for the clear rejection of a band count whose scratch would not fit.  The file
-name makes pytest collect it last.
+for the clear rejection of a band count whose scratch would not fit.  The
+entry is called before rsdft_gpu_hamiltonian every time, so a no-alloc path
+that fell back on the library's workspace would find none yet; the first test
+asserts that the library's workspace and the device's free memory do not
+change across a call.  The file name makes pytest collect it last.
 """
 import os
 import re
@@ -32,14 +35,39 @@ def scratch_values():
 
 
 def both(gpu, c, psi):
+    """(rsdft_gpu_hamiltonian, rsdft_gpu_hamiltonian_noalloc) of psi; the
+    no-alloc entry runs first."""
     nb = psi.shape[1]
     t = dev(psi)
     h_ref = torch.empty_like(t)
     h_new = torch.full_like(t, float("nan"))
-    gpu.hamiltonian(1, 1, t, h_ref, 1, c.ML, 1, nb)
     gpu.hamiltonian_noalloc(1, 1, t, h_new, 1, c.ML, 1, nb)
     torch.cuda.synchronize()
+    gpu.hamiltonian(1, 1, t, h_ref, 1, c.ML, 1, nb)
+    torch.cuda.synchronize()
     return host(h_ref), host(h_new)
+
+
+def test_noalloc_allocates_nothing(gpu, cells):
+    """Across a call the library's own workspace does not grow, and across a
+    second call (after the driver has loaded the kernels' code) the device's
+    free memory does not change."""
+    c, o = prepare(gpu, cells, "si64")
+    lib = _lib.load()
+    psi = np.asfortranarray(c.psi0()[:, :24])
+    t = dev(psi)
+    h = torch.full_like(t, float("nan"))
+    torch.cuda.synchronize()
+    ws0 = lib.rsdft_gpu_workspace_bytes()
+    gpu.hamiltonian_noalloc(1, 1, t, h, 1, c.ML, 1, 24)
+    torch.cuda.synchronize()
+    assert lib.rsdft_gpu_workspace_bytes() == ws0
+    free0 = torch.cuda.mem_get_info()[0]
+    gpu.hamiltonian_noalloc(1, 1, t, h, 1, c.ML, 1, 24)
+    torch.cuda.synchronize()
+    assert torch.cuda.mem_get_info()[0] == free0
+    assert lib.rsdft_gpu_workspace_bytes() == ws0
+    assert rel(host(h), o.hamiltonian(psi)) <= 1e-12
 
 
 def test_noalloc_matches_hamiltonian_twice(gpu, cells):
