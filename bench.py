@@ -302,7 +302,7 @@ def main():
     res = torch.zeros_like(esp)
 
     def supported(mode):
-        u = start.t().contiguous().t()
+        u = api.fortran_copy(start)
         try:
             g.gram_schmidt(1, MB, 1, 1, u, mode=mode)
             g.subspace_diag(1, 1, u, esp, mode=mode)
@@ -337,7 +337,7 @@ def main():
     sampler = ClockSampler(local)
     sampler.start()
     for mode in modes:
-        u = start.t().contiguous().t()
+        u = api.fortran_copy(start)
         for _ in range(args.warmup):
             iterate(u, mode)
         barrier()
@@ -363,8 +363,8 @@ def main():
     acc = {}
     if head != "fp64" and not args.no_accuracy:
         niter = 10
-        ua = start.t().contiguous().t()
-        ub = start.t().contiguous().t()
+        ua = api.fortran_copy(start)
+        ub = api.fortran_copy(start)
         ea = torch.zeros_like(esp)
         eb = torch.zeros_like(esp)
         ra = torch.zeros_like(esp)

@@ -191,6 +191,27 @@ int rsdft_gpu_orth_subspace_diag(int k, int s, double *unk, long ld, int mb, dou
 int rsdft_gpu_eigensolver_sweep(int k, int s, double *unk, long ld, int mb, double *esp, double *res, int ncg,
                                 int mloop, int ipc, int mode);
 
+/* calc_sweep's loop for the Gamma point with the bands kept on the device:
+ * for iter = 1..diter, for every spin s = 1..nspin, the sweep of
+ * rsdft_gpu_eigensolver_sweep on unk(:, :, s) (spin s at unk + (s-1) ld mb),
+ * then esp_gather (nothing to gather on one process), calc_fermi
+ * (Methfessel-Paxton order kinteg, smearing ekbt, nelectron electrons; fixed
+ * spin moment dspn while iter <= nfixed when nspin = 2) and conv_check:
+ * iconv_check 2 or 3 stops once max |esp - esp0| over bands 1..mb_ref of
+ * every spin is below tol_esp (3 also returns res = |esp - esp0|, -1 below
+ * tol_esp; 2 returns the CG residuals).  esp (mb, nspin) holds esp0 of the
+ * first iteration on entry and the Ritz values on exit; occ (mb, nspin) the
+ * occupations; *iter_out the iteration the loop stopped at, *conv_out 1 if
+ * it converged; *efermi (may be NULL) the Fermi level.  iconv_check 1 (the
+ * total-energy test) needs the SCF total energy: RSDFT_EUNSUP.
+ * (replaces calc_sweep, sweep_module.f90:60-226, with esp_gather,
+ * esp_gather_module.f90:11-61, calc_fermi, fermi_mp_module.f90:95-284, and
+ * conv_check, sweep_module.f90:228-280) */
+int rsdft_gpu_calc_sweep(double *unk, long ld, int mb, int nspin, double *esp, double *res, double *occ,
+                         int diter, int iconv_check, double tol_esp, int mb_ref, double nelectron, int nfixed,
+                         double dspn, double ekbt, int kinteg, int ncg, int mloop, int ipc, int mode,
+                         int *iter_out, int *conv_out, double *efermi);
+
 /* e(ns:ne) = dV <wf_n|H wf_n>, FP64 (no normalisation, as the reference).
  * (replaces esp_calc(k,s,wf,n1,n2,ns,ne,e), esp_calc_module.f90:15-49) */
 int rsdft_gpu_esp_calc(int k, int s, const double *wf, int n1, int n2, int ns, int ne, double *e);

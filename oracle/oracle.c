@@ -382,6 +382,202 @@ int oracle_force_nloc(const double *unk, long ML, int MB, const double *occ, con
     return 0;
 }
 
+/* ===========================================================================
+ * Reference path of the nonlocal force's derivative table (test
+ * infrastructure): the tabulated, interpolated duVdR of calc_force_ps_nloc2
+ * (ps_nloc2_module.f90:1489-1586), from the radial derivative tables of
+ * ps_nloc2_init_derivative (ps_nloc2_init_module.f90:219-301), polint /
+ * dpolint (polint_module.f90:11-77) and Ylm / Plm (ylm_module.f90:10-122).
+ * The product path uses the analytic derivative instead; these routines let
+ * the tests measure how far the two are apart.
+ * =========================================================================== */
+
+/* Plm (ylm_module.f90:75-122): associated Legendre function with the
+ * Condon-Shortley phase, upward recurrence in l */
+static double ref_plm(int L, int M, double xi)
+{
+    double x = xi;
+    if (fabs(fabs(x) - 1.0) < 1e-13) x = x < 0.0 ? -1.0 : 1.0;
+    double pmm = 1.0;
+    if (M > 0) {
+        const double somx2 = sqrt((1.0 - x) * (1.0 + x));
+        double fact = 1.0;
+        for (int i = 1; i <= M; ++i) {
+            pmm = -pmm * fact * somx2;
+            fact += 2.0;
+        }
+    }
+    if (L == M) return pmm;
+    double pmmp1 = x * (2.0 * M + 1.0) * pmm;
+    if (L == M + 1) return pmmp1;
+    double pll = 0.0;
+    for (int ll = M + 2; ll <= L; ++ll) {
+        pll = (x * (2.0 * ll - 1.0) * pmmp1 - (ll + M - 1.0) * pmm) / (ll - M);
+        pmm = pmmp1;
+        pmmp1 = pll;
+    }
+    return pll;
+}
+
+/* Ylm(x,y,z,L,M) (ylm_module.f90:10-72): real spherical harmonics */
+double oracle_ylm(double x, double y, double z, int L, int Min)
+{
+    const double pi = 3.141592653589793238, pi4 = 4.0 * pi;
+    const int M = Min < 0 ? -Min : Min;
+    if (L == 0) return 1.0 / sqrt(pi4);
+    if (x == 0.0 && y == 0.0 && z == 0.0) return 0.0;
+    double c = 1.0;
+    for (int k = L - M + 1; k <= L + M; ++k) c *= (double)k;
+    const double Clm = sqrt((2.0 * L + 1.0) / (c * pi4));
+    const double r = sqrt(x * x + y * y + z * z), ct = z / r;
+    double phi;
+    if (fabs(x) < 1e-10) phi = 0.5 * pi * (y < 0.0 ? -1.0 : 1.0);
+    else {
+        phi = atan(y / x);
+        if (x < 0) phi += pi;
+    }
+    if (Min > 0) return sqrt(2.0) * Clm * ref_plm(L, M, ct) * cos(phi * M);
+    if (Min == 0) return Clm * ref_plm(L, M, ct);
+    if (M % 2 == 0) return -sqrt(2.0) * Clm * ref_plm(L, M, ct) * sin(phi * M);
+    return sqrt(2.0) * Clm * ref_plm(L, M, ct) * sin(phi * M);
+}
+
+/* polint (polint_module.f90:11-41): Neville interpolation of ya(xa) at x; dy
+ * is the change of the averaged last column, the error estimate */
+static void ref_polint(const double *xa, const double *ya, int n, double x, double *y, double *dy, double *f0)
+{
+    for (int i = 0; i < n; ++i) f0[i] = ya[i];
+    double f0nm = ya[0], f0nm_0 = f0nm;
+    for (int m = 1; m <= n - 1; ++m) {
+        for (int i = 0; i < n - m; ++i) {
+            const double a = x - xa[i], b = x - xa[i + m];
+            f0[i] = (b * f0[i] - a * f0[i + 1]) / (b - a);
+        }
+        f0nm_0 = f0nm;
+        double s = 0.0;
+        for (int i = 0; i < n - m; ++i) s += f0[i];
+        f0nm = s / (n - m);
+    }
+    *y = f0[0];
+    *dy = f0nm - f0nm_0;
+}
+
+/* dpolint (polint_module.f90:44-77): the derivative of the Neville
+ * polynomial at x, with the same kind of error estimate */
+static void ref_dpolint(const double *xa, const double *ya, int n, double x, double *y, double *dy, double *f0,
+                        double *f1)
+{
+    for (int i = 0; i < n; ++i) {
+        f0[i] = ya[i];
+        f1[i] = 0.0;
+    }
+    double f1nm = (ya[1] - ya[0]) / (xa[1] - xa[0]), f1nm_0 = f1nm;
+    for (int m = 1; m <= n - 1; ++m) {
+        for (int i = 0; i < n - m; ++i) {
+            const double a = x - xa[i], b = x - xa[i + m];
+            f1[i] = (f0[i] - f0[i + 1] + b * f1[i] - a * f1[i + 1]) / (b - a);
+            f0[i] = (b * f0[i] - a * f0[i + 1]) / (b - a);
+        }
+        f1nm_0 = f1nm;
+        double s = 0.0;
+        for (int i = 0; i < n - m; ++i) s += f1[i];
+        f1nm = s / (n - m);
+    }
+    *y = f1[0];
+    *dy = f1nm - f1nm_0;
+}
+
+/* ps_nloc2_init_derivative (ps_nloc2_init_module.f90:219-301) for one
+ * orbital of angular momentum L with radial function viod on rad[0..nrc-1]:
+ * dv(i) = the dpolint derivative over the windows [i-m, i+m] (m = 1..20,
+ * clipped) with the smallest error estimate, then for J = |L-1| .. L+1
+ * (row t = J - |L-1| of out, nrc values each)
+ *   out = sqrt(4 pi / 3) (rad^2 dv + (2 + L(L+1) - J(J+1))/2 rad viod) */
+int oracle_dviod(const double *rad, const double *viod, int nrc, int L, double *out)
+{
+    double *dv = malloc(sizeof(double) * (size_t)nrc), *f0 = malloc(sizeof(double) * 64),
+           *f1 = malloc(sizeof(double) * 64);
+    if (!dv || !f0 || !f1) { free(dv); free(f0); free(f1); return -1; }
+    for (int i = 0; i < nrc; ++i) {
+        double y0 = 0.0, dy0 = 1e10, y, dy;
+        for (int m = 1; m <= 20; ++m) {
+            const int m1 = i - m > 0 ? i - m : 0, m2 = i + m < nrc - 1 ? i + m : nrc - 1;
+            ref_dpolint(rad + m1, viod + m1, m2 - m1 + 1, rad[i], &y, &dy, f0, f1);
+            if (fabs(dy) < dy0) { y0 = y; dy0 = fabs(dy); }
+        }
+        dv[i] = y0;
+    }
+    const double c43 = sqrt(4.0 * acos(-1.0) / 3.0);
+    const int J0 = L > 0 ? L - 1 : 1 - L;
+    for (int J = J0, t = 0; J <= L + 1; ++J, ++t) {
+        const double cj = 0.5 * (2.0 + L * (L + 1) - J * (J + 1));
+        for (int i = 0; i < nrc; ++i) out[(long)t * nrc + i] = c43 * (rad[i] * rad[i] * dv[i] + cj * rad[i] * viod[i]);
+    }
+    free(dv); free(f0); free(f1);
+    return 0;
+}
+
+/* duVdR(1:3, j, lma) of calc_force_ps_nloc2 (ps_nloc2_module.f90:1507-1586,
+ * the polint branch) for the npt points of one projector (L, m):
+ * d[3 j .. 3 j + 2] = point - atom; dviod = oracle_dviod's rows for this
+ * orbital; gaunt = the three coupling tables of this (L, m), indexed
+ * [k][L1][L1z + L + 1] for L1 = 0 .. L + 1 (k = x, y, z);
+ * out[3 j + k] the derivative of uV with respect to the atom position. */
+int oracle_duvdr_ref(int L, const double *d, int npt, const double *rad, int nrc, const double *dviod,
+                     const double *gaunt, double *out)
+{
+    const double ep = 1e-8;
+    const int J0 = L > 0 ? L - 1 : 1 - L, W = 2 * L + 3, NL1 = L + 2;
+    int bad = 0;
+#pragma omp parallel for schedule(static) reduction(+ : bad)
+    for (int j = 0; j < npt; ++j) {
+        double f0[64];
+        const double x = d[3L * j], y = d[3L * j + 1], z = d[3L * j + 2];
+        const double r = sqrt(x * x + y * y + z * z);
+        double yy1 = 0.0, yy2 = 0.0, yy3 = 0.0;
+        for (int L1 = J0; L1 <= L + 1; ++L1) {
+            if (!(fabs(x) > 1e-14 || fabs(y) > 1e-14 || fabs(z) > 1e-14 || L1 == 0)) continue;
+            const double *dvi = dviod + (long)(L1 - J0) * nrc;
+            /* bisection on rad (1-based indices as the reference) */
+            int ir0 = 1, ir1 = nrc;
+            while (ir1 - ir0 > 1) {
+                const int ir = (ir0 + ir1) / 2;
+                if (rad[ir - 1] > r) ir1 = ir;
+                else ir0 = ir;
+            }
+            const int ir = ir0;
+            double tmp0 = 0.0;
+            if (ir <= 2) {
+                tmp0 = dvi[1] / (rad[1] * rad[1]);
+                if (ir < 1) ++bad;
+            } else if (ir <= nrc) {
+                double err0 = 1e10, tmp1, err;
+                for (int im = 1; im <= 20; ++im) {
+                    const int m1 = ir - im > 1 ? ir - im : 1, m2 = ir + im < nrc ? ir + im : nrc;
+                    ref_polint(rad + m1 - 1, dvi + m1 - 1, m2 - m1 + 1, r, &tmp1, &err, f0);
+                    if (fabs(err) < err0) {
+                        tmp0 = tmp1;
+                        err0 = fabs(err);
+                        if (err0 < ep) break;
+                    }
+                }
+                tmp0 = tmp0 / (r * r);
+            }
+            for (int L1z = -L1; L1z <= L1; ++L1z) {
+                const double t1 = tmp0 * oracle_ylm(x, y, z, L1, L1z);
+                const long g = (long)L1 * W + (L1z + L + 1);
+                yy1 += t1 * gaunt[0L * NL1 * W + g];
+                yy2 += t1 * gaunt[1L * NL1 * W + g];
+                yy3 -= t1 * gaunt[2L * NL1 * W + g];
+            }
+        }
+        out[3L * j] = yy1;
+        out[3L * j + 1] = yy2;
+        out[3L * j + 2] = yy3;
+    }
+    return bad ? -1 : 0;
+}
+
 int oracle_num_threads(void)
 {
 #ifdef _OPENMP

@@ -19,7 +19,13 @@ the reference makes:
   1x1 grid = dsyevd('V','L'));
 * ``subspace_rotv_sl`` subspace_rotv_sl_module.f90:24-135 (psi <- psi V);
 * ``dense_hamiltonian`` the explicit matrix of construct_hamiltonian_matrix
-  (hamiltonian_matrix_module.f90:31-145), an independent check of hpsi.
+  (hamiltonian_matrix_module.f90:31-145), an independent check of hpsi;
+* ``reference_duvdr`` the reference's tabulated, interpolated derivative
+  table of the nonlocal force (calc_force_ps_nloc2, ps_nloc2_module.f90:
+  1489-1586, on the radial tables of ps_nloc2_init_derivative,
+  ps_nloc2_init_module.f90:219-301, polint_module.f90, ylm_module.f90), with
+  ``gaunt_l1`` the coupling coefficients of get_gaunt_coefficient_L1
+  (force_sub_sub_module.f90:64-387) computed from their definition.
 """
 from __future__ import annotations
 
@@ -66,6 +72,10 @@ def lib():
         L.oracle_cg.argtypes = [_dp, ctypes.c_long, ctypes.c_int, _dp, _dp, ctypes.c_int, ctypes.c_int, _ip]
         L.oracle_force_nloc.argtypes = [_dp, ctypes.c_long, ctypes.c_int, _dp, _dp, _ip, ctypes.c_int, _dp]
         L.oracle_num_threads.restype = ctypes.c_int
+        L.oracle_ylm.argtypes = [ctypes.c_double] * 3 + [ctypes.c_int, ctypes.c_int]
+        L.oracle_ylm.restype = ctypes.c_double
+        L.oracle_dviod.argtypes = [_dp, _dp, ctypes.c_int, ctypes.c_int, _dp]
+        L.oracle_duvdr_ref.argtypes = [ctypes.c_int, _dp, ctypes.c_int, _dp, ctypes.c_int, _dp, _dp, _dp]
         _lib = L
     return _lib
 
@@ -159,6 +169,17 @@ class Oracle:
         return subspace_mate(u, hpsi, self.dV, mblk)
 
     # ----------------------------------------------------------------- force
+    def force_nloc_with(self, unk, occ, duv):
+        """force_nloc with the derivative table ``duv`` (nnz, 3) in place of
+        the cell's analytic one (e.g. ``reference_duvdr(cell)``)."""
+        u = np.asfortranarray(unk, dtype=np.float64)
+        occ = np.ascontiguousarray(occ, dtype=np.float64)
+        d = np.ascontiguousarray(duv, dtype=np.float64)
+        am = np.ascontiguousarray(self.cell.amap, dtype=np.int32)
+        f = np.zeros((self.cell.natom, 3))
+        lib().oracle_force_nloc(_p(u), self.ML, u.shape[1], _p(occ), _p(d), _p(am, _ip), self.cell.natom, _p(f))
+        return f
+
     def force_nloc(self, unk, occ):
         c = self.cell
         u = np.asfortranarray(unk, dtype=np.float64)
@@ -334,3 +355,172 @@ def dense_hamiltonian(cell):
 def vloc_adjoint(unk, occ, dV):
     """dE/dV(r) = sum_n f_n psi_n(r)^2 dV for E = sum f_n <psi|H|psi> dV."""
     return (np.asarray(unk) ** 2) @ np.asarray(occ) * dV
+
+
+# ---------------------------------------------------------------------------
+# Reference path of the nonlocal force's derivative table
+RAD_DR = 2e-3  # radial grid of the synthetic projector tables (rad1)
+
+
+def gaunt_l1(lmax: int):
+    """G[k][L][m + lmax][L1][L1z + lmax + 1] = integral over the unit sphere
+    of Ylm(L, m) * Ylm(1, q_k) * Ylm(L1, L1z), q = (1, -1, 0) for k = x, y,
+    z, with the reference's real harmonics (ylm_module.f90): the tables Y1,
+    Y2, Y3 of get_gaunt_coefficient_L1 (force_sub_sub_module.f90:64-387) for
+    L <= lmax, L1 <= lmax + 1.  Gauss-Legendre in cos(theta) x uniform phi,
+    exact for these polynomial degrees."""
+    L = lib()
+    mu, wmu = np.polynomial.legendre.leggauss(12)
+    nphi = 24
+    phi = 2.0 * np.pi * np.arange(nphi) / nphi
+    pts = []
+    for a, wa in zip(mu, wmu):
+        st = np.sqrt(1.0 - a * a)
+        for p in phi:
+            pts.append((st * np.cos(p), st * np.sin(p), a, wa * 2.0 * np.pi / nphi))
+    lm_all = [(l, m) for l in range(lmax + 3) for m in range(-l, l + 1)]
+    Y = {lm: np.array([L.oracle_ylm(x, y, z, lm[0], lm[1]) for x, y, z, _ in pts]) for lm in lm_all}
+    w = np.array([p[3] for p in pts])
+    G = np.zeros((3, lmax + 1, 2 * lmax + 1, lmax + 2, 2 * lmax + 3))
+    for k, q in enumerate((1, -1, 0)):
+        for l in range(lmax + 1):
+            for m in range(-l, l + 1):
+                for l1 in range(lmax + 2):
+                    for m1 in range(-l1, l1 + 1):
+                        G[k, l, m + lmax, l1, m1 + lmax + 1] = np.sum(w * Y[(l, m)] * Y[(1, q)] * Y[(l1, m1)])
+    return G
+
+
+def reference_duvdr(cell):
+    """duVdR (nnz, 3) of the cell's projectors by the reference's tabulated
+    path, aligned with ``cell.jjp``: per atom and l the radial function
+    viod(r) = sqrt(D) r^l exp(-r^2 / alpha) on rad1 = 0, dr, .., rc;
+    ps_nloc2_init_derivative's dviod tables (dpolint derivatives); per
+    periodic image of each sphere point the polint-interpolated
+    dviod(r) / r^2 contracted with Ylm and the coupling coefficients
+    (ps_nloc2_module.f90:1507-1586); images of one grid point summed, as
+    the force's JJ_MAP loop does (:1634-1645)."""
+    from rsdft_b200 import cell as C
+
+    Lb = lib()
+    n = cell.ngrid[0]
+    h = cell.h
+    nrc = int(round(C.PROJ_RC / RAD_DR)) + 1
+    rad = np.ascontiguousarray(np.arange(nrc) * RAD_DR)
+    G = gaunt_l1(1)
+    kp = int(np.ceil(C.PROJ_RC / h.min())) + 1
+    p1, p2, p3 = C._box_offsets(kp)
+    out = np.zeros((int(cell.lma_ptr[-1]), 3))
+    lma = 0
+    for ia in range(cell.natom):
+        R = cell.atoms[ia]
+        c0 = np.floor(R / h).astype(int)
+        u1, u2, u3 = c0[0] + p1, c0[1] + p2, c0[2] + p3
+        d = np.stack([u1 * h[0] - R[0], u2 * h[1] - R[1], u3 * h[2] - R[2]], axis=1)
+        r2 = np.einsum("ij,ij->i", d, d)
+        sel = r2 <= C.PROJ_RC ** 2 + 1e-10
+        d = np.ascontiguousarray(d[sel])
+        idx = np.mod(u1[sel], n) + n * (np.mod(u2[sel], n) + n * np.mod(u3[sel], n))
+        order = np.argsort(idx, kind="stable")
+        _, start = np.unique(idx[order], return_index=True)
+        for l in (0, 1):
+            viod = np.ascontiguousarray(np.sqrt(cell.dvals[ia, l]) * rad ** l * np.exp(-rad ** 2 / C.PROJ_ALPHA))
+            nj = 3 if l == 1 else 1
+            dv = np.zeros(nj * nrc)
+            if Lb.oracle_dviod(_p(rad), _p(viod), nrc, l, _p(dv)) != 0:
+                raise RuntimeError("oracle_dviod failed")
+            for m in (range(-1, 2) if l == 1 else (0,)):
+                while not (cell.amap[lma] == ia and cell.lmap[lma] == l and cell.mmap[lma] == m):
+                    raise RuntimeError(f"projector order differs at lma {lma}")
+                g = np.ascontiguousarray(G[:, l, m + 1, : l + 2, 1 - l: 1 - l + 2 * l + 3])
+                dd = np.zeros((len(d), 3))
+                if Lb.oracle_duvdr_ref(l, _p(d), len(d), _p(rad), nrc, _p(dv), _p(g), _p(dd)) != 0:
+                    raise RuntimeError("oracle_duvdr_ref: point below the radial grid")
+                merged = np.add.reduceat(dd[order], start, axis=0)
+                s0, e0 = cell.lma_ptr[lma], cell.lma_ptr[lma + 1]
+                if e0 - s0 != len(merged):
+                    raise RuntimeError(f"sphere of projector {lma} differs from the cell's")
+                out[s0:e0] = merged
+                lma += 1
+    return out
+
+
+# ---------------------------------------------------------------------------
+# calc_sweep's scalar steps
+def mp_ff0(n: int, x: np.ndarray) -> np.ndarray:
+    """ff0 (fermi_mp_module.f90:287-306): Methfessel-Paxton occupation of
+    order n (0.5 (1 - erf x) plus the Hermite series with factor(1) =
+    -1/(4 sqrt(pi)), factor(i) = -factor(i-1)/(4 i), :147-153); erf is
+    scipy's in place of the reference's bberf."""
+    from scipy.special import erf
+
+    x = np.asarray(x, dtype=np.float64)
+    ff0 = 0.5 * (1.0 - erf(x))
+    if n <= 0:
+        return ff0
+    fac = -1.0 / (4.0 * np.sqrt(np.pi))
+    hp0 = np.ones_like(x)
+    hp1 = 2.0 * x
+    ff = fac * hp1
+    for i in range(2, n + 1):
+        fac = -fac / (4.0 * i)
+        hp2 = 2.0 * x * hp1 - 2.0 * (2 * i - 3) * hp0
+        hp3 = 2.0 * x * hp2 - 2.0 * (2 * i - 2) * hp1
+        ff = ff + fac * hp3
+        hp0, hp1 = hp2, hp3
+    return ff0 + ff * np.exp(-x * x)
+
+
+def calc_fermi(esp: np.ndarray, nelectron: float, ekbt: float = 1e-5, kinteg: int = 5, nfixed: int = 0,
+               dspn: float = 0.0, it: int = 1):
+    """calc_fermi (fermi_mp_module.f90:95-284) for one Gamma point (wbz = 1),
+    all bands: esp (MB, MSP).  Bisection in the reference's loop order
+    (sequential sums over s, n).  Returns (occ (MB, MSP), efermi)."""
+    esp = np.asarray(esp, dtype=np.float64).reshape(esp.shape[0], -1)
+    mb, msp = esp.shape
+    occ = np.zeros_like(esp)
+
+    def bisect(cols, zne, w):
+        e = esp[:, cols]
+        ef1, ef2 = e.min(), e.max()
+        if ef1 == ef2:
+            ef1, ef2 = ef1 - 0.01, ef2 + 0.01
+        ef2 += min(ekbt * 1e2, 0.1)
+        ef0, ef, octmp = 1e10, 0.0, 0.0
+        for _ in range(1000):
+            ef = 0.5 * (ef1 + ef2)
+            if ef == ef0:
+                return ef, True
+            ff = mp_ff0(kinteg, (e - ef) / ekbt)
+            occ[:, cols] = ff
+            octmp = 0.0
+            for s in range(e.shape[1]):
+                for n in range(mb):
+                    octmp = octmp + ff[n, s] * w
+            if octmp - zne > 0.0:
+                ef2 = ef
+            elif octmp - zne < 0.0:
+                ef1 = ef
+            else:
+                return ef, True
+            ef0 = ef
+        return ef, abs(octmp - zne) <= 1e-10
+
+    if msp == 1 or it > nfixed:
+        ef, ok = bisect(list(range(msp)), nelectron, 2.0 / msp)
+    else:
+        ok = True
+        for s in range(msp):
+            ef, o = bisect([s], 0.5 * nelectron + (1 - 2 * s) * 0.5 * dspn, 1.0)
+            ok = ok and o
+    if not ok:
+        raise RuntimeError("EF IS NOT CONVERGED")
+    return 2.0 * occ / msp, ef
+
+
+def conv_check(esp, esp0, mb_ref: int, tol_esp: float):
+    """conv_check_2 (sweep_module.f90:255-266): max |esp - esp0| over bands
+    1..mb_ref of every spin, and whether it is below tol_esp."""
+    d = np.abs(np.asarray(esp) - np.asarray(esp0)).reshape(len(esp0) if np.ndim(esp0) == 1 else esp0.shape[0], -1)
+    m = float(d[:mb_ref].max())
+    return m, m < tol_esp

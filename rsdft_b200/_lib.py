@@ -43,6 +43,9 @@ SIGNATURES = {
     "rsdft_gpu_orth_subspace_diag": (_c_int, [_c_int, _c_int, _vp, _c_long, _c_int, _vp, _c_int]),
     "rsdft_gpu_eigensolver_sweep": (_c_int, [_c_int, _c_int, _vp, _c_long, _c_int, _vp, _vp, _c_int, _c_int,
                                              _c_int, _c_int]),
+    "rsdft_gpu_calc_sweep": (_c_int, [_vp, _c_long, _c_int, _c_int, _vp, _vp, _vp, _c_int, _c_int, _c_double, _c_int,
+                                      _c_double, _c_int, _c_double, _c_double, _c_int, _c_int, _c_int, _c_int, _c_int,
+                                      _vp, _vp, _vp]),
     "rsdft_gpu_esp_calc": (_c_int, [_c_int, _c_int, _vp, _c_int, _c_int, _c_int, _c_int, _vp]),
     "rsdft_gpu_residual": (_c_int, [_c_int, _c_int, _vp, _c_long, _c_int, _vp, _vp]),
     "rsdft_gpu_force_nloc": (_c_int, [_c_int, _vp, _c_long, _c_int, _vp, _vp]),

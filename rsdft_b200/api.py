@@ -16,6 +16,7 @@ replace (j-iwata/RSDFT v1.3.0, src/):
 ``calc_force_ps_nloc2(MI,force2,..)`` ps_nloc2_module.f90:1281
 ``hpsi_adjoint(psi, ...)``            (adjoint of op_localpot + op_ps_nloc2_hp)
 ``calc_density(unk, occ, rho)``      density_module.f90:115 (calc_density, NCPP)
+``calc_sweep(unk, esp, res, occ,..)``  sweep_module.f90:60 (calc_sweep's loop)
 ``write_wf(path, unk, ngrid, ...)``   io_write_module.f90:19 (simple_wf_io_write)
 ``read_wf(path, unk, ngrid, ...)``    io_read_module.f90:15 (simple_wf_io_read)
 ====================================  ==========================================
@@ -76,6 +77,13 @@ def fortran_empty(ml: int, nb: int, device="cuda", dtype=None):
     import torch
 
     return torch.empty((nb, ml), dtype=dtype or torch.float64, device=device).t()
+
+
+def fortran_copy(t):
+    """A new (ML, nb) column-major tensor holding the values of the
+    column-major tensor t.  (t.t().contiguous().t() is not a copy: t.t() is
+    already contiguous, so it returns t's own storage.)"""
+    return t.t().clone().t()
 
 
 def _ld(a) -> int:
@@ -235,6 +243,26 @@ class RsdftGpu:
     def subspace_rotv_sl(self, k, s, unk, vsub) -> None:
         _lib.call("rsdft_gpu_subspace_rotv", k, s, _ptr(unk, name="unk"), _ld(unk), unk.shape[1],
                   _ptr(vsub, name="vsub"), _ld(vsub))
+
+    def calc_sweep(self, unk, esp, res, occ, *, diter, nelectron, nspin=1, iconv_check=2, tol_esp=1e-7,
+                   mb_ref=None, nfixed=0, dspn=0.0, ekbt=1e-5, kinteg=5, ncg=4, mloop=3, ipc=4,
+                   mode=MODE_FP64) -> dict:
+        """calc_sweep (sweep_module.f90:60-226) on device-resident bands:
+        CG + GS + subspace per spin, calc_fermi, conv_check, up to diter
+        iterations.  unk is (ML, MB * nspin); esp / res / occ hold MB * nspin
+        values (esp: esp0 on entry).  Returns the iteration count, whether
+        conv_check passed and the Fermi level."""
+        import ctypes
+
+        mb = unk.shape[1] // nspin
+        it = ctypes.c_int(0)
+        cv = ctypes.c_int(0)
+        ef = ctypes.c_double(0.0)
+        _lib.call("rsdft_gpu_calc_sweep", _ptr(unk, name="unk"), _ld(unk), mb, nspin, _ptr(esp, name="esp"),
+                  _ptr(res, name="res"), _ptr(occ, name="occ"), diter, iconv_check, tol_esp,
+                  mb if mb_ref is None else mb_ref, float(nelectron), nfixed, dspn, ekbt, kinteg, ncg, mloop, ipc,
+                  mode, ctypes.addressof(it), ctypes.addressof(cv), ctypes.addressof(ef))
+        return {"iter": it.value, "converged": bool(cv.value), "efermi": ef.value}
 
     def esp_calc(self, k, s, wf, n1, n2, ns, ne, e) -> None:
         _lib.call("rsdft_gpu_esp_calc", k, s, _ptr(wf, name="wf"), n1, n2, ns, ne, _ptr(e, name="e"))

@@ -20,6 +20,7 @@
 
 #include "common.cuh"
 #include "kernels.cuh"
+#include "dmma.cuh"
 #include "mixed.cuh"
 
 namespace rsdft {
@@ -58,31 +59,12 @@ __global__ void k_reduce_partials(const double* __restrict__ P, int nch, int m, 
     C[(long)j * m + i] = alpha * s;
 }
 
-// C (m x n) = alpha A^T B with A, B tall (ML rows, leading dimension ld):
-// split-K over the grid in equal chunks (strided-batched DGEMM), partial
-// products reduced in a fixed order.  sym = 1 returns the symmetric part.
+// C (m x n) = alpha A^T B with A, B tall (ML rows, leading dimension ld) on
+// the FP64 tensor cores (dmma.cu): split-K over the grid, partial tiles
+// reduced in a fixed order.  sym = 1 returns the symmetric part.
 static int gemm_tn_splitk(const double* A, const double* B, long ld, int m, int n, double alpha, int sym,
                           double* C) {
-    Context& c = ctx();
-    const long ml = c.ml;
-    const int nch = (int)std::max<long>(1, std::min<long>(64, (ml + 8191) / 8192));
-    long kc = (ml + nch - 1) / nch;
-    kc = (kc + 7) / 8 * 8;
-    const int full = (int)(ml / kc);
-    const long rem = ml - (long)full * kc;
-    const int parts = full + (rem > 0 ? 1 : 0);
-    double* P = nullptr;
-    RS_CHECK(workspace_t("splitk_partials", (size_t)parts * m * n, &P));
-    const double one = 1.0, zero = 0.0;
-    if (full > 0)
-        RS_BLAS(cublasDgemmStridedBatched(c.blas, CUBLAS_OP_T, CUBLAS_OP_N, m, n, (int)kc, &one, A, (int)ld, kc, B,
-                                          (int)ld, kc, &zero, P, m, (long long)m * n, full));
-    if (rem > 0)
-        RS_BLAS(cublasDgemm(c.blas, CUBLAS_OP_T, CUBLAS_OP_N, m, n, (int)rem, &one, A + (long)full * kc, (int)ld,
-                            B + (long)full * kc, (int)ld, &zero, P + (long)full * m * n, m));
-    launch(k_reduce_partials, dim3(div_up(m, 128), n), 128, 0, c.stream, P, parts, m, n, alpha, sym, C);
-    RS_LAUNCH();
-    return RSDFT_OK;
+    return dmma_gram(A, B, ld, ctx().ml, m, n, alpha, sym, C, m);
 }
 
 static int check_info(int* dinfo, const char* what) {
@@ -101,7 +83,6 @@ static int check_info(int* dinfo, const char* what) {
 // product is one DGEMM (in and out are different buffers).
 static int cholqr_pass(const double* psi, double* out, long ld, int nb, double* S, int* dinfo, int mode) {
     Context& c = ctx();
-    const double zero = 0.0, one = 1.0;
     const void* split = nullptr;
     if (mode == RSDFT_MODE_FP64)
         RS_CHECK(gemm_tn_splitk(psi, psi, ld, nb, nb, c.dV, 0, S));
@@ -125,8 +106,7 @@ static int cholqr_pass(const double* psi, double* out, long ld, int nb, double* 
     launch(k_zero_lower, dim3(div_up(nb, 128), nb), 128, 0, c.stream, S, nb, nb);
     RS_LAUNCH();
     if (mode == RSDFT_MODE_FP64)
-        RS_BLAS(cublasDgemm(c.blas, CUBLAS_OP_N, CUBLAS_OP_N, (int)c.ml, nb, nb, &one, psi, (int)ld, S, nb, &zero, out,
-                            (int)ld));
+        RS_CHECK(dmma_gemm(false, c.ml, nb, nb, 1.0, psi, ld, S, nb, 0.0, out, ld));
     else
         RS_CHECK(rotate_mixed(psi, out, ld, nb, S, nb, mode_terms(mode), split));
     return RSDFT_OK;
@@ -167,14 +147,12 @@ int subspace_diag_device(double* psi, long ld, int mb, int spin, double* esp, in
     double *hpsi = nullptr, *H = nullptr;
     RS_CHECK(workspace_t("sub_hpsi", (size_t)ld * mb, &hpsi));
     RS_CHECK(workspace_t("sub_H", (size_t)mb * mb, &H));
-    const double zero = 0.0, one = 1.0;
     if (mode == RSDFT_MODE_FP64) {
         RS_CHECK(hpsi_device<double>(psi, hpsi, ld, mb, spin, nullptr));
         // Hsub = dV/2 (psi^T H psi + (H psi)^T psi): the symmetric part of dV psi^T (H psi)
         RS_CHECK(gemm_tn_splitk(psi, hpsi, ld, mb, mb, c.dV, 1, H));
         RS_CHECK(syevd(H, mb, esp, CUBLAS_FILL_MODE_UPPER, "subspace_diag: syevd"));
-        RS_BLAS(cublasDgemm(c.blas, CUBLAS_OP_N, CUBLAS_OP_N, (int)c.ml, mb, mb, &one, psi, (int)ld, H, mb, &zero,
-                            hpsi, (int)ld));
+        RS_CHECK(dmma_gemm(false, c.ml, mb, mb, 1.0, psi, ld, H, mb, 0.0, hpsi, ld));
     } else {
         RS_CHECK(hpsi_device<double>(psi, hpsi, ld, mb, spin, nullptr));
         const void* split = nullptr;
@@ -246,7 +224,6 @@ int orth_subspace_diag_device(double* psi, long ld, int mb, int spin, double* es
     RS_CHECK(workspace_t("osd_T", (size_t)mb * mb, &T));
     RS_CHECK(workspace_t("osd_minmax", 2, &mm));
     RS_CHECK(workspace_t("gs_info", 4, &dinfo));
-    const double zero = 0.0, one = 1.0;
     const void* split = nullptr;
     RS_CHECK(hpsi_device<double>(psi, hpsi, ld, mb, spin, nullptr));
     if (mode == RSDFT_MODE_FP64) {
@@ -282,13 +259,12 @@ int orth_subspace_diag_device(double* psi, long ld, int mb, int spin, double* es
     launch(k_zero_lower, dim3(div_up(mb, 128), mb), 128, 0, c.stream, S, mb, mb);
     RS_LAUNCH();
     // Hr = R^-T H R^-1 (T = H R^-1, then H = R^-T T), eigenpairs, T = R^-1 V
-    RS_BLAS(cublasDgemm(c.blas, CUBLAS_OP_N, CUBLAS_OP_N, mb, mb, mb, &one, H, mb, S, mb, &zero, T, mb));
-    RS_BLAS(cublasDgemm(c.blas, CUBLAS_OP_T, CUBLAS_OP_N, mb, mb, mb, &one, S, mb, T, mb, &zero, H, mb));
+    RS_CHECK(dmma_gemm(false, mb, mb, mb, 1.0, H, mb, S, mb, 0.0, T, mb));
+    RS_CHECK(dmma_gemm(true, mb, mb, mb, 1.0, S, mb, T, mb, 0.0, H, mb));
     RS_CHECK(syevd(H, mb, esp, CUBLAS_FILL_MODE_UPPER, "orth_subspace_diag: syevd"));
-    RS_BLAS(cublasDgemm(c.blas, CUBLAS_OP_N, CUBLAS_OP_N, mb, mb, mb, &one, S, mb, H, mb, &zero, T, mb));
+    RS_CHECK(dmma_gemm(false, mb, mb, mb, 1.0, S, mb, H, mb, 0.0, T, mb));
     if (mode == RSDFT_MODE_FP64) {
-        RS_BLAS(cublasDgemm(c.blas, CUBLAS_OP_N, CUBLAS_OP_N, (int)c.ml, mb, mb, &one, psi, (int)ld, T, mb, &zero,
-                            hpsi, (int)ld));
+        RS_CHECK(dmma_gemm(false, c.ml, mb, mb, 1.0, psi, ld, T, mb, 0.0, hpsi, ld));
         RS_CUDA(cudaMemcpy2DAsync(psi, ld * sizeof(double), hpsi, ld * sizeof(double), c.ml * sizeof(double), mb,
                                   cudaMemcpyDeviceToDevice, c.stream));
     } else {
@@ -313,7 +289,6 @@ int orth_subspace_diag_f32(const float* x32, const float* hx, double* psi, long 
     RS_CHECK(workspace_t("osd_T", (size_t)mb * mb, &T));
     RS_CHECK(workspace_t("osd_minmax", 2, &mm));
     RS_CHECK(workspace_t("gs_info", 4, &dinfo));
-    const double zero = 0.0, one = 1.0;
     if (hx) {
         h32 = const_cast<float*>(hx);
     } else {
@@ -350,11 +325,26 @@ int orth_subspace_diag_f32(const float* x32, const float* hx, double* psi, long 
     RS_CHECK(check_info(dinfo, "eigensolver_sweep: triangular inverse"));
     launch(k_zero_lower, dim3(div_up(mb, 128), mb), 128, 0, c.stream, S, mb, mb);
     RS_LAUNCH();
-    RS_BLAS(cublasDgemm(c.blas, CUBLAS_OP_N, CUBLAS_OP_N, mb, mb, mb, &one, H, mb, S, mb, &zero, T, mb));
-    RS_BLAS(cublasDgemm(c.blas, CUBLAS_OP_T, CUBLAS_OP_N, mb, mb, mb, &one, S, mb, T, mb, &zero, H, mb));
+    RS_CHECK(dmma_gemm(false, mb, mb, mb, 1.0, H, mb, S, mb, 0.0, T, mb));
+    RS_CHECK(dmma_gemm(true, mb, mb, mb, 1.0, S, mb, T, mb, 0.0, H, mb));
     RS_CHECK(syevd(H, mb, esp, CUBLAS_FILL_MODE_UPPER, "eigensolver_sweep: syevd"));
-    RS_BLAS(cublasDgemm(c.blas, CUBLAS_OP_N, CUBLAS_OP_N, mb, mb, mb, &one, S, mb, H, mb, &zero, T, mb));
+    RS_CHECK(dmma_gemm(false, mb, mb, mb, 1.0, S, mb, H, mb, 0.0, T, mb));
     return rotate_mixed(x32, psi, ld, mb, T, mb, mode_terms(mode), split);
+}
+
+}  // namespace rsdft
+
+namespace rsdft {
+
+int sweep_device(double* d, long ld, int mb, int s, double* W, double* R, int ncg, int mloop, int ipc, int mode) {
+    if (mode == RSDFT_MODE_FP64) {
+        RS_CHECK(cg_device(d, ld, mb, s, W, R, ncg, mloop, ipc, mode));
+        return orth_subspace_diag_device(d, ld, mb, s, W, mode);
+    }
+    float* x32 = nullptr;
+    const float* hx = nullptr;
+    RS_CHECK(cg_device_f32(d, ld, mb, s, W, R, ncg, mloop, ipc, &x32, &hx));
+    return orth_subspace_diag_f32(x32, hx, d, ld, mb, s, W, mode);
 }
 
 }  // namespace rsdft
@@ -465,9 +455,7 @@ int rsdft_gpu_subspace_rotv(int k, int s, double* unk, long ld, int mb, const do
     RS_CHECK(workspace_t("sub_hpsi", (size_t)ld * mb, &tmp));
     RS_CUDA(cudaMemcpy2DAsync(V, (size_t)mb * sizeof(double), vsub, (size_t)ldv * sizeof(double),
                               (size_t)mb * sizeof(double), mb, cudaMemcpyDefault, c.stream));
-    const double zero = 0.0, one = 1.0;
-    RS_BLAS(cublasDgemm(c.blas, CUBLAS_OP_N, CUBLAS_OP_N, (int)c.ml, mb, mb, &one, d, (int)ld, V, mb, &zero, tmp,
-                        (int)ld));
+    RS_CHECK(dmma_gemm(false, c.ml, mb, mb, 1.0, d, ld, V, mb, 0.0, tmp, ld));
     RS_CUDA(cudaMemcpy2DAsync(d, ld * sizeof(double), tmp, ld * sizeof(double), c.ml * sizeof(double), mb,
                               cudaMemcpyDeviceToDevice, c.stream));
     RS_CHECK(wf_release(unk, d, ld, mb, st));
@@ -496,17 +484,13 @@ int rsdft_gpu_eigensolver_sweep(int k, int s, double* unk, long ld, int mb, doub
     if (st && overlap) RS_CUDA(cudaStreamSynchronize(c.stream));
     RS_CHECK(workspace_t("sweep_W", (size_t)mb, &W));
     RS_CHECK(workspace_t("sweep_R", (size_t)mb, &R));
-    if (mode == RSDFT_MODE_FP64) {
-        RS_CHECK(cg_device(d, ld, mb, s, W, R, ncg, mloop, ipc, mode));
-        RS_CHECK(orth_subspace_diag_device(d, ld, mb, s, W, mode));
-    } else {
+    if (st && overlap) {
         float* x32 = nullptr;
         const float* hx = nullptr;
-        if (st && overlap)
-            RS_CHECK(cg_device_f32_staged(unk, d, ld, mb, s, W, R, ncg, mloop, ipc, nchunk, &x32, &hx));
-        else
-            RS_CHECK(cg_device_f32(d, ld, mb, s, W, R, ncg, mloop, ipc, &x32, &hx));
+        RS_CHECK(cg_device_f32_staged(unk, d, ld, mb, s, W, R, ncg, mloop, ipc, nchunk, &x32, &hx));
         RS_CHECK(orth_subspace_diag_f32(x32, hx, d, ld, mb, s, W, mode));
+    } else {
+        RS_CHECK(sweep_device(d, ld, mb, s, W, R, ncg, mloop, ipc, mode));
     }
     RS_CHECK(stage_out(esp, W, sizeof(double) * mb));
     RS_CHECK(stage_out(res, R, sizeof(double) * mb));

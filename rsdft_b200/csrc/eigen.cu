@@ -37,6 +37,7 @@
 #include <cfloat>
 
 #include "common.cuh"
+#include "dmma.cuh"
 #include "kernels.cuh"
 #include "tma.cuh"
 
@@ -750,9 +751,9 @@ int syevd_fast(double* A, int n, double* W, cublasFillMode_t uplo) {
         double* src = A;
         double* dst = Z2;
         for (int it = 0; it < 2; ++it) {
-            RS_BLAS(cublasDgemm(c.blas, CUBLAS_OP_T, CUBLAS_OP_N, n, n, n, &one, src, n, src, n, &zero, G, n));
+            RS_CHECK(dmma_gemm(true, n, n, n, one, src, n, src, n, zero, G, n));
             RS_CUDA(cudaMemcpyAsync(dst, src, sizeof(double) * (size_t)n * n, cudaMemcpyDeviceToDevice, c.stream));
-            RS_BLAS(cublasDgemm(c.blas, CUBLAS_OP_N, CUBLAS_OP_N, n, n, n, &half, src, n, G, n, &c15, dst, n));
+            RS_CHECK(dmma_gemm(false, n, n, n, half, src, n, G, n, c15, dst, n));
             double* t = src;
             src = dst;
             dst = t;

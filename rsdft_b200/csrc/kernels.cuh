@@ -62,6 +62,11 @@ int subspace_diag_device(double* psi, long ld, int mb, int spin, double* esp_dev
 // Gram-Schmidt + Rayleigh-Ritz as one step (device data).
 int orth_subspace_diag_device(double* psi, long ld, int mb, int spin, double* esp_dev, int mode);
 
+// One calc_sweep step for spin `spin` on device bands: conjugate_gradient,
+// then gram_schmidt + subspace_diag as one Rayleigh-Ritz step; W, R receive
+// the Ritz values and CG residuals (device, mb each).
+int sweep_device(double* d, long ld, int mb, int spin, double* W, double* R, int ncg, int mloop, int ipc, int mode);
+
 // Mixed forms: the CG sweep on an FP32 copy of unk, left in the workspace
 // (*x32_out, leading dimension ld) for orth_subspace_diag_f32.  hx_out (if
 // given) receives the sweep's H x32 (in the CG workspace), or null when an

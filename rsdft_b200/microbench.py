@@ -91,7 +91,7 @@ def run_hpsi(args) -> dict:
 def run_iteration(args) -> dict:
     torch, api, g, cell, st, psi = _setup(args.workload, args.ngrid, args.bands)
     MB = cell.nband
-    u = psi.t().contiguous().t()
+    u = api.fortran_copy(psi)
     g.gram_schmidt(1, MB, 1, 1, u)
     esp = torch.zeros(MB, dtype=torch.float64, device="cuda")
     res = torch.zeros_like(esp)
@@ -105,7 +105,7 @@ def run_iteration(args) -> dict:
 def run_rr(args) -> dict:
     torch, api, g, cell, st, psi = _setup(args.workload, args.ngrid, args.bands)
     MB = cell.nband
-    u = psi.t().contiguous().t()
+    u = api.fortran_copy(psi)
     g.gram_schmidt(1, MB, 1, 1, u)
     esp = torch.zeros(MB, dtype=torch.float64, device="cuda")
     mode = MODES[args.mode]
@@ -121,14 +121,14 @@ def run_large(args) -> dict:
     mixed vs FP64, hpsi bandwidth on all bands."""
     torch, api, g, cell, st, psi = _setup(args.workload)
     MB, ML = cell.nband, cell.ML
-    start = psi.t().contiguous().t()
+    start = api.fortran_copy(psi)
     g.gram_schmidt(1, MB, 1, 1, start)
     occ = np.zeros(MB)
     occ[: cell.nocc] = 2.0
     out = {"what": "large", "workload": args.workload, "grid": list(cell.ngrid), "bands": MB, "steps": args.steps}
     res = {}
     for name, mode in (("fp64", 0), ("mixed-bf16x3", 1)):
-        u = start.t().contiguous().t()
+        u = api.fortran_copy(start)
         esp = torch.zeros(MB, dtype=torch.float64, device="cuda")
         r = torch.zeros_like(esp)
         times = []

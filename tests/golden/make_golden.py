@@ -5,12 +5,18 @@
    the reference's committed run log examples/Si216/a.log:249-273 (and
    coef_lap0 from the same block).  This is the reference's own known-answer
    output for the hot path's set-up.
-2. ``oracle_si8_g12.npz``: sampled outputs of the oracle (hpsi, one CG sweep,
+2. ``gaunt_l1.json``: the coupling coefficients of the force's derivative
+   table for projector angular momenta L = 0 and 1 -- the entries
+   Y1/Y2/Y3(L, m, L1, L1z) that get_gaunt_coefficient_L1 assigns
+   (force_sub_sub_module.f90:64-387), read from that source file as text.
+3. ``oracle_si8_g12.npz``: sampled outputs of the oracle (hpsi, one CG sweep,
    Gram-Schmidt, subspace diagonalisation, nonlocal force) on the seeded
    12^3 cell, so that later edits of the oracle cannot drift unnoticed.
 
-Run from the repository root: ``python tests/golden/make_golden.py``.  Step 1
-needs the reference tree (REFERENCE env var, default /root/reference).
+Run from the repository root:
+``python tests/golden/make_golden.py --reference <path of the RSDFT tree>``
+writes all three; ``--oracle-only`` rewrites only the oracle fixture (no
+reference tree needed).
 """
 from __future__ import annotations
 
@@ -56,6 +62,22 @@ def fd_kat(reference: str) -> dict:
     }
 
 
+def gaunt_l1(reference: str, lmax: int = 1) -> dict:
+    """Y1/Y2/Y3(L, m, L1, L1z) entries with L <= lmax, as assigned in
+    get_gaunt_coefficient_L1 (values printed with 15 decimals)."""
+    path = os.path.join(reference, "src", "force_sub_sub_module.f90")
+    src = open(path).read()
+    body = src[src.index("SUBROUTINE get_gaunt_coefficient_L1"):src.index("END SUBROUTINE get_gaunt_coefficient_L1")]
+    pat = re.compile(r"(Y[123])\(\s*(-?\d+)\s*,\s*(-?\d+)\s*,\s*(-?\d+)\s*,\s*(-?\d+)\s*\)\s*=\s*([-+.\dEeDd]+)")
+    out = {"Y1": [], "Y2": [], "Y3": []}
+    for m in pat.finditer(body):
+        name, L, mm, L1, L1z, v = m.groups()
+        if int(L) <= lmax:
+            out[name].append([int(L), int(mm), int(L1), int(L1z), float(v.lower().replace("d", "e"))])
+    return {"source": "force_sub_sub_module.f90:64-387 (get_gaunt_coefficient_L1), entries with L <= %d" % lmax,
+            "note": "Y1, Y2, Y3 couple through the l = 1 harmonics of m = 1, -1, 0 (x, y, z)", **out}
+
+
 def oracle_fixture() -> dict:
     from oracle import oracle as O
     from rsdft_b200.cell import build_cell
@@ -84,10 +106,19 @@ def oracle_fixture() -> dict:
 
 
 if __name__ == "__main__":
-    ref = os.environ.get("REFERENCE", "/root/reference")
-    if os.path.isdir(ref):
+    import argparse
+
+    ap = argparse.ArgumentParser()
+    g = ap.add_mutually_exclusive_group(required=True)
+    g.add_argument("--reference", help="root of the RSDFT source tree (read-only)")
+    g.add_argument("--oracle-only", action="store_true")
+    args = ap.parse_args()
+    if args.reference:
         with open(os.path.join(HERE, "fd_kat_si216.json"), "w") as fh:
-            json.dump(fd_kat(ref), fh, indent=1)
+            json.dump(fd_kat(args.reference), fh, indent=1)
         print("wrote fd_kat_si216.json")
+        with open(os.path.join(HERE, "gaunt_l1.json"), "w") as fh:
+            json.dump(gaunt_l1(args.reference), fh, indent=1)
+        print("wrote gaunt_l1.json")
     np.savez_compressed(os.path.join(HERE, "oracle_si8_g12.npz"), **oracle_fixture())
     print("wrote oracle_si8_g12.npz")

@@ -156,3 +156,22 @@ def test_hellmann_feynman_reconverged(gpu, converged):
         gpu.setup(c)
     fd = (E[0] - E[1]) / (2 * h)
     assert abs(dr[ia, k] - fd) <= FD_TOL, (dr[ia, k], fd)
+
+
+def test_force_vs_reference_tabulated_path(gpu, converged):
+    """The GPU force (analytic projector derivative) against the oracle's
+    restatement of the reference's own force_ps_nloc2 arithmetic
+    (dpolint-tabulated, polint-interpolated duVdR with Gaunt coupling,
+    ps_nloc2_module.f90:1489-1586) on the converged FP64 bands of the
+    differentiation workload: equal within the reference table's own
+    truncation error, far inside the 1e-5 Ha/bohr finite-difference target."""
+    from oracle import oracle as O
+
+    c, o, (u64, _, _), _ = converged
+    occ = occupations(c)
+    f = np.zeros((3, c.natom), order="F")
+    gpu.calc_force_ps_nloc2(c.natom, f, u64, occ)
+    f_gpu = f.T
+    f_ref = O.Oracle(c).force_nloc_with(host(u64), occ, O.reference_duvdr(c))
+    err = np.abs(f_gpu - f_ref).max()
+    assert err <= 1e-7 + 1e-4 * np.abs(f_ref).max(), err

@@ -99,8 +99,8 @@ def test_mixed_gate_si216_unconverged(gpu, cells):
     assert float(res[: c.nocc].max()) > 1e-6
     # the bands after a further CG sweep, not yet orthonormal
     gpu.conjugate_gradient(1, c.ML, c.nband, 1, 1, u, esp, res, ncg=4, mloop=3)
-    ua = u.t().contiguous().t()
-    ub = u.t().contiguous().t()
+    ua = api.fortran_copy(u)
+    ub = api.fortran_copy(u)
     ea = torch.zeros_like(esp)
     eb = torch.zeros_like(esp)
     gpu.orth_subspace_diag(1, 1, ua, ea, mode=api.MODE_FP64)

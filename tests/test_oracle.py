@@ -167,3 +167,23 @@ def test_golden_oracle_regression():
     assert np.allclose(w, g["sub_esp"], rtol=1e-11, atol=1e-12)
     f = o.force_nloc(u3, c.occupations())
     assert np.allclose(f, g["force"], rtol=1e-8, atol=1e-10)
+
+
+def test_calc_fermi_restatement():
+    """calc_fermi (fermi_mp_module.f90:95-284): the electron count is matched,
+    occupations lie in [0, 2] (up to the Methfessel-Paxton overshoot, which
+    vanishes for well separated levels), degenerate levels share equally,
+    and the fixed-moment branch fills each spin to its own count."""
+    rng = np.random.default_rng(7)
+    e = np.sort(rng.uniform(-0.5, 0.8, 40))
+    e[19] = e[20]  # a degenerate pair at the Fermi level: 19 + 1 of 2 levels filled
+    occ, ef = O.calc_fermi(e, 40.0)
+    assert abs(occ.sum() - 40.0) <= 1e-10
+    assert occ[19, 0] == occ[20, 0] and abs(occ[19, 0] - 1.0) <= 1e-12
+    assert np.all(occ[:19] > 2.0 - 1e-12) and np.all(occ[21:] < 1e-12)
+    assert e[18] < ef < e[21]
+    e2 = np.stack([e, e + 0.05], axis=1)
+    occ2, _ = O.calc_fermi(e2, 40.0, nfixed=5, dspn=2.0, it=1)
+    assert abs(occ2[:, 0].sum() - 21.0) <= 1e-10 and abs(occ2[:, 1].sum() - 19.0) <= 1e-10
+    occ3, _ = O.calc_fermi(e2, 40.0, nfixed=5, dspn=2.0, it=6)  # past nfixed: one common level
+    assert abs(occ3.sum() - 40.0) <= 1e-10
