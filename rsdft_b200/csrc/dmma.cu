@@ -53,6 +53,11 @@ __device__ __forceinline__ void cp_async8(double* dst, const double* src, bool v
     const int n = valid ? 8 : 0;  // 0 source bytes: the 8 destination bytes are zero-filled
     asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;" ::"r"(d), "l"(src), "r"(n) : "memory");
 }
+__device__ __forceinline__ void cp_async16(double* dst, const double* src, bool valid) {
+    const uint32_t d = (uint32_t)__cvta_generic_to_shared(dst);
+    const int n = valid ? 16 : 0;
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;" ::"r"(d), "l"(src), "r"(n) : "memory");
+}
 __device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
 template <int N>
 __device__ __forceinline__ void cp_async_wait() {
@@ -81,8 +86,8 @@ __device__ __forceinline__ void tile_of(const DmmaArgs& g, int t, int& tm, int& 
     tm = t;
 }
 
-template <int BM, int BN, int WM, int WN, bool KMAJOR>
-__global__ void __launch_bounds__(32 * WM * WN, 1) k_dmma(DmmaArgs g) {
+template <int BM, int BN, int WM, int WN, bool KMAJOR, bool VEC, int CPS>
+__global__ void __launch_bounds__(32 * WM * WN, CPS) k_dmma(DmmaArgs g) {
     constexpr int BK = DM_BK, NS = DM_NS, NT = 32 * WM * WN;
     constexpr int SA = BK + 4;
     constexpr int SB = KMAJOR ? BK + 4 : BN + 8;
@@ -103,29 +108,39 @@ __global__ void __launch_bounds__(32 * WM * WN, 1) k_dmma(DmmaArgs g) {
     const long k1 = min(g.K, k0 + g.kchunk);
     const int nkb = k1 > k0 ? (int)((k1 - k0 + BK - 1) / BK) : 0;
 
+    // operand tiles: 8-byte copies, or 16-byte ones (pairs of doubles along
+    // the contiguous dimension) when every row start is 16-byte aligned and
+    // the pair is wholly inside or outside the valid range (K, M, N even)
     auto load_stage = [&](int s, int kb) {
         const long kb0 = k0 + (long)kb * BK;
         double* as = As + s * AST;
-        for (int e = threadIdx.x; e < BM * BK; e += NT) {
-            const int r = e / BK, kk = e % BK;
+        constexpr int V = VEC ? 2 : 1;
+        for (int e = threadIdx.x; e < BM * BK / V; e += NT) {
+            const int r = e / (BK / V), kk = (e % (BK / V)) * V;
             const long k = kb0 + kk;
             const bool ok = m0 + r < g.M && k < k1;
-            cp_async8(as + r * SA + kk, ok ? g.A + (long)(m0 + r) * g.lda + k : g.A, ok);
+            const double* src = ok ? g.A + (long)(m0 + r) * g.lda + k : g.A;
+            if (VEC) cp_async16(as + r * SA + kk, src, ok);
+            else cp_async8(as + r * SA + kk, src, ok);
         }
         double* bs = Bs + s * BST;
         if (KMAJOR) {
-            for (int e = threadIdx.x; e < BN * BK; e += NT) {
-                const int r = e / BK, kk = e % BK;
+            for (int e = threadIdx.x; e < BN * BK / V; e += NT) {
+                const int r = e / (BK / V), kk = (e % (BK / V)) * V;
                 const long k = kb0 + kk;
                 const bool ok = n0 + r < g.N && k < k1;
-                cp_async8(bs + r * SB + kk, ok ? g.B + k + (long)(n0 + r) * g.ldb : g.B, ok);
+                const double* src = ok ? g.B + k + (long)(n0 + r) * g.ldb : g.B;
+                if (VEC) cp_async16(bs + r * SB + kk, src, ok);
+                else cp_async8(bs + r * SB + kk, src, ok);
             }
         } else {
-            for (int e = threadIdx.x; e < BN * BK; e += NT) {
-                const int kk = e / BN, c = e % BN;
+            for (int e = threadIdx.x; e < BN * BK / V; e += NT) {
+                const int kk = e / (BN / V), c = (e % (BN / V)) * V;
                 const long k = kb0 + kk;
                 const bool ok = n0 + c < g.N && k < k1;
-                cp_async8(bs + kk * SB + c, ok ? g.B + k * g.ldb + (n0 + c) : g.B, ok);
+                const double* src = ok ? g.B + k * g.ldb + (n0 + c) : g.B;
+                if (VEC) cp_async16(bs + kk * SB + c, src, ok);
+                else cp_async8(bs + kk * SB + c, src, ok);
             }
         }
     };
@@ -175,19 +190,33 @@ __global__ void __launch_bounds__(32 * WM * WN, 1) k_dmma(DmmaArgs g) {
             }
         return;
     }
+    const bool pair = g.ldcn == 1 && (g.ldcm % 2) == 0 && (reinterpret_cast<uintptr_t>(g.C) % 16) == 0;
 #pragma unroll
     for (int i = 0; i < TM; ++i)
 #pragma unroll
-        for (int j = 0; j < TN; ++j)
+        for (int j = 0; j < TN; ++j) {
+            const int m = m0 + wm0 + 8 * i + fr, n = n0 + wn0 + 8 * j + 2 * fc;
+            if (m >= g.M) continue;
+            double* o = g.C + (long)m * g.ldcm + (long)n * g.ldcn;
+            if (pair && n + 1 < g.N) {
+                double2 v = make_double2(g.alpha * acc[i][j][0], g.alpha * acc[i][j][1]);
+                if (g.beta != 0.0) {
+                    const double2 old = *reinterpret_cast<const double2*>(o);
+                    v.x = fma(g.beta, old.x, v.x);
+                    v.y = fma(g.beta, old.y, v.y);
+                }
+                *reinterpret_cast<double2*>(o) = v;
+                continue;
+            }
 #pragma unroll
             for (int e = 0; e < 2; ++e) {
-                const int m = m0 + wm0 + 8 * i + fr, n = n0 + wn0 + 8 * j + 2 * fc + e;
-                if (m < g.M && n < g.N) {
-                    double* o = g.C + (long)m * g.ldcm + (long)n * g.ldcn;
+                if (n + e < g.N) {
+                    double* oe = o + (long)e * g.ldcn;
                     const double v = g.alpha * acc[i][j][e];
-                    *o = g.beta == 0.0 ? v : fma(g.beta, *o, v);
+                    *oe = g.beta == 0.0 ? v : fma(g.beta, *oe, v);
                 }
             }
+        }
 }
 
 // C(i, j) = alpha * sum over splits (fixed order) of the raw tile sums;
@@ -219,15 +248,30 @@ __global__ void k_dmma_reduce(const double* __restrict__ P, int nsplit, int ntil
     C[(long)j * ldc + i] = alpha * v;
 }
 
-template <int BM, int BN, int WM, int WN, bool KMAJOR>
-int launch_dmma(const DmmaArgs& g, int nsplit) {
+template <int BM, int BN, int WM, int WN, bool KMAJOR, int CPS>
+int launch_dmma(const DmmaArgs& g, int nsplit, bool vec) {
     constexpr int SA = DM_BK + 4;
     constexpr int SB = KMAJOR ? DM_BK + 4 : BN + 8;
     constexpr size_t smem = (size_t)DM_NS * (BM * SA + (KMAJOR ? BN * SB : DM_BK * SB)) * sizeof(double);
-    RS_CHECK(set_smem_optin((const void*)k_dmma<BM, BN, WM, WN, KMAJOR>, (int)smem));
-    launch(k_dmma<BM, BN, WM, WN, KMAJOR>, dim3(g.ntiles, nsplit), 32 * WM * WN, smem, ctx().stream, g);
+    const void* fn = vec ? (const void*)k_dmma<BM, BN, WM, WN, KMAJOR, true, CPS>
+                         : (const void*)k_dmma<BM, BN, WM, WN, KMAJOR, false, CPS>;
+    RS_CHECK(set_smem_optin(fn, (int)smem));
+    if (vec)
+        launch(k_dmma<BM, BN, WM, WN, KMAJOR, true, CPS>, dim3(g.ntiles, nsplit), 32 * WM * WN, smem, ctx().stream, g);
+    else
+        launch(k_dmma<BM, BN, WM, WN, KMAJOR, false, CPS>, dim3(g.ntiles, nsplit), 32 * WM * WN, smem, ctx().stream,
+               g);
     RS_LAUNCH();
     return RSDFT_OK;
+}
+
+// 16-byte operand copies are exact when both operands' bases and leading
+// dimensions keep every row start 16-byte aligned and the K, M, N limits
+// are even (a pair of doubles is then wholly valid or wholly out of range)
+bool vec_ok(const DmmaArgs& g) {
+    auto al = [](const void* p) { return (reinterpret_cast<uintptr_t>(p) % 16) == 0; };
+    return al(g.A) && al(g.B) && g.lda % 2 == 0 && g.ldb % 2 == 0 && g.K % 2 == 0 && g.M % 2 == 0 && g.N % 2 == 0 &&
+           g.kchunk % 2 == 0;
 }
 
 }  // namespace
@@ -260,7 +304,7 @@ int dmma_gram(const double* A, const double* B, long ld, long kdim, int m, int n
     double* P = nullptr;
     RS_CHECK(workspace_t("dmma_partials", (size_t)nsplit * g.ntiles * BM * BN, &P));
     g.partial = P;
-    RS_CHECK((launch_dmma<BM, BN, 4, 4, true>(g, nsplit)));
+    RS_CHECK((launch_dmma<BM, BN, 4, 4, true, 1>(g, nsplit, vec_ok(g))));
     launch(k_dmma_reduce<BM, BN>, dim3(div_up(m, 128), n), 128, 0, c.stream, (const double*)P, nsplit, g.ntiles,
            g.ntm, g.sym, m, alpha, symmetrize, C, ldc);
     RS_LAUNCH();
@@ -292,20 +336,21 @@ int dmma_gemm(bool transA, long m, int n, int k, double alpha, const double* A, 
         return RSDFT_EINVAL;
     }
     g.N = (int)m;
+    const bool vec = vec_ok(g);
     if (m >= 4096) {
-        // tall output (a rotation psi V): 128 bands x 128 grid points per CTA,
-        // sixteen warps of 32 x 32 (four per SM sub-partition keep the DMMA
-        // pipe busy through the fixed-latency stalls of each warp)
-        constexpr int BM = 128, BN = 128;
+        // tall output (a rotation psi V): 128 bands x 64 grid points per
+        // CTA, eight warps of 32 x 32, two CTAs per SM so that one CTA's
+        // operand prologue and store epilogue overlap the other's MMAs
+        constexpr int BM = 128, BN = 64;
         g.ntm = div_up(n, BM);
         g.ntiles = g.ntm * div_up(m, BN);
-        return transA ? launch_dmma<BM, BN, 4, 4, true>(g, 1) : launch_dmma<BM, BN, 4, 4, false>(g, 1);
+        return transA ? launch_dmma<BM, BN, 4, 2, true, 2>(g, 1, vec) : launch_dmma<BM, BN, 4, 2, false, 2>(g, 1, vec);
     }
     // small dense products: 32 x 32 tiles, four warps
     constexpr int BM = 32, BN = 32;
     g.ntm = div_up(n, BM);
     g.ntiles = g.ntm * div_up(m, BN);
-    return transA ? launch_dmma<BM, BN, 2, 2, true>(g, 1) : launch_dmma<BM, BN, 2, 2, false>(g, 1);
+    return transA ? launch_dmma<BM, BN, 2, 2, true, 4>(g, 1, vec) : launch_dmma<BM, BN, 2, 2, false, 4>(g, 1, vec);
 }
 
 }  // namespace rsdft

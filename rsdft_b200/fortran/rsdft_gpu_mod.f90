@@ -11,6 +11,7 @@
 ! gpu_subspace_mate_sl          subspace_mate_sl       subspace_mate_sl_module.f90:27
 ! gpu_subspace_solv_sl          subspace_solv_sl       subspace_solv_sl_module.f90:15
 ! gpu_subspace_rotv_sl          subspace_rotv_sl       subspace_rotv_sl_module.f90:24
+! gpu_calc_sweep                calc_sweep (loop)      sweep_module.f90:60
 ! gpu_esp_calc                  esp_calc               esp_calc_module.f90:15
 ! gpu_calc_force_ps_nloc2       calc_force_ps_nloc2    ps_nloc2_module.f90:1281
 ! gpu_calc_density              calc_density (NCPP)    density_module.f90:115
@@ -31,7 +32,7 @@ MODULE rsdft_gpu_mod
   PUBLIC :: gpu_init, gpu_setup_grid, gpu_setup_vloc, gpu_setup_nonlocal, gpu_register_wf, gpu_sync_to_host, &
             gpu_sync_to_device, gpu_hamiltonian, gpu_conjugate_gradient, gpu_gram_schmidt, gpu_subspace_diag, &
             gpu_subspace_mate_sl, gpu_subspace_solv_sl, gpu_subspace_rotv_sl, gpu_esp_calc, gpu_calc_force_ps_nloc2, &
-            gpu_calc_density, gpu_wf_io_write, gpu_wf_io_read
+            gpu_calc_density, gpu_wf_io_write, gpu_wf_io_read, gpu_calc_sweep
 
   integer(c_int), parameter, PUBLIC :: RSDFT_MODE_FP64 = 0, RSDFT_MODE_MIXED_BF16X3 = 1, &
                                        RSDFT_MODE_MIXED_TF32 = 2, RSDFT_MODE_MIXED_BF16X2 = 3
@@ -117,6 +118,15 @@ MODULE rsdft_gpu_mod
        type(c_ptr), value :: unk, esp, res
        integer(c_long), value :: ld
      end function rsdft_gpu_eigensolver_sweep
+     integer(c_int) function rsdft_gpu_calc_sweep(unk, ld, mb, nspin, esp, res, occ, diter, iconv_check, tol_esp, &
+          mb_ref, nelectron, nfixed, dspn, ekbt, kinteg, ncg, mloop, ipc, mode, iter_out, conv_out, efermi) &
+          bind(C, name="rsdft_gpu_calc_sweep")
+       import :: c_int, c_long, c_double, c_ptr
+       type(c_ptr), value :: unk, esp, res, occ, iter_out, conv_out, efermi
+       integer(c_long), value :: ld
+       integer(c_int), value :: mb, nspin, diter, iconv_check, mb_ref, nfixed, kinteg, ncg, mloop, ipc, mode
+       real(c_double), value :: tol_esp, nelectron, dspn, ekbt
+     end function rsdft_gpu_calc_sweep
      integer(c_int) function rsdft_gpu_subspace_mate(k, s, unk, ld, mb, hsub, ldh) &
           bind(C, name="rsdft_gpu_subspace_mate")
        import :: c_int, c_long, c_ptr
@@ -282,6 +292,26 @@ CONTAINS
     call check(rsdft_gpu_conjugate_gradient(n1, n2, mb, k, s, c_loc(unk), c_loc(esp), c_loc(res), ncg, mloop, ipc, &
                mode), "conjugate_gradient")
   END SUBROUTINE gpu_conjugate_gradient
+
+  ! calc_sweep's loop for one Gamma point: unk(ML, MB, nspin) stays on the
+  ! device (register it first); esp holds esp0 on entry; ierr_out is the
+  ! iteration the loop stopped at, as the reference's (its loop leaves at
+  ! iter == Diter at the latest, so its "not converged" -2 never occurs)
+  SUBROUTINE gpu_calc_sweep(unk, esp, res, occ, Diter, iconv_check, tol_esp, mb_ref, Nelectron, Nfixed, dspn, &
+                            ekbt, kinteg, ncg, mloop, ipc, mode, ierr_out, efermi)
+    real(8), intent(INOUT), target :: unk(:, :, :)
+    real(8), intent(INOUT), target :: esp(:, :), res(:, :), occ(:, :)
+    integer, intent(IN) :: Diter, iconv_check, mb_ref, Nfixed, kinteg, ncg, mloop, ipc, mode
+    real(8), intent(IN) :: tol_esp, Nelectron, dspn, ekbt
+    integer, intent(OUT) :: ierr_out
+    real(8), intent(OUT), target :: efermi
+    integer(c_int), target :: it, cv
+    call check(rsdft_gpu_calc_sweep(c_loc(unk), int(size(unk, 1), c_long), int(size(unk, 2), c_int), &
+               int(size(unk, 3), c_int), c_loc(esp), c_loc(res), c_loc(occ), Diter, iconv_check, tol_esp, mb_ref, &
+               Nelectron, Nfixed, dspn, ekbt, kinteg, ncg, mloop, ipc, mode, c_loc(it), c_loc(cv), c_loc(efermi)), &
+               "calc_sweep")
+    ierr_out = it
+  END SUBROUTINE gpu_calc_sweep
 
   SUBROUTINE gpu_gram_schmidt(n0, n1, k, s, unk, mode)
     integer, intent(IN) :: n0, n1, k, s, mode

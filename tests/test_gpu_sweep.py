@@ -29,7 +29,7 @@ def host_loop(gpu, c, u, esp, diter, tol, mode):
         esp0 = esp.copy()
         gpu.eigensolver_sweep(1, 1, u, esp, res, ncg=4, mloop=3, mode=mode)
         occ, ef = O.calc_fermi(esp, ne)
-        m, conv = O.conv_check(esp, esp0, c.nband, tol)
+        m, conv = O.conv_check(esp, esp0, c.nocc, tol)
         if conv or it == diter:
             return it, conv, occ.ravel(), ef, res
     raise AssertionError
@@ -39,7 +39,7 @@ def host_loop(gpu, c, u, esp, diter, tol, mode):
 def test_calc_sweep_matches_host_loop(gpu, cells, mode):
     c, o = prepare(gpu, cells, "si8")
     start = np.asfortranarray(o.gram_schmidt_t(c.psi0()))
-    tol = 1e-9 if mode == api.MODE_FP64 else 1e-6
+    tol = 1e-9 if mode == api.MODE_FP64 else 1e-6  # eigenvalue change of the occupied bands (mb_ref)
     # reference loop on a device copy
     ua = dev(start)
     ea = np.zeros(c.nband)
@@ -51,7 +51,8 @@ def test_calc_sweep_matches_host_loop(gpu, cells, mode):
         esp = np.zeros(c.nband)
         res = np.zeros(c.nband)
         occ = np.zeros(c.nband)
-        r = gpu.calc_sweep(unk, esp, res, occ, diter=40, nelectron=2.0 * c.nocc, tol_esp=tol, mode=mode)
+        r = gpu.calc_sweep(unk, esp, res, occ, diter=40, nelectron=2.0 * c.nocc, tol_esp=tol, mb_ref=c.nocc,
+                           mode=mode)
         gpu.sync_to_host(unk)
     finally:
         gpu.unregister_wf(unk)
