@@ -62,9 +62,10 @@ __global__ void k_reduce_partials(const double* __restrict__ P, int nch, int m, 
 // C (m x n) = alpha A^T B with A, B tall (ML rows, leading dimension ld) on
 // the FP64 tensor cores (dmma.cu): split-K over the grid, partial tiles
 // reduced in a fixed order.  sym = 1 returns the symmetric part.
+// sym_op: B = H A with H symmetric, so only the upper tiles are formed.
 static int gemm_tn_splitk(const double* A, const double* B, long ld, int m, int n, double alpha, int sym,
-                          double* C) {
-    return dmma_gram(A, B, ld, ctx().ml, m, n, alpha, sym, C, m);
+                          double* C, bool sym_op = false) {
+    return dmma_gram(A, B, ld, ctx().ml, m, n, alpha, sym, C, m, sym_op);
 }
 
 static int check_info(int* dinfo, const char* what) {
@@ -150,7 +151,7 @@ int subspace_diag_device(double* psi, long ld, int mb, int spin, double* esp, in
     if (mode == RSDFT_MODE_FP64) {
         RS_CHECK(hpsi_device<double>(psi, hpsi, ld, mb, spin, nullptr));
         // Hsub = dV/2 (psi^T H psi + (H psi)^T psi): the symmetric part of dV psi^T (H psi)
-        RS_CHECK(gemm_tn_splitk(psi, hpsi, ld, mb, mb, c.dV, 1, H));
+        RS_CHECK(gemm_tn_splitk(psi, hpsi, ld, mb, mb, c.dV, 1, H, true));
         RS_CHECK(syevd(H, mb, esp, CUBLAS_FILL_MODE_UPPER, "subspace_diag: syevd"));
         RS_CHECK(dmma_gemm(false, c.ml, mb, mb, 1.0, psi, ld, H, mb, 0.0, hpsi, ld));
     } else {
@@ -228,7 +229,7 @@ int orth_subspace_diag_device(double* psi, long ld, int mb, int spin, double* es
     RS_CHECK(hpsi_device<double>(psi, hpsi, ld, mb, spin, nullptr));
     if (mode == RSDFT_MODE_FP64) {
         RS_CHECK(gemm_tn_splitk(psi, psi, ld, mb, mb, c.dV, 0, S));
-        RS_CHECK(gemm_tn_splitk(psi, hpsi, ld, mb, mb, c.dV, 1, H));
+        RS_CHECK(gemm_tn_splitk(psi, hpsi, ld, mb, mb, c.dV, 1, H, true));
     } else {
         RS_CHECK(gram_mixed_pair(psi, hpsi, ld, mb, c.dV, mode_terms(mode), S, H, &split));
     }

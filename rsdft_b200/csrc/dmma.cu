@@ -279,7 +279,7 @@ bool vec_ok(const DmmaArgs& g) {
 // Tall Gram: C (m x n, column-major, ldc) = alpha A^T B for A (K x m), B
 // (K x n) column-major with leading dimension ld, K = kdim (the grid).
 int dmma_gram(const double* A, const double* B, long ld, long kdim, int m, int n, double alpha, int symmetrize,
-              double* C, long ldc) {
+              double* C, long ldc, bool symmetric_product) {
     Context& c = ctx();
     constexpr int BM = 128, BN = 128;
     DmmaArgs g{};
@@ -292,7 +292,10 @@ int dmma_gram(const double* A, const double* B, long ld, long kdim, int m, int n
     g.K = kdim;
     g.ntm = div_up(m, BM);
     const int ntn = div_up(n, BN);
-    g.sym = (A == B && m == n) ? 1 : 0;
+    // upper tiles only for a symmetric product: A^T A, or A^T (H A) of a
+    // symmetric operator (its lower tiles equal the upper ones to rounding;
+    // the diagonal tiles are symmetrised by the reduction)
+    g.sym = (m == n && (A == B || (symmetric_product && symmetrize))) ? 1 : 0;
     g.ntiles = g.sym ? g.ntm * (g.ntm + 1) / 2 : g.ntm * ntn;
     // whole waves of CTAs (one per SM: 123 KB of stages): the largest split
     // count with tiles x splits <= 2 x SMs, K split evenly

@@ -68,6 +68,22 @@ def test_hpsi_fd_orders(gpu, md):
     assert rel(out, ref) <= TOL
 
 
+@pytest.mark.parametrize("ngrid", [16, 24])
+@pytest.mark.parametrize("md", [1, 2, 3, 4, 5, 6, 7, 8])
+def test_hpsi_fd_orders_tensor_stencil(gpu, ngrid, md):
+    """Grids whose rows are whole 8-point tiles take the FP64 stencil with the
+    in-plane derivatives on the DMMA pipe (k_stencil_dmma); every Md, and the
+    periodic wrap of 16- and 24-row grids (y halo boxes on both sides)."""
+    c = build_cell(Workload(f"si8_md{md}_g{ngrid}", 1, ngrid, 6, 3, 0.03, 79, md=md))
+    gpu.setup(c)
+    o = O.Oracle(c)
+    psi = np.asfortranarray(c.psi0())
+    ref = o.hamiltonian(psi)
+    out = np.zeros_like(psi, order="F")
+    gpu.hamiltonian(1, 1, psi, out, 1, c.ML, 1, psi.shape[1])
+    assert rel(out, ref) <= TOL
+
+
 def test_hpsi_symmetric(gpu, cells):
     c, o = prepare(gpu, cells, "si8")
     psi = np.asfortranarray(c.psi0()[:, :8])
