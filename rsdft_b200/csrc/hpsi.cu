@@ -516,177 +516,6 @@ __global__ void __launch_bounds__(384, 1) k_stencil_tma(const __grid_constant__ 
     if (!ok) atomicExch(err, 1);
 }
 
-// FP64 stencil with the in-plane part on the FP64 tensor pipe (DMMA).
-//
-// The x and y second derivatives of one plane are banded Toeplitz products:
-// for an 8 x 8 output tile at (y0, x0),
-//   D = Psi(8 rows, x0-Md .. x0+7+Md) Bx + Ay Psi(y0-Md .. y0+7+Md, 8 cols)
-// with Bx(x', x) = c(x' - x) (c0 at 0, cx_m at |x'-x| = m, else 0) and
-// Ay(y, y') = cy(|y' - y|).  Each is KS = ceil((8 + 2 Md)/4) m8n8k4 steps; the
-// coefficient fragments depend only on the lane and the step, so they live
-// in registers, and each operand element a lane needs is one 8-byte shared
-// load (20 bytes per point per axis instead of the ~56 of the vector window
-// loads).  The z direction keeps the register push march of k_stencil_tma:
-// each lane owns the two points of its D fragment, D[lane/4][2 (lane%4) + e].
-//
-// Geometry: a CTA owns 8 full-width rows (one 8-row group; 8 x 8 tiles, one
-// warp per tile column, n1 / 8 consumer warps) of one band and marches z.
-// Stage rows: MH halo rows, the 8 own rows, MH halo rows (MH = Md rounded up
-// to a multiple of 4, so that every box of the periodic y wrap starts on a
-// 128-byte boundary), then the 8 Vloc rows; row pitch RS = n1 + 4 doubles, so
-// the eight rows of a fragment load fall on distinct 32-byte bank groups.
-template <int MD>
-struct DmmaStencilShape {
-    static constexpr int MH = (MD + 3) / 4 * 4;
-    static constexpr int KS = (8 + 2 * MD + 3) / 4;
-    static constexpr int ROWS = 8 + 2 * MH;  // psi rows of a stage
-};
-
-__device__ __forceinline__ void dmma884(double (&d)[2], double a, double b) {
-    asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0, %1}, {%2}, {%3}, {%0, %1};"
-                 : "+d"(d[0]), "+d"(d[1])
-                 : "d"(a), "d"(b));
-}
-
-template <int MD, int NW>
-__global__ void __launch_bounds__(32 * NW, 1) k_stencil_dmma(const __grid_constant__ TmaMaps maps, StencilArgs<double> a,
-                                                           const CoefT<double> cf, int RS, int S, int ncw,
-                                                           int* __restrict__ err) {
-    using Sh = DmmaStencilShape<MD>;
-    constexpr int MH = Sh::MH, KS = Sh::KS, ROWS = Sh::ROWS;
-    constexpr int Q = 2 * MD + 1;
-    extern __shared__ __align__(128) unsigned char smem[];
-    const int n1 = a.n1, n2 = a.n2, n3 = a.n3;
-    const int SE = (ROWS + 8) * RS;  // doubles per stage: psi rows, then Vloc rows
-    double* stages = reinterpret_cast<double*>(smem);
-    uint64_t* full = reinterpret_cast<uint64_t*>(smem + (size_t)S * SE * sizeof(double));
-    uint64_t* empty = full + S;
-
-    const int t = threadIdx.x;
-    const int warp = t >> 5, lane = t & 31;
-    const int nzc = a.nzc;
-    const int band = blockIdx.y / nzc;
-    const int zc = blockIdx.y - band * nzc;
-    if (a.band_active && !a.band_active[band]) return;  // uniform per CTA
-    const int y0 = blockIdx.x * 8;
-    const int zs = zc * a.zlen;
-    const int zlen = min(zs + a.zlen, n3) - zs;
-    const int nk = zlen + 2 * MD;
-    const long plane = (long)n1 * n2;
-
-    if (t == 0) {
-        for (int s = 0; s < S; ++s) {
-            mbar_init(&full[s], 1);
-            mbar_init(&empty[s], ncw);
-        }
-        mbar_fence_init();
-    }
-    __syncthreads();
-
-    if (warp == ncw) {
-        // ------------------------------------------------------ producer
-        bool ok = true;
-        if (lane == 0) {
-            const uint32_t b_in = (uint32_t)((size_t)(ROWS + 8) * RS * sizeof(double));
-            const uint32_t b_out = (uint32_t)((size_t)8 * RS * sizeof(double));
-            for (int k = 0; k < nk; ++k) {
-                const int s = k % S;
-                if (k >= S && !mbar_wait(&empty[s], ((k / S) - 1) & 1)) ok = false;
-                double* dst = stages + (size_t)s * SE;
-                const int zp = pwrap(zs - MD + k, n3);
-                const bool inner = k >= MD && k < MD + zlen;
-                fence_proxy_async_smem();
-                mbar_arrive_expect_tx(&full[s], inner ? b_in : b_out);
-                if (!inner) {
-                    tma_load_4d(dst + MH * RS, &maps.mid, 0, y0, zp, band, &full[s]);
-                    continue;
-                }
-                if (y0 - MH >= 0 && y0 + 8 + MH <= n2) {
-                    tma_load_4d(dst, &maps.full, 0, y0 - MH, zp, band, &full[s]);
-                } else if (n2 == 8) {
-                    tma_load_4d(dst, &maps.wrap, 0, n2 - MH, zp, band, &full[s]);
-                    tma_load_4d(dst + MH * RS, &maps.mid, 0, 0, zp, band, &full[s]);
-                    tma_load_4d(dst + (MH + 8) * RS, &maps.wrap, 0, 0, zp, band, &full[s]);
-                } else if (y0 - MH < 0) {
-                    tma_load_4d(dst, &maps.wrap, 0, n2 - MH, zp, band, &full[s]);
-                    tma_load_4d(dst + MH * RS, &maps.edge, 0, 0, zp, band, &full[s]);
-                } else {
-                    tma_load_4d(dst, &maps.edge, 0, y0 - MH, zp, band, &full[s]);
-                    tma_load_4d(dst + (8 + MH) * RS, &maps.wrap, 0, 0, zp, band, &full[s]);
-                }
-                tma_load_4d(dst + ROWS * RS, &maps.vloc, 0, y0, zp, 0, &full[s]);
-            }
-        }
-        __syncwarp();
-        if (!ok) atomicExch(err, 1);
-        return;
-    }
-
-    // ---------------------------------------------------------- consumers
-    const int fr = lane >> 2, fc = lane & 3;
-    const int x0 = 8 * warp;
-    // coefficient fragments: x part B(k = fc, n = fr), y part A(row = fr, k = fc)
-    double bx[KS], ay[KS];
-#pragma unroll
-    for (int s = 0; s < KS; ++s) {
-        const int d = -MD + 4 * s + fc - fr;
-        const int ad = d < 0 ? -d : d;
-        bx[s] = d == 0 ? cf.c0 : (ad <= MD ? cf.cx[ad - 1] : 0.0);
-        ay[s] = (ad >= 1 && ad <= MD) ? cf.cy[ad - 1] : 0.0;
-    }
-    // per-lane shared-memory offsets (doubles) of the operand elements
-    int xoff[KS], yoff[KS];
-#pragma unroll
-    for (int s = 0; s < KS; ++s) {
-        int xx = x0 - MD + 4 * s + fc;
-        xx += xx < 0 ? n1 : (xx >= n1 ? -n1 : 0);
-        xoff[s] = (MH + fr) * RS + xx;
-        const int yy = min(MH - MD + 4 * s + fc, ROWS - 1);  // rows past the window meet a zero coefficient
-        yoff[s] = yy * RS + x0 + fr;
-    }
-    const int coff = (MH + fr) * RS + x0 + 2 * fc;  // this lane's two points
-    const int voff = (ROWS + fr) * RS + x0 + 2 * fc;
-    double* __restrict__ hb = a.hpsi + (long)band * a.ld + (long)n1 * (y0 + fr) + x0 + 2 * fc;
-
-    double acc[Q][2];
-#pragma unroll
-    for (int q = 0; q < Q; ++q) acc[q][0] = acc[q][1] = 0.0;
-
-    bool ok = true;
-    int s = 0, u = 0;
-    uint32_t ph = 0;
-    for (int k = 0; k < nk; ++k) {
-        if (!mbar_wait(&full[s], ph)) ok = false;
-        const double* st = stages + (size_t)s * SE;
-        const bool inner = k >= MD && k < MD + zlen;  // uniform
-        double c[2], in[2] = {0.0, 0.0};
-        const double2 cc = *reinterpret_cast<const double2*>(st + coff);
-        c[0] = cc.x;
-        c[1] = cc.y;
-        if (inner) {
-            double dx[2] = {0.0, 0.0}, dy[2] = {0.0, 0.0};
-#pragma unroll
-            for (int j = 0; j < KS; ++j) {
-                dmma884(dx, st[xoff[j]], bx[j]);
-                dmma884(dy, ay[j], st[yoff[j]]);
-            }
-            const double2 vv = *reinterpret_cast<const double2*>(st + voff);
-            in[0] = fma(vv.x, c[0], dx[0] + dy[0]);
-            in[1] = fma(vv.y, c[1], dx[1] + dy[1]);
-        }
-        __syncwarp();
-        if (lane == 0) mbar_arrive(&empty[s]);  // this warp is done with the stage
-        double* hp = k >= 2 * MD ? hb + plane * (zs + k - 2 * MD) : nullptr;
-        push_slot<double, MD, 2, 1>(u, acc, c, in, inner, cf, hp, n1);
-        if (++s == S) {
-            s = 0;
-            ph ^= 1u;
-        }
-        if (++u == Q) u = 0;
-    }
-    if (!ok) atomicExch(err, 1);
-}
-
 // Nonlocal scatter after the stencil: hpsi(p, b) += sum over the sphere
 // groups g covering p of sum_q uV(p, g, q) uVunk(g + q, b)
 // (ps_nloc2_op_module.f90:255-263), one thread per covered point and a chunk
@@ -839,79 +668,13 @@ static int launch_tma(StencilArgs<T> a, const StencilCoef& cf, int nb, cudaStrea
     return RSDFT_OK;
 }
 
-// k_stencil_dmma for an FP64 band block, when the grid has the shape it
-// takes (rows of 16..128 points in whole 8-point tiles, 8-row groups, y wrap
-// boxes that fit); *used = false otherwise.
-template <int MD>
-static int launch_dmma_stencil(StencilArgs<double> a, const StencilCoef& cf, int nb, cudaStream_t st, bool* used) {
-    Context& c = ctx();
-    using Sh = DmmaStencilShape<MD>;
-    *used = false;
-    const int n1 = a.n1, n2 = a.n2;
-    if (n1 % 8 != 0 || n1 < 16 || n1 > 128 || n2 % 8 != 0 || Sh::MH > n2 || !(n2 == 8 || n2 >= 8 + Sh::MH))
-        return RSDFT_OK;
-    if (reinterpret_cast<uintptr_t>(a.hpsi) % 16 != 0 || (a.ld * sizeof(double)) % 16 != 0) return RSDFT_OK;
-    const int RS = n1 + 4;
-    const size_t stage = (size_t)(Sh::ROWS + 8) * RS * sizeof(double);
-    const size_t budget = 220 * 1024;
-    const int S = (int)std::min<size_t>(budget / (stage + 16), 8);
-    if (S < 3) return RSDFT_OK;
-    const int sms = c.num_sms > 0 ? c.num_sms : 148;
-    const long base = (long)(n2 / 8) * nb;
-    int nzc = (int)std::min<long>(std::max<long>(1, (sms + base - 1) / base), std::max(1, a.n3 / (4 * MD)));
-    while ((long)nb * nzc > 65535 && nzc > 1) --nzc;
-    a.zlen = div_up(a.n3, nzc);
-    a.nzc = div_up(a.n3, a.zlen);
-    TmaMaps maps;
-    const CUtensorMapDataType dt = CU_TENSOR_MAP_DATA_TYPE_FLOAT64;
-    const unsigned long long dims[4] = {(unsigned long long)n1, (unsigned long long)n2, (unsigned long long)a.n3,
-                                        (unsigned long long)nb};
-    const unsigned long long strides[3] = {(unsigned long long)n1 * 8, (unsigned long long)n1 * n2 * 8,
-                                           (unsigned long long)a.ld * 8};
-    const unsigned long long vdims[4] = {(unsigned long long)n1, (unsigned long long)n2, (unsigned long long)a.n3,
-                                         1ull};
-    const unsigned long long vstrides[3] = {strides[0], strides[1], (unsigned long long)n1 * n2 * a.n3 * 8};
-    const unsigned int R = (unsigned)RS, MH = (unsigned)Sh::MH;
-    const unsigned int bf[4] = {R, (unsigned)Sh::ROWS, 1, 1}, be[4] = {R, 8 + MH, 1, 1}, bm[4] = {R, 8, 1, 1},
-                       bw[4] = {R, MH, 1, 1};
-    if (encode_tmap_4d(&maps.full, dt, a.psi, dims, strides, bf) != RSDFT_OK ||
-        encode_tmap_4d(&maps.edge, dt, a.psi, dims, strides, be) != RSDFT_OK ||
-        encode_tmap_4d(&maps.mid, dt, a.psi, dims, strides, bm) != RSDFT_OK ||
-        encode_tmap_4d(&maps.wrap, dt, a.psi, dims, strides, bw) != RSDFT_OK ||
-        encode_tmap_4d(&maps.vloc, dt, a.vloc, vdims, vstrides, bm) != RSDFT_OK)
-        return RSDFT_OK;  // not usable for this shape: the caller takes another kernel
-    const size_t smem = (size_t)S * stage + (size_t)S * 16;
-    const int ncw = n1 / 8;
-    dim3 grid(n2 / 8, (unsigned)(nb * a.nzc));
-    // the register budget follows the thread count: up to 10 warps (rows of
-    // up to 72 points), 13 (96), else up to 17 warps
-    if (ncw + 1 <= 10) {
-        RS_CHECK(set_smem_optin((const void*)k_stencil_dmma<MD, 10>, (int)smem));
-        launch(k_stencil_dmma<MD, 10>, grid, 32 * (ncw + 1), smem, st, maps, a, coef_as<double>(cf), RS, S, ncw,
-               c.err_flag);
-    } else if (ncw + 1 <= 13) {
-        RS_CHECK(set_smem_optin((const void*)k_stencil_dmma<MD, 13>, (int)smem));
-        launch(k_stencil_dmma<MD, 13>, grid, 32 * (ncw + 1), smem, st, maps, a, coef_as<double>(cf), RS, S, ncw,
-               c.err_flag);
-    } else {
-        RS_CHECK(set_smem_optin((const void*)k_stencil_dmma<MD, 17>, (int)smem));
-        launch(k_stencil_dmma<MD, 17>, grid, 32 * (ncw + 1), smem, st, maps, a, coef_as<double>(cf), RS, S, ncw,
-               c.err_flag);
-    }
-    RS_LAUNCH();
-    *used = true;
-    return RSDFT_OK;
-}
-
 template <typename T, int MD>
 static int launch_stencil_md2(StencilArgs<T> a, const StencilCoef& cf, int nb, cudaStream_t st) {
     const Context& c = ctx();
     bool used = false;
-    // FP64: the in-plane derivatives on the DMMA pipe where the shape allows
-    if constexpr (sizeof(T) == 8) RS_CHECK(launch_dmma_stencil<MD>(a, cf, nb, st, &used));
     // two rows per thread up to Md = 6; one above, where the 2 Md + 1
     // accumulators of two rows no longer fit the register budget
-    if (!used) RS_CHECK((launch_tma<T, MD, (MD <= 6 ? 2 : 1)>(a, cf, nb, st, &used)));
+    RS_CHECK((launch_tma<T, MD, (MD <= 6 ? 2 : 1)>(a, cf, nb, st, &used)));
     if (used) {
         if (a.gpt_ptr && c.nl_npt > 0) {
             constexpr int BCH = 32;

@@ -70,10 +70,10 @@ def test_hpsi_fd_orders(gpu, md):
 
 @pytest.mark.parametrize("ngrid", [16, 24])
 @pytest.mark.parametrize("md", [1, 2, 3, 4, 5, 6, 7, 8])
-def test_hpsi_fd_orders_tensor_stencil(gpu, ngrid, md):
-    """Grids whose rows are whole 8-point tiles take the FP64 stencil with the
-    in-plane derivatives on the DMMA pipe (k_stencil_dmma); every Md, and the
-    periodic wrap of 16- and 24-row grids (y halo boxes on both sides)."""
+def test_hpsi_fd_orders_tma_stencil(gpu, ngrid, md):
+    """Grids with 16-byte-aligned rows take the TMA z-march stencil
+    (k_stencil_tma): every Md with the periodic wrap of 16- and 24-row grids
+    (y halo boxes on both sides, a tile as high as the grid)."""
     c = build_cell(Workload(f"si8_md{md}_g{ngrid}", 1, ngrid, 6, 3, 0.03, 79, md=md))
     gpu.setup(c)
     o = O.Oracle(c)
