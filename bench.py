@@ -358,8 +358,11 @@ def main():
         results[mode] = {"ms": ms, "esp": esp.cpu().numpy().copy()}
 
     # ---- accuracy of the headline form against FP64 from the same start:
-    # 10 iterations each, then the FP64 closing pass (CholeskyQR2 + Rayleigh
-    # quotients and residuals in FP64) on both
+    # 10 iterations each (separate copies of the start bands), then the FP64
+    # closing pass (CholeskyQR2 + Rayleigh quotients and residuals in FP64)
+    # on both; at iteration 3, before the bands converge, the two
+    # trajectories' Ritz values and one Rayleigh-Ritz step of the headline
+    # form against the FP64 step on the same (FP64 CG) bands
     acc = {}
     if head != "fp64" and not args.no_accuracy:
         niter = 10
@@ -369,10 +372,25 @@ def main():
         eb = torch.zeros_like(esp)
         ra = torch.zeros_like(esp)
         rb = torch.zeros_like(esp)
-        for _ in range(niter):
+        occ = cell.nocc
+        early = {}
+        for it in range(1, niter + 1):
             g.eigensolver_iteration(ua, ea, ra, ncg=args.ncg, mloop=args.mloop, mode=0)
             g.eigensolver_iteration(ub, eb, rb, ncg=args.ncg, mloop=args.mloop, mode=MODES[head])
-        sub_err = float((ea[: cell.nocc] - eb[: cell.nocc]).abs().max())
+            if it == 3:
+                x = api.fortran_copy(ua)
+                e0, r0 = torch.zeros_like(esp), torch.zeros_like(esp)
+                g.conjugate_gradient(1, ML, MB, 1, 1, x, e0, r0, ncg=args.ncg, mloop=args.mloop, mode=0)
+                y = api.fortran_copy(x)
+                e1, e2 = torch.zeros_like(esp), torch.zeros_like(esp)
+                g.orth_subspace_diag(1, 1, x, e1, mode=0)
+                g.orth_subspace_diag(1, 1, y, e2, mode=MODES[head])
+                early = {"iteration": it,
+                         "trajectory_eig_diff_occupied_ha": float((ea[:occ] - eb[:occ]).abs().max()),
+                         "rayleigh_ritz_step_eig_err_occupied_ha": float((e1[:occ] - e2[:occ]).abs().max()),
+                         "fp64_residual_max_occupied": float(ra[:occ].max())}
+                del x, y
+        sub_err = float((ea[:occ] - eb[:occ]).abs().max())
         orth_before = float(((ub.t() @ ub) * cell.dV - torch.eye(MB, dtype=torch.float64, device="cuda")).abs().max())
         f0, f1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         g.finalize_fp64(ua, ea, ra)
@@ -380,7 +398,6 @@ def main():
         g.finalize_fp64(ub, eb, rb)
         f1.record(stream)
         barrier()
-        occ = cell.nocc
         orth = float(((ub.t() @ ub) * cell.dV - torch.eye(MB, dtype=torch.float64, device="cuda")).abs().max())
         acc = {"iterations": niter,
                "eig_err_max_occupied_ha": float((ea[:occ] - eb[:occ]).abs().max()),
@@ -389,7 +406,9 @@ def main():
                "orth_err_after_fp64_pass": orth,
                "orth_err_before_fp64_pass": orth_before,
                "fp64_closing_pass_ms": f0.elapsed_time(f1),
-               "residual_max_occupied": float(rb[:occ].max())}
+               "residual_max_occupied": float(rb[:occ].max()),
+               "unconverged": early}
+        del ua, ub
 
     # ---- hpsi roofline on all bands (device pointers, K launches)
     out = api.fortran_empty(ML, MB)

@@ -332,13 +332,27 @@ __global__ void s_init(CGScal s, int nb) {
     s.res[b] = 0.0;
 }
 
-// top of the icg loop (cg_module.f90:205-219)
-__global__ void s_top(CGScal s, int nb, int last) {
+// top of the icg loop (cg_module.f90:205-219): a band stops once its
+// Rayleigh quotient moved by less than tol_e in the last line step (the
+// reference's 1e-15, cg_module.f90:218, in FP64)
+__global__ void s_top(CGScal s, int nb, int last, double tol_e) {
     int b = blockIdx.x * blockDim.x + threadIdx.x;
     if (b >= nb || !s.active[b]) return;
     const double rb = s.rb[b];
     s.res[b] = rb / 4.0;
-    if (rb < 0.0 || fabs(s.E[b] - s.E1[b]) < 1e-15 || last) s.active[b] = 0;
+    if (rb < 0.0 || fabs(s.E[b] - s.E1[b]) < tol_e || last) s.active[b] = 0;
+}
+
+// The stopping tolerance of a line step.  FP64 bands use the reference's
+// 1e-15.  The Rayleigh quotient of an FP32 band (FP64 dots of FP32 vectors
+// and an FP32 H x) never settles that far: once converged it keeps moving by
+// 3e-12 .. 3e-11 Ha per step (median 2.5e-11, measured on the 216-atom cell
+// after 10 to 30 iterations), so the FP32 form stops a band at 1e-10 Ha, the
+// same rule one level above its noise floor, four orders of magnitude below
+// the 1e-6 Ha eigenvalue tolerance of the mixed forms.
+template <typename T>
+constexpr double cg_stop_tol() {
+    return sizeof(T) == 8 ? 1e-15 : 1e-10;
 }
 
 __global__ void s_pc0(CGScal s, int nb) {
@@ -556,7 +570,7 @@ static int cg_run(T* x, long ld, int mb, int spin, double* esp, double* res, int
     const bool sstep = ipc == 4 && mloop >= 1 && mloop <= SS_MAXM;
     for (int icg = 1; icg <= ncg + 1; ++icg) {
         const int last = icg == ncg + 1;
-        launch(s_top, sb, 128, 0, st, s, mb, last);
+        launch(s_top, sb, 128, 0, st, s, mb, last, cg_stop_tol<T>());
         if (last) break;
         if (sstep) {
             // --- preconditioner, rb = <Pg|g> dV and the search direction p
