@@ -88,7 +88,7 @@ static int cholqr_pass(const double* psi, double* out, long ld, int nb, double* 
     if (mode == RSDFT_MODE_FP64)
         RS_CHECK(gemm_tn_splitk(psi, psi, ld, nb, nb, c.dV, 0, S));
     else
-        RS_CHECK(gram_mixed(psi, psi, ld, nb, c.dV, 0, mode_terms(mode), S, &split));
+        RS_CHECK(gram_mixed(psi, psi, ld, nb, c.dV, 0, mode, S, &split));
     int lwork = 0;
     RS_SOLVER(cusolverDnDpotrf_bufferSize(c.solver, CUBLAS_FILL_MODE_UPPER, nb, S, nb, &lwork));
     double* work = nullptr;
@@ -109,7 +109,7 @@ static int cholqr_pass(const double* psi, double* out, long ld, int nb, double* 
     if (mode == RSDFT_MODE_FP64)
         RS_CHECK(dmma_gemm(false, c.ml, nb, nb, 1.0, psi, ld, S, nb, 0.0, out, ld));
     else
-        RS_CHECK(rotate_mixed(psi, out, ld, nb, S, nb, mode_terms(mode), split));
+        RS_CHECK(rotate_mixed(psi, out, ld, nb, S, nb, mode, split));
     return RSDFT_OK;
 }
 
@@ -157,10 +157,10 @@ int subspace_diag_device(double* psi, long ld, int mb, int spin, double* esp, in
     } else {
         RS_CHECK(hpsi_device<double>(psi, hpsi, ld, mb, spin, nullptr));
         const void* split = nullptr;
-        RS_CHECK(gram_mixed(psi, hpsi, ld, mb, c.dV, 1, mode_terms(mode), H, &split));
+        RS_CHECK(gram_mixed(psi, hpsi, ld, mb, c.dV, 1, mode, H, &split));
         RS_CHECK(syevd(H, mb, esp, CUBLAS_FILL_MODE_UPPER, "subspace_diag: syevd"));
         // reads only the BF16 split of psi: written in place
-        RS_CHECK(rotate_mixed(psi, psi, ld, mb, H, mb, mode_terms(mode), split));
+        RS_CHECK(rotate_mixed(psi, psi, ld, mb, H, mb, mode, split));
         return RSDFT_OK;
     }
     RS_CUDA(cudaMemcpy2DAsync(psi, ld * sizeof(double), hpsi, ld * sizeof(double), c.ml * sizeof(double), mb,
@@ -231,7 +231,7 @@ int orth_subspace_diag_device(double* psi, long ld, int mb, int spin, double* es
         RS_CHECK(gemm_tn_splitk(psi, psi, ld, mb, mb, c.dV, 0, S));
         RS_CHECK(gemm_tn_splitk(psi, hpsi, ld, mb, mb, c.dV, 1, H, true));
     } else {
-        RS_CHECK(gram_mixed_pair(psi, hpsi, ld, mb, c.dV, mode_terms(mode), S, H, &split));
+        RS_CHECK(gram_mixed_pair(psi, hpsi, ld, mb, c.dV, mode, S, H, &split));
     }
     int lwork = 0;
     RS_SOLVER(cusolverDnDpotrf_bufferSize(c.solver, CUBLAS_FILL_MODE_UPPER, mb, S, mb, &lwork));
@@ -271,7 +271,7 @@ int orth_subspace_diag_device(double* psi, long ld, int mb, int spin, double* es
     } else {
         // the tensor-core rotation reads only the BF16 split of psi, so it
         // can write psi itself
-        RS_CHECK(rotate_mixed(psi, psi, ld, mb, T, mb, mode_terms(mode), split));
+        RS_CHECK(rotate_mixed(psi, psi, ld, mb, T, mb, mode, split));
     }
     return RSDFT_OK;
 }
@@ -297,7 +297,7 @@ int orth_subspace_diag_f32(const float* x32, const float* hx, double* psi, long 
         RS_CHECK(hpsi_device<float>(x32, h32, ld, mb, spin, nullptr));
     }
     const void* split = nullptr;
-    RS_CHECK(gram_mixed_pair(x32, h32, ld, mb, c.dV, mode_terms(mode), S, H, &split));
+    RS_CHECK(gram_mixed_pair(x32, h32, ld, mb, c.dV, mode, S, H, &split));
     int lwork = 0;
     RS_SOLVER(cusolverDnDpotrf_bufferSize(c.solver, CUBLAS_FILL_MODE_UPPER, mb, S, mb, &lwork));
     double* work = nullptr;
@@ -330,7 +330,7 @@ int orth_subspace_diag_f32(const float* x32, const float* hx, double* psi, long 
     RS_CHECK(dmma_gemm(true, mb, mb, mb, 1.0, S, mb, T, mb, 0.0, H, mb));
     RS_CHECK(syevd(H, mb, esp, CUBLAS_FILL_MODE_UPPER, "eigensolver_sweep: syevd"));
     RS_CHECK(dmma_gemm(false, mb, mb, mb, 1.0, S, mb, H, mb, 0.0, T, mb));
-    return rotate_mixed(x32, psi, ld, mb, T, mb, mode_terms(mode), split);
+    return rotate_mixed(x32, psi, ld, mb, T, mb, mode, split);
 }
 
 }  // namespace rsdft

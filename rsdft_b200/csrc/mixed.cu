@@ -1,10 +1,15 @@
 // Mixed-precision contractions on the 5th-generation tensor cores (tcgen05).
 //
 // Operands are split into BF16 terms, x = x0 + x1 + x2 (x0 = bf16(x),
-// x1 = bf16(x - x0), x2 = bf16(x - x0 - x1): 24 significant bits), and a
-// product is the sum of the term pairs with s + t < NT (NT = 3: six
-// products, "split-BF16 x3 terms"; NT = 2: three products), every pair an
-// exact BF16 x BF16 product accumulated in FP32 in tensor memory.
+// x1 = bf16(x - x0), x2 = bf16(x - x0 - x1): 24 significant bits), or into
+// two TF32 terms (x0 = tf32(x), x1 = tf32(x - x0): 22 bits), and a product is
+// the sum of the term pairs with s + t < NT (NT = 3: six products,
+// "split-BF16 x3 terms"; NT = 2: three products), every pair an exact
+// BF16 x BF16 (kind::f16) or TF32 x TF32 (kind::tf32) product accumulated in
+// FP32 in tensor memory.  A slice row of one K block is 64 bytes in both
+// kinds (32 BF16 or 16 TF32 values), so the tiles, stages and descriptors
+// are the same; only the MMA kind, the element count per block and the TMA
+// element type differ.
 //
 // k_umma (one CTA = one 128 x BN output tile):
 //   warp 0    TMA producer: per K block of 32, the NT slices of the A tile
@@ -38,7 +43,8 @@
 namespace rsdft {
 
 constexpr int UB_M = 128;      // tile rows (TMEM lanes)
-constexpr int UB_K = 32;       // K block (64 bytes of BF16: one swizzle row)
+constexpr int UB_K = 32;       // K block in BF16 values (64 bytes: one swizzle row)
+constexpr int UB_KB = 64;      // K block in bytes, both element kinds
 constexpr int U_EPI_WARPS = 8;
 constexpr int U_THREADS = 32 * (2 + U_EPI_WARPS);
 constexpr int U_SEG = 4;       // K blocks per FP32 accumulation segment (DRAIN)
@@ -49,6 +55,76 @@ __device__ __forceinline__ void split_bf16(double x, __nv_bfloat16& h, __nv_bflo
     m = __float2bfloat16_rn((float)r);
     r -= (double)__bfloat162float(m);
     l = __float2bfloat16_rn((float)r);
+}
+
+// two TF32 terms of x (round to nearest, ties away: cvt.rna.tf32.f32), as
+// FP32 bit patterns with the low 13 mantissa bits zero
+__device__ __forceinline__ uint32_t to_tf32(float x) {
+    uint32_t r;
+    asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(r) : "f"(x));
+    return r;
+}
+__device__ __forceinline__ void split_tf32(double x, uint32_t& h, uint32_t& l) {
+    h = to_tf32((float)x);
+    l = to_tf32((float)(x - (double)__uint_as_float(h)));
+}
+
+// TF32 versions of the three split kernels below: two slices of 4-byte
+// values in the same layouts
+template <typename TI>
+__global__ void __launch_bounds__(256) k_split_cols_tf32(const TI* __restrict__ psi, long ld, int nb, long ml,
+                                                         uint32_t* __restrict__ out) {
+    const long n = ml * nb;
+    const int b = blockIdx.y;
+    const long k0 = ((long)blockIdx.x * blockDim.x + threadIdx.x) * 4;
+    if (k0 >= ml) return;
+    const TI* src = psi + (long)b * ld + k0;
+    uint32_t* o = out + (long)b * ml + k0;
+    for (long k = 0; k < 4 && k0 + k < ml; ++k) {
+        uint32_t h, l;
+        split_tf32((double)src[k], h, l);
+        o[k] = h;
+        o[n + k] = l;
+    }
+}
+
+template <typename TI>
+__global__ void k_split_rows_tf32(const TI* __restrict__ psi, long ld, int nb, long ml, int mbk,
+                                  uint32_t* __restrict__ out) {
+    __shared__ double tile[32][33];
+    const long i0 = (long)blockIdx.x * 32;
+    const int m0 = blockIdx.y * 32;
+    const int tx = threadIdx.x, ty = threadIdx.y;  // 32 x 8
+    for (int r = ty; r < 32; r += 8) {
+        const long i = i0 + tx;
+        const int m = m0 + r;
+        tile[r][tx] = (i < ml && m < nb) ? (double)psi[(long)m * ld + i] : 0.0;
+    }
+    __syncthreads();
+    const long n = ml * mbk;
+    for (int r = ty; r < 32; r += 8) {
+        const long i = i0 + r;
+        const int m = m0 + tx;
+        if (i < ml && m < mbk) {
+            uint32_t h, l;
+            split_tf32(tile[tx][r], h, l);
+            const long e = i * mbk + m;
+            out[e] = h;
+            out[n + e] = l;
+        }
+    }
+}
+
+__global__ void k_split_small_tf32(const double* __restrict__ V, int mb, int ldv, int mbk, uint32_t* __restrict__ out) {
+    const long n = (long)mb * mbk;
+    for (long e = (long)blockIdx.x * blockDim.x + threadIdx.x; e < n; e += (long)gridDim.x * blockDim.x) {
+        const int col = (int)(e / mbk), m = (int)(e - (long)col * mbk);
+        const double x = m < mb ? V[(long)col * ldv + m] : 0.0;
+        uint32_t h, l;
+        split_tf32(x, h, l);
+        out[e] = h;
+        out[n + e] = l;
+    }
 }
 
 // slices[s][b][k] = term s of psi(k, b): same layout as psi (K-major per
@@ -164,10 +240,12 @@ __device__ __forceinline__ void pair_tiles(const UmmaArgs& g, int pair, int& tm,
     tm = r;
 }
 
-template <int BN, int NT, int NS, bool DRAIN, bool BMN>
+template <int BN, int NT, int NS, bool DRAIN, bool BMN, bool TF = false>
 __global__ void __launch_bounds__(U_THREADS, 1) k_umma(const __grid_constant__ UmmaMaps maps, UmmaArgs g) {
-    constexpr int ABYTES = UB_M * UB_K * 2;  // one A slice tile
-    constexpr int BBYTES = BN * UB_K * 2;
+    static_assert(!(TF && BMN), "TF32 operands are K-major");
+    constexpr int ABYTES = UB_M * UB_KB;  // one A slice tile
+    constexpr int BBYTES = BN * UB_KB;
+    constexpr int UKE = TF ? UB_KB / 4 : UB_K;  // K values per block
     constexpr int STAGE = NT * (ABYTES + BBYTES);
     // Accumulators, double-buffered between the MMA chain and the epilogue.
     // DRAIN: two per buffer, one for the hi x hi product and one for the
@@ -178,7 +256,7 @@ __global__ void __launch_bounds__(U_THREADS, 1) k_umma(const __grid_constant__ U
     constexpr int NACC = DRAIN ? 4 : 2;
     constexpr int TCOLS = NACC * BN;  // 512 for BN = 128 (DRAIN) and BN = 256 (DIRECT)
     static_assert(TCOLS <= 512, "tensor memory holds 512 columns");
-    constexpr uint32_t IDESC = umma_idesc_bf16(UB_M, BN, BMN);
+    constexpr uint32_t IDESC = TF ? umma_idesc_tf32(UB_M, BN) : umma_idesc_bf16(UB_M, BN, BMN);
     // MN-major B (BMN): the tile is BN / 32 boxes of 32 N values x UB_K K rows
     constexpr uint32_t B_LBO = 32 * UB_K * 2, B_SBO = 8 * 64;
     extern __shared__ __align__(1024) unsigned char smem[];
@@ -254,7 +332,7 @@ __global__ void __launch_bounds__(U_THREADS, 1) k_umma(const __grid_constant__ U
                     }
                     unsigned char* st = smem + (size_t)s * STAGE;
                     mbar_arrive_expect_tx(&full[s], STAGE);
-                    const int k = kb * UB_K;
+                    const int k = kb * UKE;
 #pragma unroll
                     for (int t = 0; t < NT; ++t) {
                         // the maps are rank 4 ({K, rows, slice, 1}): 4-D loads, w = 0
@@ -297,18 +375,21 @@ __global__ void __launch_bounds__(U_THREADS, 1) k_umma(const __grid_constant__ U
                         const int ta = p == 0 ? 0 : p == 1 ? 0 : p == 2 ? 1 : p == 3 ? 0 : p == 4 ? 1 : 2;
                         const int tb = p == 0 ? 0 : p == 1 ? 1 : p == 2 ? 0 : p == 3 ? 2 : p == 4 ? 1 : 0;
 #pragma unroll
-                        for (int kk = 0; kk < UB_K / 16; ++kk) {
+                        for (int kk = 0; kk < 2; ++kk) {  // two MMAs of 32 bytes of K
                             const uint64_t ad = umma_desc_sw64(sa + ta * ABYTES + kk * 32);
                             const uint64_t bd =
                                 BMN ? umma_desc_mn_sw64(sb + tb * BBYTES + kk * 16 * 64, B_LBO, B_SBO)
                                     : umma_desc_sw64(sb + tb * BBYTES + kk * 32);
-                            if (DRAIN && p > 0) {
-                                umma_bf16(dx, ad, bd, IDESC, firstx ? 0u : 1u);
+                            const uint32_t dd = (DRAIN && p > 0) ? dx : d;
+                            const uint32_t accum = (DRAIN && p > 0) ? (firstx ? 0u : 1u) : (first ? 0u : 1u);
+                            if (TF)
+                                umma_tf32(dd, ad, bd, IDESC, accum);
+                            else
+                                umma_bf16(dd, ad, bd, IDESC, accum);
+                            if (DRAIN && p > 0)
                                 firstx = false;
-                            } else {
-                                umma_bf16(d, ad, bd, IDESC, first ? 0u : 1u);
+                            else
                                 first = false;
-                            }
                         }
                     }
                     umma_commit(&empty[s]);
@@ -433,20 +514,24 @@ __global__ void k_reduce_tiles(const double* __restrict__ P, int nsplit, int npa
     C[(size_t)j * m + i] = alpha * v;
 }
 
-static int map3(CUtensorMap* mp, const __nv_bfloat16* base, long k, long rows, int box_rows) {
-    const unsigned long long dims[4] = {(unsigned long long)k, (unsigned long long)rows, 3ull, 1ull};
-    const unsigned long long strides[3] = {(unsigned long long)k * 2, (unsigned long long)k * rows * 2,
-                                           (unsigned long long)k * rows * 6};
-    const unsigned int box[4] = {(unsigned)UB_K, (unsigned)box_rows, 1u, 1u};
-    return encode_tmap_4d_swz64(mp, base, dims, strides, box);
+// Tensor map over the slices [s][rows][k] of a split (k fastest): 3 BF16 or
+// 2 TF32 slices, a 64-byte K block per row, 64-byte swizzle
+static int map3(CUtensorMap* mp, const void* base, long k, long rows, int box_rows, bool tf32 = false) {
+    const unsigned long long eb = tf32 ? 4 : 2, ns = tf32 ? 2 : 3;
+    const unsigned long long dims[4] = {(unsigned long long)k, (unsigned long long)rows, ns, 1ull};
+    const unsigned long long strides[3] = {(unsigned long long)k * eb, (unsigned long long)k * rows * eb,
+                                           (unsigned long long)k * rows * eb * ns};
+    const unsigned int box[4] = {(unsigned)(UB_KB / eb), (unsigned)box_rows, 1u, 1u};
+    return encode_tmap_4d(mp, tf32 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT32 : CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, base, dims,
+                          strides, box, CU_TENSOR_MAP_SWIZZLE_64B);
 }
 
-template <int BN, int NT, int NS, bool DRAIN, bool BMN = false>
+template <int BN, int NT, int NS, bool DRAIN, bool BMN = false, bool TF = false>
 static int launch_umma(const UmmaMaps& maps, const UmmaArgs& g, dim3 grid) {
-    constexpr int STAGE = NT * (UB_M * UB_K * 2 + BN * UB_K * 2);
+    constexpr int STAGE = NT * (UB_M * UB_KB + BN * UB_KB);
     const size_t smem = (size_t)NS * STAGE + 256;
-    RS_CHECK(set_smem_optin((const void*)k_umma<BN, NT, NS, DRAIN, BMN>, (int)smem));
-    launch(k_umma<BN, NT, NS, DRAIN, BMN>, grid, U_THREADS, smem, ctx().stream, maps, g);
+    RS_CHECK(set_smem_optin((const void*)k_umma<BN, NT, NS, DRAIN, BMN, TF>, (int)smem));
+    launch(k_umma<BN, NT, NS, DRAIN, BMN, TF>, grid, U_THREADS, smem, ctx().stream, maps, g);
     RS_LAUNCH();
     return RSDFT_OK;
 }
@@ -455,15 +540,16 @@ static int launch_umma(const UmmaMaps& maps, const UmmaArgs& g, dim3 grid) {
 // (ML x nb, leading dimension ld); B == A computes only the upper tiles.
 // Gram matrix from BF16 slices (ML x nb each, 3 slices): C = alpha sa^T sb,
 // symmetric tile pairs only when same.
-static int gram_from_slices(__nv_bfloat16* sa, __nv_bfloat16* sb, bool same, int nb, double alpha, int symmetrize,
-                            int nterms, double* C, bool upper_only = false) {
+static int gram_from_slices(void* sa, void* sb, bool same, int nb, double alpha, int symmetrize, Split sp,
+                            double* C, bool upper_only = false) {
     Context& c = ctx();
     const long ml = c.ml;
     UmmaMaps maps;
-    RS_CHECK(map3(&maps.a, sa, ml, nb, UB_M));
-    RS_CHECK(map3(&maps.b, sb, ml, nb, 128));
+    RS_CHECK(map3(&maps.a, sa, ml, nb, UB_M, sp.tf32));
+    RS_CHECK(map3(&maps.b, sb, ml, nb, 128, sp.tf32));
     UmmaArgs g{};
-    g.kblocks = (int)((ml + UB_K - 1) / UB_K);
+    const int uke = sp.tf32 ? UB_KB / 4 : UB_K;
+    g.kblocks = (int)((ml + uke - 1) / uke);
     g.ntm = g.ntn = (nb + UB_M - 1) / UB_M;
     // tile pairs tm <= tn only when the product is symmetric: A^T A, or (with
     // upper_only) A^T B for a symmetric operator B = H A, whose lower tiles
@@ -479,7 +565,9 @@ static int gram_from_slices(__nv_bfloat16* sa, __nv_bfloat16* sb, bool same, int
     RS_CHECK(workspace_t("umma_part", (size_t)nsplit * g.npairs * 128 * UB_M, &g.partial));
     g.err = c.err_flag;
     g.mrows = g.nrows = nb;
-    if (nterms == 3)
+    if (sp.tf32)
+        RS_CHECK((launch_umma<128, 2, 4, true, false, true>(maps, g, dim3(g.npairs, nsplit))));
+    else if (sp.terms == 3)
         RS_CHECK((launch_umma<128, 3, 4, true>(maps, g, dim3(g.npairs, nsplit))));
     else
         RS_CHECK((launch_umma<128, 2, 4, true>(maps, g, dim3(g.npairs, nsplit))));
@@ -489,62 +577,82 @@ static int gram_from_slices(__nv_bfloat16* sa, __nv_bfloat16* sb, bool same, int
     return RSDFT_OK;
 }
 
-// BF16 slices of a tall FP64 / FP32 block into the named workspace
+// BF16 (3 slices) or TF32 (2 slices) terms of a tall FP64 / FP32 block into
+// the named workspace
 template <typename TI>
-static int split_cols(const TI* A, long ld, int nb, const char* ws, __nv_bfloat16** out) {
+static int split_cols(const TI* A, long ld, int nb, const char* ws, Split sp, void** out) {
     Context& c = ctx();
     const long ml = c.ml;
     if (ml % 8 != 0) {
         set_error("mixed contractions need ML to be a multiple of 8");
         return RSDFT_EUNSUP;
     }
-    RS_CHECK(workspace_t(ws, 3 * (size_t)ml * nb, out));
+    if (sp.tf32) {
+        uint32_t* o = nullptr;
+        RS_CHECK(workspace_t(ws, 2 * (size_t)ml * nb, &o));
+        launch(k_split_cols_tf32<TI>, dim3(div_up(ml, 1024), nb), 256, 0, c.stream, A, ld, nb, ml, o);
+        RS_LAUNCH();
+        *out = o;
+        return RSDFT_OK;
+    }
+    __nv_bfloat16* o = nullptr;
+    RS_CHECK(workspace_t(ws, 3 * (size_t)ml * nb, &o));
     const int vec = ((ld * (long)sizeof(TI)) % 16 == 0 && reinterpret_cast<uintptr_t>(A) % 16 == 0) ? 1 : 0;
-    launch(k_split_cols<TI>, dim3(div_up(ml, 2048), nb), 256, 0, c.stream, A, ld, nb, ml, *out, vec);
+    launch(k_split_cols<TI>, dim3(div_up(ml, 2048), nb), 256, 0, c.stream, A, ld, nb, ml, o, vec);
     RS_LAUNCH();
+    *out = o;
     return RSDFT_OK;
 }
 
-int gram_mixed(const double* A, const double* B, long ld, int nb, double alpha, int symmetrize, int nterms,
+int gram_mixed(const double* A, const double* B, long ld, int nb, double alpha, int symmetrize, int mode,
                double* C, const void** a_split) {
-    __nv_bfloat16 *sa = nullptr, *sb = nullptr;
-    RS_CHECK(split_cols(A, ld, nb, "umma_sa", &sa));
+    const Split sp = mode_split(mode);
+    void *sa = nullptr, *sb = nullptr;
+    RS_CHECK(split_cols(A, ld, nb, "umma_sa", sp, &sa));
     const bool same = (A == B);
     if (same)
         sb = sa;
     else
-        RS_CHECK(split_cols(B, ld, nb, "umma_sb", &sb));
+        RS_CHECK(split_cols(B, ld, nb, "umma_sb", sp, &sb));
     if (a_split) *a_split = sa;
-    return gram_from_slices(sa, sb, same, nb, alpha, symmetrize, nterms, C);
+    return gram_from_slices(sa, sb, same, nb, alpha, symmetrize, sp, C);
 }
 
 template <typename TI>
-static int gram_pair(const TI* psi, const TI* hpsi, long ld, int nb, double alpha, int nterms, double* S, double* H,
+static int gram_pair(const TI* psi, const TI* hpsi, long ld, int nb, double alpha, int mode, double* S, double* H,
                      const void** psi_split) {
-    __nv_bfloat16 *sa = nullptr, *sb = nullptr;
-    RS_CHECK(split_cols(psi, ld, nb, "umma_sa", &sa));
-    RS_CHECK(split_cols(hpsi, ld, nb, "umma_sb", &sb));
-    if (psi_split) *psi_split = sa;
-    RS_CHECK(gram_from_slices(sa, sa, true, nb, alpha, 0, nterms, S));
+    const Split sp = mode_split(mode);
+    void *sa = nullptr, *sb = nullptr;
+    RS_CHECK(split_cols(psi, ld, nb, "umma_sa", sp, &sa));
+    RS_CHECK(split_cols(hpsi, ld, nb, "umma_sb", sp, &sb));
+    if (psi_split) *psi_split = sp.tf32 ? nullptr : sa;  // TF32 rotations split psi transposed
+    RS_CHECK(gram_from_slices(sa, sa, true, nb, alpha, 0, sp, S));
     // psi^T (H psi) is symmetric: the upper tile pairs, the diagonal tiles
     // symmetrised (subspace_mate_sl likewise forms one triangle)
-    return gram_from_slices(sa, sb, false, nb, alpha, 1, nterms, H, true);
+    return gram_from_slices(sa, sb, false, nb, alpha, 1, sp, H, true);
 }
 
-int gram_mixed_pair(const double* psi, const double* hpsi, long ld, int nb, double alpha, int nterms, double* S,
+int gram_mixed_pair(const double* psi, const double* hpsi, long ld, int nb, double alpha, int mode, double* S,
                     double* H, const void** psi_split) {
-    return gram_pair<double>(psi, hpsi, ld, nb, alpha, nterms, S, H, psi_split);
+    return gram_pair<double>(psi, hpsi, ld, nb, alpha, mode, S, H, psi_split);
 }
 
-int gram_mixed_pair(const float* psi, const float* hpsi, long ld, int nb, double alpha, int nterms, double* S,
+int gram_mixed_pair(const float* psi, const float* hpsi, long ld, int nb, double alpha, int mode, double* S,
                     double* H, const void** psi_split) {
-    return gram_pair<float>(psi, hpsi, ld, nb, alpha, nterms, S, H, psi_split);
+    return gram_pair<float>(psi, hpsi, ld, nb, alpha, mode, S, H, psi_split);
 }
 
 // The A operand of a rotation: slices[s][n][m] = term s of V(m, n), K = m
 // padded to mbk with zeros.
-static int split_v(const double* V, int nb, int ldv, int mbk, UmmaMaps* maps) {
+static int split_v(const double* V, int nb, int ldv, int mbk, Split sp, UmmaMaps* maps) {
     Context& c = ctx();
+    if (sp.tf32) {
+        uint32_t* sv = nullptr;
+        RS_CHECK(workspace_t("umma_sv", 2 * (size_t)nb * mbk, &sv));
+        launch(k_split_small_tf32, div_up((long)nb * mbk, 256), 256, 0, c.stream, V, nb, ldv, mbk, sv);
+        RS_LAUNCH();
+        return map3(&maps->a, sv, mbk, nb, UB_M, true);
+    }
     __nv_bfloat16* sv = nullptr;
     RS_CHECK(workspace_t("umma_sv", 3 * (size_t)nb * mbk, &sv));
     launch(k_split_small, div_up((long)nb * mbk, 256), 256, 0, c.stream, V, nb, ldv, mbk, sv);
@@ -552,9 +660,10 @@ static int split_v(const double* V, int nb, int ldv, int mbk, UmmaMaps* maps) {
     return map3(&maps->a, sv, mbk, nb, UB_M);
 }
 
-static UmmaArgs rotate_args(long ml, int nb, int mbk, double* out, long ld) {
+static UmmaArgs rotate_args(long ml, int nb, int mbk, double* out, long ld, bool tf32) {
     UmmaArgs g{};
-    g.kblocks = (mbk + UB_K - 1) / UB_K;
+    const int uke = tf32 ? UB_KB / 4 : UB_K;
+    g.kblocks = (mbk + uke - 1) / uke;
     g.ntm = (nb + UB_M - 1) / UB_M;
     g.ntn = (int)((ml + 255) / 256);
     g.out = out;
@@ -566,11 +675,13 @@ static UmmaArgs rotate_args(long ml, int nb, int mbk, double* out, long ld) {
 }
 
 template <bool BMN>
-static int launch_rotate(const UmmaMaps& maps, const UmmaArgs& g, int nterms) {
+static int launch_rotate(const UmmaMaps& maps, const UmmaArgs& g, Split sp) {
     Context& c = ctx();
     const int sms = c.num_sms > 0 ? c.num_sms : 148;
     const dim3 grid((unsigned)std::min(g.ntm * g.ntn, sms));
-    if (nterms == 3) return launch_umma<256, 3, 3, false, BMN>(maps, g, grid);
+    if constexpr (!BMN)
+        if (sp.tf32) return launch_umma<256, 2, 3, false, false, true>(maps, g, grid);
+    if (sp.terms == 3) return launch_umma<256, 3, 3, false, BMN>(maps, g, grid);
     return launch_umma<256, 2, 3, false, BMN>(maps, g, grid);
 }
 
@@ -579,7 +690,7 @@ static int launch_rotate(const UmmaMaps& maps, const UmmaArgs& g, int nterms) {
 // index as (32, ML / 32) so that one box is BN / 32 groups of 32 grid values
 // x UB_K bands.  Returns RSDFT_EUNSUP when that view is not available.
 static int rotate_from_split(const __nv_bfloat16* sp, double* out, long ld, int nb, const double* V, int ldv,
-                             int nterms) {
+                             Split spl) {
     Context& c = ctx();
     const long ml = c.ml;
     if (ml % 32 != 0) return RSDFT_EUNSUP;
@@ -589,40 +700,51 @@ static int rotate_from_split(const __nv_bfloat16* sp, double* out, long ld, int 
     const unsigned int box[4] = {32u, (unsigned)UB_K, 256u / 32u, 1u};
     if (encode_tmap_4d_swz64(&maps.b, sp, dims, strides, box) != RSDFT_OK) return RSDFT_EUNSUP;
     const int mbk = (nb + 7) / 8 * 8;
-    RS_CHECK(split_v(V, nb, ldv, mbk, &maps));
-    return launch_rotate<true>(maps, rotate_args(ml, nb, mbk, out, ld), nterms);
+    RS_CHECK(split_v(V, nb, ldv, mbk, spl, &maps));
+    return launch_rotate<true>(maps, rotate_args(ml, nb, mbk, out, ld, false), spl);
 }
 
 // out (ML x nb, leading dimension ldo) = psi V, V (nb x nb, leading dimension ldv)
 template <typename TI>
-static int rotate(const TI* psi, double* out, long ld, int nb, const double* V, int ldv, int nterms,
+static int rotate(const TI* psi, double* out, long ld, int nb, const double* V, int ldv, int mode,
                   const void* psi_split) {
-    if (psi_split) {
-        const int r = rotate_from_split(static_cast<const __nv_bfloat16*>(psi_split), out, ld, nb, V, ldv, nterms);
+    const Split sp = mode_split(mode);
+    if (psi_split && !sp.tf32) {
+        const int r = rotate_from_split(static_cast<const __nv_bfloat16*>(psi_split), out, ld, nb, V, ldv, sp);
         if (r != RSDFT_EUNSUP) return r;
     }
     // transposed split: slices[s][i][m], K = band index fastest
     Context& c = ctx();
     const long ml = c.ml;
     const int mbk = (nb + 7) / 8 * 8;
-    __nv_bfloat16* st = nullptr;
-    RS_CHECK(workspace_t("umma_st", 3 * (size_t)ml * mbk, &st));
-    launch(k_split_rows<TI>, dim3(div_up(ml, 32), div_up(mbk, 32)), dim3(32, 8), 0, c.stream, psi, ld, nb, ml, mbk, st);
+    void* st = nullptr;
+    const dim3 sg(div_up(ml, 32), div_up(mbk, 32)), sb(32, 8);
+    if (sp.tf32) {
+        uint32_t* t = nullptr;
+        RS_CHECK(workspace_t("umma_st", 2 * (size_t)ml * mbk, &t));
+        launch(k_split_rows_tf32<TI>, sg, sb, 0, c.stream, psi, ld, nb, ml, mbk, t);
+        st = t;
+    } else {
+        __nv_bfloat16* t = nullptr;
+        RS_CHECK(workspace_t("umma_st", 3 * (size_t)ml * mbk, &t));
+        launch(k_split_rows<TI>, sg, sb, 0, c.stream, psi, ld, nb, ml, mbk, t);
+        st = t;
+    }
     RS_LAUNCH();
     UmmaMaps maps;
-    RS_CHECK(split_v(V, nb, ldv, mbk, &maps));
-    RS_CHECK(map3(&maps.b, st, mbk, ml, 256));
-    return launch_rotate<false>(maps, rotate_args(ml, nb, mbk, out, ld), nterms);
+    RS_CHECK(split_v(V, nb, ldv, mbk, sp, &maps));
+    RS_CHECK(map3(&maps.b, st, mbk, ml, 256, sp.tf32));
+    return launch_rotate<false>(maps, rotate_args(ml, nb, mbk, out, ld, sp.tf32), sp);
 }
 
-int rotate_mixed(const double* psi, double* out, long ld, int nb, const double* V, int ldv, int nterms,
+int rotate_mixed(const double* psi, double* out, long ld, int nb, const double* V, int ldv, int mode,
                  const void* psi_split) {
-    return rotate<double>(psi, out, ld, nb, V, ldv, nterms, psi_split);
+    return rotate<double>(psi, out, ld, nb, V, ldv, mode, psi_split);
 }
 
-int rotate_mixed(const float* psi, double* out, long ld, int nb, const double* V, int ldv, int nterms,
+int rotate_mixed(const float* psi, double* out, long ld, int nb, const double* V, int ldv, int mode,
                  const void* psi_split) {
-    return rotate<float>(psi, out, ld, nb, V, ldv, nterms, psi_split);
+    return rotate<float>(psi, out, ld, nb, V, ldv, mode, psi_split);
 }
 
 }  // namespace rsdft

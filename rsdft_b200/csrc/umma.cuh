@@ -1,11 +1,12 @@
 // tcgen05 (5th-generation tensor core) helpers for sm_100a, inline PTX.
 //
-// Conventions: cta_group::1, kind::f16 with BF16 operands and FP32
-// accumulation in tensor memory (TMEM), operands in shared memory with the
-// 64-byte swizzle (8 rows x 64 B atoms), which is the layout a TMA tile load
-// with CU_TENSOR_MAP_SWIZZLE_64B and a 32-element inner box produces: K-major
-// (rows along M/N, 32 K values per row) or, for B, MN-major (rows along K,
-// 32 N values per row).
+// Conventions: cta_group::1, kind::f16 with BF16 operands or kind::tf32 with
+// TF32 operands, FP32 accumulation in tensor memory (TMEM), operands in
+// shared memory with the 64-byte swizzle (8 rows x 64 B atoms), which is the
+// layout a TMA tile load with CU_TENSOR_MAP_SWIZZLE_64B and a 64-byte inner
+// box produces (32 BF16 or 16 TF32 values): K-major (rows along M/N, one
+// 64-byte K block per row) or, for BF16 B, MN-major (rows along K, 32 N
+// values per row).  A K block is two MMAs (K = 16 BF16 / 8 TF32, 32 bytes).
 #pragma once
 
 #include <cstdint>
@@ -48,6 +49,12 @@ __host__ __device__ constexpr uint32_t umma_idesc_bf16(int M, int N, bool b_mn =
            ((uint32_t)(M >> 4) << 24);
 }
 
+// Instruction descriptor, kind::tf32: D = F32, A = B = TF32 (format 2), both
+// K-major.
+__host__ __device__ constexpr uint32_t umma_idesc_tf32(int M, int N) {
+    return (1u << 4) | (2u << 7) | (2u << 10) | ((uint32_t)(N >> 3) << 17) | ((uint32_t)(M >> 4) << 24);
+}
+
 // ------------------------------------------------------------------ TMEM
 __device__ __forceinline__ void tmem_alloc(uint32_t* dst_smem, uint32_t ncols) {
     asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(dst_smem)),
@@ -74,6 +81,19 @@ __device__ __forceinline__ void umma_bf16(uint32_t d_tmem, uint64_t adesc, uint6
         ".reg .pred p;\n"
         "setp.ne.b32 p, %4, 0;\n"
         "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n"
+        "}\n" ::"r"(d_tmem),
+        "l"(adesc), "l"(bdesc), "r"(idesc), "r"(accumulate)
+        : "memory");
+}
+
+// D[tmem] (+)= A[smem] * B[smem]^T with TF32 operands, issued by one thread.
+__device__ __forceinline__ void umma_tf32(uint32_t d_tmem, uint64_t adesc, uint64_t bdesc, uint32_t idesc,
+                                          uint32_t accumulate) {
+    asm volatile(
+        "{\n"
+        ".reg .pred p;\n"
+        "setp.ne.b32 p, %4, 0;\n"
+        "tcgen05.mma.cta_group::1.kind::tf32 [%0], %1, %2, %3, p;\n"
         "}\n" ::"r"(d_tmem),
         "l"(adesc), "l"(bdesc), "r"(idesc), "r"(accumulate)
         : "memory");
