@@ -109,6 +109,29 @@ int rsdft_gpu_sync_to_device(double *unk);
 int rsdft_gpu_hamiltonian(int k, int s, const double *tpsi, double *htpsi, int n1, int n2, int ib1,
                           int ib2);
 
+/* The three operators of hamiltonian, apart, for a caller that splits the
+ * grid over ranks (each rank's context holds its slab extended by halo
+ * planes, and the projector entries of its own points):
+ *   op_local:            htpsi = (T + Vloc(:, s)) tpsi on the z planes
+ *                        [z0, z0 + nz) of the context's grid (other planes
+ *                        of htpsi untouched), kinetic and local potential
+ *                        only (replaces op_kinetic + op_localpot,
+ *                        hamiltonian_module.f90:42,50).  The stencil wraps
+ *                        periodically in z over the context's n3 planes, so
+ *                        on a slab extended by Md halo planes either side
+ *                        (z0 = Md, nz = n3 - 2 Md) it reads no wrapped plane;
+ *   op_nonlocal_project: uvunk(lma, b) = iuV dV sum_j uV(j, lma) tpsi(JJP(j), b)
+ *                        over the context's projector entries, uvunk
+ *                        (nzlma, nb) column-major (ps_nloc2_op_module.f90:
+ *                        161-175: a rank's partial sums, which the ranks add
+ *                        up as :179-250 do);
+ *   op_nonlocal_add:     htpsi(JJP(j), b) += uV(j, lma) uvunk(lma, b)
+ *                        (ps_nloc2_op_module.f90:255-263).
+ * tpsi/htpsi as for rsdft_gpu_hamiltonian (ld >= ML); uvunk host or device. */
+int rsdft_gpu_op_local(int s, const double *tpsi, double *htpsi, long ld, int nb, int z0, int nz);
+int rsdft_gpu_op_nonlocal_project(const double *tpsi, long ld, int nb, double *uvunk);
+int rsdft_gpu_op_nonlocal_add(const double *uvunk, double *htpsi, long ld, int nb);
+
 /* Capacity, in doubles (4 MiB), of the static scratch of
  * rsdft_gpu_hamiltonian_noalloc. */
 #define RSDFT_NOALLOC_SCRATCH_VALUES 524288L
@@ -166,6 +189,34 @@ int rsdft_gpu_subspace_solv(int mb, const double *hsub, int ldh, double *esp, do
 /* unk <- unk * Vsub.  (replaces subspace_rotv_sl(k,s),
  * subspace_rotv_sl_module.f90:24-135) */
 int rsdft_gpu_subspace_rotv(int k, int s, double *unk, long ld, int mb, const double *vsub, int ldv);
+
+/* Pieces of gram_schmidt_t / subspace_diag_la for a caller that splits the
+ * grid over ranks: each rank forms its partial sums over its own points, the
+ * ranks add them up (mpi_allreduce over comm_grid), and every rank solves the
+ * small problem redundantly and rotates its own rows.
+ *   gram:             C(m, n) = alpha a^T b over `rows` rows (leading
+ *                     dimension ld; sym = 1 returns the symmetric part of a
+ *                     square product), on the FP64 tensor pipe (replaces the
+ *                     dgemm before gram_schmidt_t_module.f90:194 and the
+ *                     dsyr2k of subspace_diag_la_module.f90:96);
+ *   overlap_cholesky: S = R^T R, rinv = R^-1 (upper, lower triangle zero),
+ *                     kappa = (max diag R / min diag R)^2, the conditioning
+ *                     gate of the one-pass step (the normalisations of
+ *                     gram_schmidt_t_module.f90:84-316 in triangular form);
+ *   rr_reduced:       R^-T Hsub R^-1 = V diag(esp) V^T, w = R^-1 V (Hsub's
+ *                     upper triangle read), the eigenproblem after
+ *                     subspace_diag_la_module.f90:122 and the rotation
+ *                     matrix of :200 composed with the Gram-Schmidt one.
+ * Matrices host or device, column-major. */
+int rsdft_gpu_gram(const double *a, const double *b, long ld, long rows, int m, int n, double alpha, int sym,
+                   double *c, int ldc);
+int rsdft_gpu_overlap_cholesky(int mb, const double *s, int lds, double *rinv, int ldr, double *kappa);
+int rsdft_gpu_rr_reduced(int mb, const double *rinv, int ldr, const double *hsub, int ldh, double *esp,
+                         double *w, int ldw);
+/* unk(1:rows, 1:mb) <- unk * v for device (or registered) unk with leading
+ * dimension ld: the rotation of subspace_rotv_sl_module.f90:92 on a rank's
+ * own rows. */
+int rsdft_gpu_rotate(double *unk, long ld, long rows, int mb, const double *v, int ldv);
 
 /* Rayleigh-Ritz in span(unk): Hsub = dV/2 (psi^T H psi + (H psi)^T psi),
  * eigen-decomposition, rotation; esp(MB) out.  (replaces subspace_diag(k,s)

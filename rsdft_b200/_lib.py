@@ -32,6 +32,13 @@ SIGNATURES = {
     "rsdft_gpu_sync_to_host": (_c_int, [_vp]),
     "rsdft_gpu_sync_to_device": (_c_int, [_vp]),
     "rsdft_gpu_hamiltonian": (_c_int, [_c_int, _c_int, _vp, _vp, _c_int, _c_int, _c_int, _c_int]),
+    "rsdft_gpu_op_local": (_c_int, [_c_int, _vp, _vp, _c_long, _c_int, _c_int, _c_int]),
+    "rsdft_gpu_op_nonlocal_project": (_c_int, [_vp, _c_long, _c_int, _vp]),
+    "rsdft_gpu_op_nonlocal_add": (_c_int, [_vp, _vp, _c_long, _c_int]),
+    "rsdft_gpu_gram": (_c_int, [_vp, _vp, _c_long, _c_long, _c_int, _c_int, _c_double, _c_int, _vp, _c_int]),
+    "rsdft_gpu_overlap_cholesky": (_c_int, [_c_int, _vp, _c_int, _vp, _c_int, _vp]),
+    "rsdft_gpu_rr_reduced": (_c_int, [_c_int, _vp, _c_int, _vp, _c_int, _vp, _vp, _c_int]),
+    "rsdft_gpu_rotate": (_c_int, [_vp, _c_long, _c_long, _c_int, _vp, _c_int]),
     "rsdft_gpu_hamiltonian_noalloc": (_c_int, [_c_int, _c_int, _vp, _vp, _c_int, _c_int, _c_int, _c_int]),
     "rsdft_gpu_conjugate_gradient": (_c_int, [_c_int, _c_int, _c_int, _c_int, _c_int, _vp, _vp, _vp, _c_int,
                                               _c_int, _c_int, _c_int]),

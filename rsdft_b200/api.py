@@ -30,6 +30,7 @@ with strides ``(1, ML)`` (``fortran_empty`` makes one).  Every call raises
 """
 from __future__ import annotations
 
+import ctypes
 import os
 
 import numpy as np
@@ -207,6 +208,51 @@ class RsdftGpu:
     def hamiltonian(self, k, s, tpsi, htpsi, n1, n2, ib1, ib2) -> None:
         _lib.call("rsdft_gpu_hamiltonian", k, s, _ptr(tpsi, name="tpsi"), _ptr(htpsi, name="htpsi"), n1, n2, ib1,
                   ib2)
+
+    def op_local(self, s, tpsi, htpsi, z0=0, nz=None) -> None:
+        """(T + Vloc) tpsi on z planes [z0, z0 + nz): op_kinetic + op_localpot
+        (hamiltonian_module.f90:42,50)."""
+        if nz is None:
+            nz = int(self.cell.ngrid[2]) - z0
+        _lib.call("rsdft_gpu_op_local", s, _ptr(tpsi, name="tpsi"), _ptr(htpsi, name="htpsi"), _ld(tpsi),
+                  tpsi.shape[1], z0, nz)
+
+    def op_nonlocal_project(self, tpsi, uvunk) -> None:
+        """uvunk (nzlma, nb) = iuV dV <uV|tpsi> over this context's projector
+        entries (ps_nloc2_op_module.f90:161-175)."""
+        _lib.call("rsdft_gpu_op_nonlocal_project", _ptr(tpsi, name="tpsi"), _ld(tpsi), tpsi.shape[1],
+                  _ptr(uvunk, name="uvunk"))
+
+    def op_nonlocal_add(self, uvunk, htpsi) -> None:
+        """htpsi += uV uvunk at this context's projector points
+        (ps_nloc2_op_module.f90:255-263)."""
+        _lib.call("rsdft_gpu_op_nonlocal_add", _ptr(uvunk, name="uvunk"), _ptr(htpsi, name="htpsi"), _ld(htpsi),
+                  htpsi.shape[1])
+
+    def gram(self, a, b, cmat, *, alpha=1.0, sym=0) -> None:
+        """cmat(m, n) = alpha a^T b over a's rows (the partial sum of one grid
+        slab; gram_schmidt_t_module.f90:187, subspace_diag_la_module.f90:96)."""
+        if a.shape[0] != b.shape[0] or _ld(a) != _ld(b):
+            raise ValueError("gram: a and b need the same rows and leading dimension")
+        _lib.call("rsdft_gpu_gram", _ptr(a, name="a"), _ptr(b, name="b"), _ld(a), a.shape[0], a.shape[1],
+                  b.shape[1], float(alpha), int(sym), _ptr(cmat, name="c"), _ld(cmat))
+
+    def overlap_cholesky(self, smat, rinv) -> float:
+        """rinv = R^-1 for smat = R^T R; returns (max diag R / min diag R)^2."""
+        kappa = ctypes.c_double(0.0)
+        _lib.call("rsdft_gpu_overlap_cholesky", smat.shape[0], _ptr(smat, name="s"), _ld(smat),
+                  _ptr(rinv, name="rinv"), _ld(rinv), ctypes.addressof(kappa))
+        return float(kappa.value)
+
+    def rr_reduced(self, rinv, hsub, esp, w) -> None:
+        """R^-T Hsub R^-1 = V diag(esp) V^T and w = R^-1 V."""
+        _lib.call("rsdft_gpu_rr_reduced", hsub.shape[0], _ptr(rinv, name="rinv"), _ld(rinv),
+                  _ptr(hsub, name="hsub"), _ld(hsub), _ptr(esp, name="esp"), _ptr(w, name="w"), _ld(w))
+
+    def rotate(self, unk, v) -> None:
+        """unk <- unk v on unk's rows (device tensor, any leading dimension)."""
+        _lib.call("rsdft_gpu_rotate", _ptr(unk, name="unk"), _ld(unk), unk.shape[0], unk.shape[1],
+                  _ptr(v, name="v"), _ld(v))
 
     def hamiltonian_noalloc(self, k, s, tpsi, htpsi, n1, n2, ib1, ib2) -> None:
         """H psi without any device allocation (static 4 MiB scratch; see the

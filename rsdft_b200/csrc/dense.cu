@@ -79,6 +79,34 @@ static int check_info(int* dinfo, const char* what) {
     return RSDFT_OK;
 }
 
+// S (nb x nb) = R^T R in place: the upper triangle becomes R
+static int potrf_upper(double* S, int nb, int* dinfo, const char* what) {
+    Context& c = ctx();
+    int lwork = 0;
+    RS_SOLVER(cusolverDnDpotrf_bufferSize(c.solver, CUBLAS_FILL_MODE_UPPER, nb, S, nb, &lwork));
+    double* work = nullptr;
+    RS_CHECK(workspace_t("gs_potrf", (size_t)lwork + 1, &work));
+    RS_SOLVER(cusolverDnDpotrf(c.solver, CUBLAS_FILL_MODE_UPPER, nb, S, nb, work, lwork, dinfo));
+    return check_info(dinfo, what);
+}
+
+// R (upper triangle of S) -> R^-1 in place, the lower triangle zeroed
+static int trtri_upper(double* S, int nb, int* dinfo, const char* what) {
+    Context& c = ctx();
+    size_t dws = 0, hws = 0;
+    RS_SOLVER(cusolverDnXtrtri_bufferSize(c.solver, CUBLAS_FILL_MODE_UPPER, CUBLAS_DIAG_NON_UNIT, nb, CUDA_R_64F, S,
+                                          nb, &dws, &hws));
+    void* dw = nullptr;
+    RS_CHECK(workspace("gs_trtri", dws + 16, &dw));
+    char* hw = host_workspace(hws + 16);
+    RS_SOLVER(cusolverDnXtrtri(c.solver, CUBLAS_FILL_MODE_UPPER, CUBLAS_DIAG_NON_UNIT, nb, CUDA_R_64F, S, nb, dw,
+                               dws, hw, hws, dinfo));
+    RS_CHECK(check_info(dinfo, what));
+    launch(k_zero_lower, dim3(div_up(nb, 128), nb), 128, 0, c.stream, S, nb, nb);
+    RS_LAUNCH();
+    return RSDFT_OK;
+}
+
 // One CholeskyQR pass in FP64: S = dV psi^T psi = R^T R, out = psi R^-1.
 // R^-1 comes from a triangular inverse of the small factor, so the tall
 // product is one DGEMM (in and out are different buffers).
@@ -89,23 +117,8 @@ static int cholqr_pass(const double* psi, double* out, long ld, int nb, double* 
         RS_CHECK(gemm_tn_splitk(psi, psi, ld, nb, nb, c.dV, 0, S));
     else
         RS_CHECK(gram_mixed(psi, psi, ld, nb, c.dV, 0, mode, S, &split));
-    int lwork = 0;
-    RS_SOLVER(cusolverDnDpotrf_bufferSize(c.solver, CUBLAS_FILL_MODE_UPPER, nb, S, nb, &lwork));
-    double* work = nullptr;
-    RS_CHECK(workspace_t("gs_potrf", (size_t)lwork + 1, &work));
-    RS_SOLVER(cusolverDnDpotrf(c.solver, CUBLAS_FILL_MODE_UPPER, nb, S, nb, work, lwork, dinfo));
-    RS_CHECK(check_info(dinfo, "gram_schmidt: overlap Cholesky"));
-    size_t dws = 0, hws = 0;
-    RS_SOLVER(cusolverDnXtrtri_bufferSize(c.solver, CUBLAS_FILL_MODE_UPPER, CUBLAS_DIAG_NON_UNIT, nb, CUDA_R_64F, S,
-                                          nb, &dws, &hws));
-    void* dw = nullptr;
-    RS_CHECK(workspace("gs_trtri", dws + 16, &dw));
-    char* hw = host_workspace(hws + 16);
-    RS_SOLVER(cusolverDnXtrtri(c.solver, CUBLAS_FILL_MODE_UPPER, CUBLAS_DIAG_NON_UNIT, nb, CUDA_R_64F, S, nb, dw,
-                               dws, hw, hws, dinfo));
-    RS_CHECK(check_info(dinfo, "gram_schmidt: triangular inverse"));
-    launch(k_zero_lower, dim3(div_up(nb, 128), nb), 128, 0, c.stream, S, nb, nb);
-    RS_LAUNCH();
+    RS_CHECK(potrf_upper(S, nb, dinfo, "gram_schmidt: overlap Cholesky"));
+    RS_CHECK(trtri_upper(S, nb, dinfo, "gram_schmidt: triangular inverse"));
     if (mode == RSDFT_MODE_FP64)
         RS_CHECK(dmma_gemm(false, c.ml, nb, nb, 1.0, psi, ld, S, nb, 0.0, out, ld));
     else
@@ -166,6 +179,16 @@ int subspace_diag_device(double* psi, long ld, int mb, int spin, double* esp, in
     RS_CUDA(cudaMemcpy2DAsync(psi, ld * sizeof(double), hpsi, ld * sizeof(double), c.ml * sizeof(double), mb,
                               cudaMemcpyDeviceToDevice, c.stream));
     return RSDFT_OK;
+}
+
+// The reduced eigenproblem of the fused Rayleigh-Ritz step: with Rinv = R^-1
+// (upper) and H the symmetric Hsub, Hr = R^-T H R^-1 (T = H R^-1, then
+// H = R^-T T), Hr = V diag(esp) V^T, T = R^-1 V.  H is overwritten.
+static int rr_reduced(const double* Rinv, double* H, double* T, int mb, double* esp, const char* what) {
+    RS_CHECK(dmma_gemm(false, mb, mb, mb, 1.0, H, mb, Rinv, mb, 0.0, T, mb));
+    RS_CHECK(dmma_gemm(true, mb, mb, mb, 1.0, Rinv, mb, T, mb, 0.0, H, mb));
+    RS_CHECK(syevd(H, mb, esp, CUBLAS_FILL_MODE_UPPER, what));
+    return dmma_gemm(false, mb, mb, mb, 1.0, Rinv, mb, H, mb, 0.0, T, mb);
 }
 
 // min and max of the diagonal of an n x n matrix (one block)
@@ -233,12 +256,7 @@ int orth_subspace_diag_device(double* psi, long ld, int mb, int spin, double* es
     } else {
         RS_CHECK(gram_mixed_pair(psi, hpsi, ld, mb, c.dV, mode, S, H, &split));
     }
-    int lwork = 0;
-    RS_SOLVER(cusolverDnDpotrf_bufferSize(c.solver, CUBLAS_FILL_MODE_UPPER, mb, S, mb, &lwork));
-    double* work = nullptr;
-    RS_CHECK(workspace_t("gs_potrf", (size_t)lwork + 1, &work));
-    RS_SOLVER(cusolverDnDpotrf(c.solver, CUBLAS_FILL_MODE_UPPER, mb, S, mb, work, lwork, dinfo));
-    RS_CHECK(check_info(dinfo, "orth_subspace_diag: overlap Cholesky"));
+    RS_CHECK(potrf_upper(S, mb, dinfo, "orth_subspace_diag: overlap Cholesky"));
     launch(k_diag_minmax, 1, 256, 0, c.stream, S, mb, mb, mm);
     RS_LAUNCH();
     double hmm[2] = {0.0, 0.0};
@@ -248,22 +266,8 @@ int orth_subspace_diag_device(double* psi, long ld, int mb, int spin, double* es
         RS_CHECK(gram_schmidt_device(psi, ld, mb, mode));
         return subspace_diag_device(psi, ld, mb, spin, esp, mode);
     }
-    size_t dws = 0, hws = 0;
-    RS_SOLVER(cusolverDnXtrtri_bufferSize(c.solver, CUBLAS_FILL_MODE_UPPER, CUBLAS_DIAG_NON_UNIT, mb, CUDA_R_64F, S,
-                                          mb, &dws, &hws));
-    void* dw = nullptr;
-    RS_CHECK(workspace("gs_trtri", dws + 16, &dw));
-    char* hw = host_workspace(hws + 16);
-    RS_SOLVER(cusolverDnXtrtri(c.solver, CUBLAS_FILL_MODE_UPPER, CUBLAS_DIAG_NON_UNIT, mb, CUDA_R_64F, S, mb, dw,
-                               dws, hw, hws, dinfo));
-    RS_CHECK(check_info(dinfo, "orth_subspace_diag: triangular inverse"));
-    launch(k_zero_lower, dim3(div_up(mb, 128), mb), 128, 0, c.stream, S, mb, mb);
-    RS_LAUNCH();
-    // Hr = R^-T H R^-1 (T = H R^-1, then H = R^-T T), eigenpairs, T = R^-1 V
-    RS_CHECK(dmma_gemm(false, mb, mb, mb, 1.0, H, mb, S, mb, 0.0, T, mb));
-    RS_CHECK(dmma_gemm(true, mb, mb, mb, 1.0, S, mb, T, mb, 0.0, H, mb));
-    RS_CHECK(syevd(H, mb, esp, CUBLAS_FILL_MODE_UPPER, "orth_subspace_diag: syevd"));
-    RS_CHECK(dmma_gemm(false, mb, mb, mb, 1.0, S, mb, H, mb, 0.0, T, mb));
+    RS_CHECK(trtri_upper(S, mb, dinfo, "orth_subspace_diag: triangular inverse"));
+    RS_CHECK(rr_reduced(S, H, T, mb, esp, "orth_subspace_diag: syevd"));
     if (mode == RSDFT_MODE_FP64) {
         RS_CHECK(dmma_gemm(false, c.ml, mb, mb, 1.0, psi, ld, T, mb, 0.0, hpsi, ld));
         RS_CUDA(cudaMemcpy2DAsync(psi, ld * sizeof(double), hpsi, ld * sizeof(double), c.ml * sizeof(double), mb,
@@ -298,12 +302,7 @@ int orth_subspace_diag_f32(const float* x32, const float* hx, double* psi, long 
     }
     const void* split = nullptr;
     RS_CHECK(gram_mixed_pair(x32, h32, ld, mb, c.dV, mode, S, H, &split));
-    int lwork = 0;
-    RS_SOLVER(cusolverDnDpotrf_bufferSize(c.solver, CUBLAS_FILL_MODE_UPPER, mb, S, mb, &lwork));
-    double* work = nullptr;
-    RS_CHECK(workspace_t("gs_potrf", (size_t)lwork + 1, &work));
-    RS_SOLVER(cusolverDnDpotrf(c.solver, CUBLAS_FILL_MODE_UPPER, mb, S, mb, work, lwork, dinfo));
-    RS_CHECK(check_info(dinfo, "eigensolver_sweep: overlap Cholesky"));
+    RS_CHECK(potrf_upper(S, mb, dinfo, "eigensolver_sweep: overlap Cholesky"));
     launch(k_diag_minmax, 1, 256, 0, c.stream, S, mb, mb, mm);
     RS_LAUNCH();
     double hmm[2] = {0.0, 0.0};
@@ -315,21 +314,8 @@ int orth_subspace_diag_f32(const float* x32, const float* hx, double* psi, long 
         RS_CHECK(gram_schmidt_device(psi, ld, mb, mode));
         return subspace_diag_device(psi, ld, mb, spin, esp, mode);
     }
-    size_t dws = 0, hws = 0;
-    RS_SOLVER(cusolverDnXtrtri_bufferSize(c.solver, CUBLAS_FILL_MODE_UPPER, CUBLAS_DIAG_NON_UNIT, mb, CUDA_R_64F, S,
-                                          mb, &dws, &hws));
-    void* dw = nullptr;
-    RS_CHECK(workspace("gs_trtri", dws + 16, &dw));
-    char* hw = host_workspace(hws + 16);
-    RS_SOLVER(cusolverDnXtrtri(c.solver, CUBLAS_FILL_MODE_UPPER, CUBLAS_DIAG_NON_UNIT, mb, CUDA_R_64F, S, mb, dw,
-                               dws, hw, hws, dinfo));
-    RS_CHECK(check_info(dinfo, "eigensolver_sweep: triangular inverse"));
-    launch(k_zero_lower, dim3(div_up(mb, 128), mb), 128, 0, c.stream, S, mb, mb);
-    RS_LAUNCH();
-    RS_CHECK(dmma_gemm(false, mb, mb, mb, 1.0, H, mb, S, mb, 0.0, T, mb));
-    RS_CHECK(dmma_gemm(true, mb, mb, mb, 1.0, S, mb, T, mb, 0.0, H, mb));
-    RS_CHECK(syevd(H, mb, esp, CUBLAS_FILL_MODE_UPPER, "eigensolver_sweep: syevd"));
-    RS_CHECK(dmma_gemm(false, mb, mb, mb, 1.0, S, mb, H, mb, 0.0, T, mb));
+    RS_CHECK(trtri_upper(S, mb, dinfo, "eigensolver_sweep: triangular inverse"));
+    RS_CHECK(rr_reduced(S, H, T, mb, esp, "eigensolver_sweep: syevd"));
     return rotate_mixed(x32, psi, ld, mb, T, mb, mode, split);
 }
 
@@ -460,6 +446,110 @@ int rsdft_gpu_subspace_rotv(int k, int s, double* unk, long ld, int mb, const do
     RS_CUDA(cudaMemcpy2DAsync(d, ld * sizeof(double), tmp, ld * sizeof(double), c.ml * sizeof(double), mb,
                               cudaMemcpyDeviceToDevice, c.stream));
     RS_CHECK(wf_release(unk, d, ld, mb, st));
+    return RSDFT_OK;
+}
+
+int rsdft_gpu_gram(const double* a, const double* b, long ld, long rows, int m, int n, double alpha, int sym,
+                   double* cmat, int ldc) {
+    RS_ENTRY();
+    RS_CHECK(require_init());
+    Context& c = ctx();
+    if (!a || !b || !cmat || rows < 1 || ld < rows || m < 1 || n < 1 || ldc < m || (sym && m != n)) {
+        set_error("gram: bad arguments (rows=%ld ld=%ld m=%d n=%d ldc=%d sym=%d)", rows, ld, m, n, ldc, sym);
+        return RSDFT_EINVAL;
+    }
+    // the span each operand covers: its last column ends at row `rows`
+    void *da = nullptr, *db = nullptr;
+    RS_CHECK(stage_in(a, sizeof(double) * ((size_t)ld * (m - 1) + rows), "gram_a", &da));
+    RS_CHECK(stage_in(b, sizeof(double) * ((size_t)ld * (n - 1) + rows), "gram_b", &db));
+    double* C = nullptr;
+    RS_CHECK(workspace_t("gram_c", (size_t)m * n, &C));
+    RS_CHECK(dmma_gram((const double*)da, (const double*)db, ld, rows, m, n, alpha, sym, C, m));
+    RS_CUDA(cudaMemcpy2DAsync(cmat, (size_t)ldc * sizeof(double), C, (size_t)m * sizeof(double),
+                              (size_t)m * sizeof(double), n, cudaMemcpyDefault, c.stream));
+    RS_CUDA(cudaStreamSynchronize(c.stream));
+    return RSDFT_OK;
+}
+
+int rsdft_gpu_overlap_cholesky(int mb, const double* s, int lds, double* rinv, int ldr, double* kappa) {
+    RS_ENTRY();
+    RS_CHECK(require_init());
+    Context& c = ctx();
+    if (mb < 1 || lds < mb || ldr < mb || !s || !rinv) {
+        set_error("overlap_cholesky: bad arguments");
+        return RSDFT_EINVAL;
+    }
+    double *S = nullptr, *mm = nullptr;
+    int* dinfo = nullptr;
+    RS_CHECK(workspace_t("slab_S", (size_t)mb * mb, &S));
+    RS_CHECK(workspace_t("osd_minmax", 2, &mm));
+    RS_CHECK(workspace_t("gs_info", 4, &dinfo));
+    RS_CUDA(cudaMemcpy2DAsync(S, (size_t)mb * sizeof(double), s, (size_t)lds * sizeof(double),
+                              (size_t)mb * sizeof(double), mb, cudaMemcpyDefault, c.stream));
+    RS_CHECK(potrf_upper(S, mb, dinfo, "overlap_cholesky: Cholesky"));
+    launch(k_diag_minmax, 1, 256, 0, c.stream, S, mb, mb, mm);
+    RS_LAUNCH();
+    double hmm[2] = {0.0, 0.0};
+    RS_CUDA(cudaMemcpyAsync(hmm, mm, sizeof(hmm), cudaMemcpyDeviceToHost, c.stream));
+    RS_CHECK(trtri_upper(S, mb, dinfo, "overlap_cholesky: triangular inverse"));
+    RS_CUDA(cudaMemcpy2DAsync(rinv, (size_t)ldr * sizeof(double), S, (size_t)mb * sizeof(double),
+                              (size_t)mb * sizeof(double), mb, cudaMemcpyDefault, c.stream));
+    RS_CUDA(cudaStreamSynchronize(c.stream));
+    if (kappa) *kappa = hmm[0] > 0.0 ? (hmm[1] / hmm[0]) * (hmm[1] / hmm[0]) : INFINITY;
+    return RSDFT_OK;
+}
+
+int rsdft_gpu_rr_reduced(int mb, const double* rinv, int ldr, const double* hsub, int ldh, double* esp, double* w,
+                         int ldw) {
+    RS_ENTRY();
+    RS_CHECK(require_init());
+    Context& c = ctx();
+    if (mb < 1 || ldr < mb || ldh < mb || ldw < mb || !rinv || !hsub || !esp || !w) {
+        set_error("rr_reduced: bad arguments");
+        return RSDFT_EINVAL;
+    }
+    double *R = nullptr, *H = nullptr, *T = nullptr, *E = nullptr;
+    RS_CHECK(workspace_t("slab_S", (size_t)mb * mb, &R));
+    RS_CHECK(workspace_t("sub_H", (size_t)mb * mb, &H));
+    RS_CHECK(workspace_t("osd_T", (size_t)mb * mb, &T));
+    RS_CHECK(workspace_t("slab_esp", (size_t)mb, &E));
+    RS_CUDA(cudaMemcpy2DAsync(R, (size_t)mb * sizeof(double), rinv, (size_t)ldr * sizeof(double),
+                              (size_t)mb * sizeof(double), mb, cudaMemcpyDefault, c.stream));
+    RS_CUDA(cudaMemcpy2DAsync(H, (size_t)mb * sizeof(double), hsub, (size_t)ldh * sizeof(double),
+                              (size_t)mb * sizeof(double), mb, cudaMemcpyDefault, c.stream));
+    RS_CHECK(rr_reduced(R, H, T, mb, E, "rr_reduced: syevd"));
+    RS_CUDA(cudaMemcpy2DAsync(w, (size_t)ldw * sizeof(double), T, (size_t)mb * sizeof(double),
+                              (size_t)mb * sizeof(double), mb, cudaMemcpyDefault, c.stream));
+    RS_CUDA(cudaMemcpyAsync(esp, E, sizeof(double) * mb, cudaMemcpyDefault, c.stream));
+    RS_CUDA(cudaStreamSynchronize(c.stream));
+    return RSDFT_OK;
+}
+
+int rsdft_gpu_rotate(double* unk, long ld, long rows, int mb, const double* v, int ldv) {
+    RS_ENTRY();
+    RS_CHECK(require_init());
+    Context& c = ctx();
+    if (!unk || !v || rows < 1 || ld < rows || mb < 1 || ldv < mb) {
+        set_error("rotate: bad arguments (rows=%ld ld=%ld mb=%d ldv=%d)", rows, ld, mb, ldv);
+        return RSDFT_EINVAL;
+    }
+    void* du = nullptr;
+    const size_t span = sizeof(double) * ((size_t)ld * (mb - 1) + rows);
+    const int r = resolve(unk, span, &du);
+    if (r < 0) return r;
+    if (!r) {
+        set_error("rotate: unk must be device memory or a registered array");
+        return RSDFT_EINVAL;
+    }
+    double *V = nullptr, *tmp = nullptr;
+    RS_CHECK(workspace_t("rotv_V", (size_t)mb * mb, &V));
+    RS_CHECK(workspace_t("rot_tmp", (size_t)rows * mb, &tmp));
+    RS_CUDA(cudaMemcpy2DAsync(V, (size_t)mb * sizeof(double), v, (size_t)ldv * sizeof(double),
+                              (size_t)mb * sizeof(double), mb, cudaMemcpyDefault, c.stream));
+    double* d = static_cast<double*>(du);
+    RS_CHECK(dmma_gemm(false, rows, mb, mb, 1.0, d, ld, V, mb, 0.0, tmp, rows));
+    RS_CUDA(cudaMemcpy2DAsync(d, ld * sizeof(double), tmp, rows * sizeof(double), rows * sizeof(double), mb,
+                              cudaMemcpyDeviceToDevice, c.stream));
     return RSDFT_OK;
 }
 

@@ -131,6 +131,7 @@ struct StencilArgs {
     long ld;
     int n1, n2, n3;
     int zlen, nzc;
+    int z0, nzo;  // output planes [z0, z0 + nzo) (0, n3 when nzo = 0)
     const T* vloc;
     const int* pt_ptr;
     const int* pt_lma;
@@ -162,8 +163,8 @@ __global__ void __launch_bounds__(TX * 16) k_stencil(StencilArgs<T> a, StencilCo
     const long plane = (long)n1 * n2;
     const T* __restrict__ p = a.psi + (long)band * a.ld;
     T* __restrict__ h = a.hpsi + (long)band * a.ld;
-    const int zs = zc * a.zlen;
-    const int ze = min(zs + a.zlen, n3);
+    const int zs = a.z0 + zc * a.zlen;
+    const int ze = min(zs + a.zlen, a.z0 + a.nzo);
     const long col = act ? (long)x + (long)n1 * y : 0;
 
     T cx[MD], cy[MD], cz[MD];
@@ -366,8 +367,8 @@ __global__ void __launch_bounds__(384, 1) k_stencil_tma(const __grid_constant__ 
     const int zc = blockIdx.y - band * nzc;
     if (a.band_active && !a.band_active[band]) return;  // uniform per CTA
     const int y0 = blockIdx.x * TY;
-    const int zs = zc * a.zlen;
-    const int zlen = min(zs + a.zlen, n3) - zs;
+    const int zs = a.z0 + zc * a.zlen;
+    const int zlen = min(zs + a.zlen, a.z0 + a.nzo) - zs;
     const int nk = zlen + 2 * MD;  // arrival k <-> plane zs - Md + k
     const long plane = (long)n1 * n2;
 
@@ -636,10 +637,10 @@ static int launch_tma(StencilArgs<T> a, const StencilCoef& cf, int nb, cudaStrea
     if (reinterpret_cast<uintptr_t>(a.hpsi) % 16 != 0 || (a.ld * sizeof(T)) % 16 != 0) return RSDFT_OK;
     const int sms = c.num_sms > 0 ? c.num_sms : 148;
     const long base = (long)(a.n2 / g.TY) * nb;
-    int nzc = (int)std::min<long>(std::max<long>(1, (sms + base - 1) / base), std::max(1, a.n3 / (4 * MD)));
+    int nzc = (int)std::min<long>(std::max<long>(1, (sms + base - 1) / base), std::max(1, a.nzo / (4 * MD)));
     while ((long)nb * nzc > 65535 && nzc > 1) --nzc;
-    a.zlen = div_up(a.n3, nzc);
-    a.nzc = div_up(a.n3, a.zlen);
+    a.zlen = div_up(a.nzo, nzc);
+    a.nzc = div_up(a.nzo, a.zlen);
     TmaMaps maps;
     const CUtensorMapDataType dt = sizeof(T) == 8 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT64 : CU_TENSOR_MAP_DATA_TYPE_FLOAT32;
     const unsigned long long dims[4] = {(unsigned long long)a.n1, (unsigned long long)a.n2,
@@ -690,10 +691,10 @@ static int launch_stencil_md2(StencilArgs<T> a, const StencilCoef& cf, int nb, c
     const int tx = (a.n1 % 32 == 0 || a.n1 > 24) ? 32 : (a.n1 % 24 == 0 ? 24 : 16);
     const long base = (long)div_up(a.n1, tx) * div_up(a.n2, 16) * nb;
     const long want = 8L * (c.num_sms > 0 ? c.num_sms : 148);
-    int nzc = (int)std::min<long>(std::max<long>(1, (want + base - 1) / base), std::max(1, a.n3 / 8));
+    int nzc = (int)std::min<long>(std::max<long>(1, (want + base - 1) / base), std::max(1, a.nzo / 8));
     while ((long)nb * nzc > 65535 && nzc > 1) --nzc;
-    a.zlen = div_up(a.n3, nzc);
-    a.nzc = div_up(a.n3, a.zlen);
+    a.zlen = div_up(a.nzo, nzc);
+    a.nzc = div_up(a.nzo, a.zlen);
     launch_stencil_md<T, MD>(a, cf, nb, st);
     RS_LAUNCH();
     return RSDFT_OK;
@@ -701,6 +702,10 @@ static int launch_stencil_md2(StencilArgs<T> a, const StencilCoef& cf, int nb, c
 
 template <typename T>
 static int launch_stencil(StencilArgs<T> a, const StencilCoef& cf, int md, int nb, cudaStream_t st) {
+    if (a.nzo <= 0) {
+        a.z0 = 0;
+        a.nzo = a.n3;
+    }
     switch (md) {
         case 1: return launch_stencil_md2<T, 1>(a, cf, nb, st);
         case 2: return launch_stencil_md2<T, 2>(a, cf, nb, st);
@@ -785,6 +790,110 @@ extern "C" int rsdft_gpu_hamiltonian(int k, int s, const double* tpsi, double* h
     RS_CHECK(wf_acquire(tpsi, ld, nb, "ham_in", &dpsi, &sp));
     RS_CHECK(wf_acquire(htpsi, ld, nb, "ham_out", &dh, &sh, false));
     RS_CHECK(hpsi_device<double>(dpsi, dh, ld, nb, s, nullptr));
+    RS_CHECK(wf_release(htpsi, dh, ld, nb, sh));
+    return RSDFT_OK;
+}
+
+// ----------------------------------------------------- the three operators
+// hamiltonian applies op_kinetic, op_localpot and op_nonlocal in turn
+// (hamiltonian_module.f90:42-58).  A domain-decomposed caller needs them
+// apart: the kinetic + local part on a slab extended by its halo planes, and
+// the nonlocal part as projection partial sums over the slab's own points,
+// which the ranks add up before the scatter (ps_nloc2_op_module.f90:
+// 161-250).  These entries give those pieces on the context's grid and
+// projector tables.
+namespace rsdft {
+namespace {
+
+int check_block(const char* who, int s, long ld, int nb) {
+    Context& c = ctx();
+    if (s < 1 || s > c.nspin) {
+        set_error("%s: s=%d outside 1..%d", who, s, c.nspin);
+        return RSDFT_EINVAL;
+    }
+    if (ld < c.ml || nb < 1 || nb > 65535) {
+        set_error("%s: ld=%ld (ML=%ld), nb=%d", who, ld, c.ml, nb);
+        return RSDFT_EINVAL;
+    }
+    return RSDFT_OK;
+}
+
+}  // namespace
+}  // namespace rsdft
+
+extern "C" int rsdft_gpu_op_local(int s, const double* tpsi, double* htpsi, long ld, int nb, int z0, int nz) {
+    RS_ENTRY();
+    RS_CHECK(require_grid());
+    Context& c = ctx();
+    RS_CHECK(check_block("op_local", s, ld, nb));
+    if (z0 < 0 || nz < 1 || z0 + nz > c.n3) {
+        set_error("op_local: planes [%d, %d) outside 0..%d", z0, z0 + nz, c.n3);
+        return RSDFT_EINVAL;
+    }
+    if (!c.vloc || c.vloc_ml != c.ml) {
+        set_error("op_local: rsdft_gpu_set_vloc has not been called for the current grid");
+        return RSDFT_ENOTINIT;
+    }
+    double *dpsi, *dh;
+    bool sp, sh;
+    RS_CHECK(wf_acquire(tpsi, ld, nb, "ham_in", &dpsi, &sp));
+    RS_CHECK(wf_acquire(htpsi, ld, nb, "ham_out", &dh, &sh, false));
+    StencilArgs<double> a{};
+    a.psi = dpsi;
+    a.hpsi = dh;
+    a.ld = ld;
+    a.n1 = c.n1;
+    a.n2 = c.n2;
+    a.n3 = c.n3;
+    a.vloc = c.vloc + (long)(s - 1) * c.ml;
+    a.nzlma = c.nzlma;
+    a.z0 = z0;
+    a.nzo = nz;
+    RS_CHECK(launch_stencil<double>(a, c.sc, c.md, nb, c.stream));
+    RS_CHECK(wf_release(htpsi, dh, ld, nb, sh));
+    return RSDFT_OK;
+}
+
+extern "C" int rsdft_gpu_op_nonlocal_project(const double* tpsi, long ld, int nb, double* uvunk) {
+    RS_ENTRY();
+    RS_CHECK(require_grid());
+    Context& c = ctx();
+    RS_CHECK(check_block("op_nonlocal_project", 1, ld, nb));
+    if (!uvunk) {
+        set_error("op_nonlocal_project: NULL uvunk");
+        return RSDFT_EINVAL;
+    }
+    if (!c.nl_set || c.nzlma == 0) return RSDFT_OK;
+    double* dpsi;
+    bool sp;
+    RS_CHECK(wf_acquire(tpsi, ld, nb, "ham_in", &dpsi, &sp));
+    double* du = nullptr;
+    RS_CHECK(workspace_t("op_uvunk", (size_t)c.nzlma * nb, &du));
+    RS_CHECK(launch_project<double>(dpsi, ld, nb, du, nullptr, c.stream));
+    RS_CHECK(stage_out(uvunk, du, sizeof(double) * (size_t)c.nzlma * nb));
+    return RSDFT_OK;
+}
+
+extern "C" int rsdft_gpu_op_nonlocal_add(const double* uvunk, double* htpsi, long ld, int nb) {
+    RS_ENTRY();
+    RS_CHECK(require_grid());
+    Context& c = ctx();
+    RS_CHECK(check_block("op_nonlocal_add", 1, ld, nb));
+    if (!uvunk) {
+        set_error("op_nonlocal_add: NULL uvunk");
+        return RSDFT_EINVAL;
+    }
+    if (!c.nl_set || c.nzlma == 0 || c.nl_npt == 0) return RSDFT_OK;
+    void* du = nullptr;
+    RS_CHECK(stage_in(uvunk, sizeof(double) * (size_t)c.nzlma * nb, "op_uvunk_in", &du));
+    double* dh;
+    bool sh;
+    RS_CHECK(wf_acquire(htpsi, ld, nb, "ham_out", &dh, &sh));
+    constexpr int BCH = 32;
+    dim3 grid(div_up(c.nl_npt, 128), div_up(nb, BCH));
+    launch(k_nl_scatter<double>, grid, 128, 0, c.stream, dh, ld, nb, BCH, (const int*)c.nl_pts, (const int*)c.nl_ptr,
+           c.nl_npt, (const int*)c.gpt_grp, (const double*)c.gpt_uv4, (const double*)du, c.nzlma, (const int*)nullptr);
+    RS_LAUNCH();
     RS_CHECK(wf_release(htpsi, dh, ld, nb, sh));
     return RSDFT_OK;
 }
