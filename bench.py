@@ -53,6 +53,10 @@ def parse():
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--no-e2e", action="store_true")
     p.add_argument("--no-accuracy", action="store_true", help="skip the 10-iteration accuracy comparison")
+    p.add_argument("--cpu-table", default="", help="comma-separated workloads: print the CPU rows of the "
+                   "per-configuration table (oracle hpsi, nonlocal force, and whole iterations for "
+                   "--cpu-table-iter) and exit")
+    p.add_argument("--cpu-table-iter", default="si8,si64")
     return p.parse_args()
 
 
@@ -207,6 +211,36 @@ def cpu_baseline_run(cell, ncg: int, mloop: int, steps: int, warmup: int):
     }
 
 
+def cpu_table(workloads, ncg: int, mloop: int, iter_workloads):
+    """The CPU rows of the per-configuration table: the oracle on the host
+    cores, per workload hpsi on every band, one nonlocal force evaluation
+    (lowest nocc bands doubly occupied) and, for the workloads in
+    iter_workloads, one whole iteration as cpu_iteration runs it."""
+    from oracle import oracle as O  # CPU baseline leg only
+
+    rows = {}
+    for name in workloads:
+        from rsdft_b200.cell import build_cell
+
+        cell = build_cell(name)
+        o = O.Oracle(cell)
+        psi = o.gram_schmidt_t(np.asfortranarray(cell.psi0()))
+        o.hamiltonian(np.asfortranarray(psi[:, :2]))  # threads and tables warm
+        t0 = time.perf_counter()
+        o.hamiltonian(psi)
+        row = {"hpsi_s": time.perf_counter() - t0}
+        occ = np.zeros(cell.nband)
+        occ[: cell.nocc] = 2.0
+        t0 = time.perf_counter()
+        o.force_nloc(psi, occ)
+        row["force_nloc_s"] = time.perf_counter() - t0
+        if name in iter_workloads:
+            _, sec = cpu_iteration(o, cell, psi, ncg, mloop)
+            row["iteration_s"] = sum(sec.values())
+        rows[name] = row
+    return {"what": "cpu_table", "threads": int(O.lib().oracle_num_threads()), "host": host_info(), "rows": rows}
+
+
 def metric_name(cell, ncg):
     """The headline metric's label for a workload ("Si216 72^3, 480 bands" by default)."""
     n1 = cell.ngrid[0]
@@ -275,6 +309,11 @@ def main():
     from rsdft_b200 import replicas
 
     rank, world, local = replicas.rank_info()
+    if args.cpu_table:
+        if rank == 0:
+            print(json.dumps(cpu_table(args.cpu_table.split(","), args.ncg, args.mloop,
+                                       set(args.cpu_table_iter.split(",")))), flush=True)
+        return
     if args.impl == "reference":
         run_reference(args, rank, world)
         return

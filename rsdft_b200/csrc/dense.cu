@@ -219,12 +219,18 @@ __global__ void k_diag_minmax(const double* __restrict__ a, int n, int lda, doub
 // Largest (max diag R / min diag R)^2 of the overlap's Cholesky factor for
 // which the one-step Rayleigh-Ritz is kept.  The eigenvalue error of the
 // R^-T H R^-1 form grows with the overlap's condition, and the Gram matrices'
-// own error with the precision form: FP64 1e3, 3-term split-BF16 1e2, 2-term
-// (~16 significant bits) 1e1 (measured: an overlap with diag ratio^2 93 and
-// condition 2.4e3 gave 6.5e-4 relative eigenvalue error in the 2-term form,
-// 3e-6 in the 3-term form).
+// own error with the precision form: FP64 1e3, 3-term split-BF16 (24
+// significant bits) 1e2, 2-term split-TF32 (22 bits, four times the operand
+// error) 25, 2-term split-BF16 (~16 bits) 1e1 (measured: an overlap with diag
+// ratio^2 93 and condition 2.4e3 gave 6.5e-4 relative eigenvalue error in the
+// 2-term BF16 form, 1.7e-5 in the TF32 form, 2e-6 in the 3-term form).
 static double fused_rr_kappa_max(int mode) {
-    return mode == RSDFT_MODE_FP64 ? 1e3 : (mode == RSDFT_MODE_MIXED_BF16X2 ? 1e1 : 1e2);
+    switch (mode) {
+        case RSDFT_MODE_FP64: return 1e3;
+        case RSDFT_MODE_MIXED_BF16X2: return 1e1;
+        case RSDFT_MODE_MIXED_TF32: return 25.0;
+        default: return 1e2;
+    }
 }
 
 // Gram-Schmidt followed by subspace_diag (the pair calc_sweep calls,

@@ -12,6 +12,9 @@
     the Gram-Schmidt + Rayleigh-Ritz step alone (``rsdft_gpu_orth_subspace_diag``)
     on orthonormalised seeded bands; ``--ngrid`` / ``--bands`` shrink the cell
     (same atoms, coarser grid) for small profiler captures.
+``python -m rsdft_b200.microbench table --workloads si8,si64,si216``
+    per workload: hpsi on all bands (GB/s, fraction of the measured HBM
+    copy bandwidth), FP64 and mixed iteration times, one adjoint force.
 ``python -m rsdft_b200.microbench large --workload si512``
     the large-cell run: FP64 and mixed iterations from one start (each timed),
     the FP64 closing pass, one adjoint force evaluation per form, eigenvalue
@@ -162,6 +165,60 @@ def run_large(args) -> dict:
     return out
 
 
+def _hbm_peak():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            return float(json.load(f)["hbm_gbs"]), "measured"
+    except (OSError, KeyError, ValueError):
+        return 6650.0, "fallback"
+
+
+def run_table(args) -> dict:
+    """Per workload: hpsi on all bands, FP64 and mixed iterations from the
+    same Gram-Schmidt'd seeded start, one adjoint force evaluation (lowest
+    nocc bands doubly occupied) on the FP64 bands."""
+    import torch
+
+    from rsdft_b200 import api
+    from rsdft_b200.cell import build_cell
+
+    peak, src = _hbm_peak()
+    st = torch.cuda.Stream()
+    torch.cuda.set_stream(st)
+    g = api.RsdftGpu(0)
+    g.set_stream(st.cuda_stream)
+    rows = {}
+    for name in args.workloads.split(","):
+        cell = build_cell(name)
+        g.setup(cell)
+        MB, ML = cell.nband, cell.ML
+        start = torch.from_numpy(np.ascontiguousarray(cell.psi0().T)).cuda().t()
+        g.gram_schmidt(1, MB, 1, 1, start)
+        h = api.fortran_empty(ML, MB)
+        ms = _timed(torch, st, lambda: g.hamiltonian(1, 1, start, h, 1, ML, 1, MB), 2, 5)
+        nbytes = MB * ML * 16 + ML * 8 + int(cell.lma_ptr[-1]) * 12
+        row = {"grid": list(cell.ngrid), "bands": MB,
+               "hpsi": {"ms": ms, "gbs": nbytes / (ms * 1e-3) / 1e9, "frac": nbytes / (ms * 1e-3) / 1e9 / peak,
+                        "peak_source": src}}
+        for form, mode in (("fp64", 0), ("mixed-bf16x3", 1)):
+            u = api.fortran_copy(start)
+            esp = torch.zeros(MB, dtype=torch.float64, device="cuda")
+            res = torch.zeros_like(esp)
+            it = _timed(torch, st, lambda: g.eigensolver_iteration(u, esp, res, ncg=4, mloop=3, mode=mode),
+                        args.warmup, args.steps)
+            row[form] = {"ms_per_iter": it}
+            if mode == 0:
+                occ = np.zeros(MB)
+                occ[: cell.nocc] = 2.0
+                dv = torch.zeros(ML, dtype=torch.float64, device="cuda")
+                dr = torch.zeros(3 * cell.natom, dtype=torch.float64, device="cuda")
+                row["adjoint_force_ms"] = _timed(torch, st, lambda: g.hpsi_adjoint(u, occ=occ, dl_dv=dv, dl_dr=dr),
+                                                 1, 3)
+            del u
+        rows[name] = row
+    return {"what": "table", "rows": rows}
+
+
 def main(argv=None) -> None:
     p = argparse.ArgumentParser(description=__doc__, formatter_class=argparse.RawDescriptionHelpFormatter)
     sub = p.add_subparsers(dest="what", required=True)
@@ -192,8 +249,13 @@ def main(argv=None) -> None:
     lg.add_argument("--ncg", type=int, default=4)
     lg.add_argument("--mloop", type=int, default=3)
     lg.add_argument("--steps", type=int, default=5)
+    tb = sub.add_parser("table")
+    tb.add_argument("--workloads", default="si8,si64,si216")
+    tb.add_argument("--warmup", type=int, default=2)
+    tb.add_argument("--steps", type=int, default=3)
     args = p.parse_args(argv)
-    out = {"hpsi": run_hpsi, "iteration": run_iteration, "rr": run_rr, "large": run_large}[args.what](args)
+    out = {"hpsi": run_hpsi, "iteration": run_iteration, "rr": run_rr, "large": run_large,
+           "table": run_table}[args.what](args)
     print(json.dumps(out), flush=True)
 
 
