@@ -56,9 +56,15 @@ def _stale(obj: str, src: str) -> bool:
 
 
 def build(verbose: bool = False, extra_flags=None) -> str:
+    srcs = sorted(glob.glob(os.path.join(CSRC, "*.cu")))
+    if not extra_flags and os.path.exists(LIB):
+        # the linked library is newer than every source and header: nothing
+        # to do, even where the object files did not travel with it
+        t = os.path.getmtime(LIB)
+        if all(os.path.getmtime(d) <= t for d in srcs + _headers()):
+            return LIB
     os.makedirs(BUILD, exist_ok=True)
     nvcc = _nvcc()
-    srcs = sorted(glob.glob(os.path.join(CSRC, "*.cu")))
     flags = NVCC_FLAGS + list(extra_flags or [])
     jobs = []
     objs = []

@@ -263,6 +263,10 @@ struct Pk<double> {
         o[1] = v.y;
     }
     __device__ static __forceinline__ double2 put2(const t* o) { return make_double2(o[0], o[1]); }
+    __device__ static __forceinline__ void unpack2(const t* c, double* o) {
+        o[0] = c[0];
+        o[1] = c[1];
+    }
 };
 template <>
 struct Pk<float> {
@@ -278,6 +282,12 @@ struct Pk<float> {
         o[1] = make_float2(v.z, v.w);
     }
     __device__ static __forceinline__ float4 put2(const t* o) { return make_float4(o[0].x, o[0].y, o[1].x, o[1].y); }
+    __device__ static __forceinline__ void unpack2(const t* c, float* o) {
+        o[0] = c[0].x;
+        o[1] = c[0].y;
+        o[2] = c[1].x;
+        o[3] = c[1].y;
+    }
 };
 
 // One arrival's z pushes for accumulator slot U (compile time): outputs
@@ -470,13 +480,18 @@ __global__ void __launch_bounds__(384, 1) k_stencil_tma(const __grid_constant__ 
                     }
                 }
             }
-            // x neighbours from the periodic window of each own row
+            // x neighbours from the periodic window of each own row (its
+            // centre vector is the row's own, already read with the y window)
 #pragma unroll
             for (int r = 0; r < BY; ++r) {
                 const T* rp = st + (MD + yl + r) * RS;
                 T w[NV * VX];
 #pragma unroll
                 for (int j = 0; j < NV; ++j) {
+                    if (j == MDX / VX) {
+                        P::unpack2(c + 2 * r, w + j * VX);
+                        continue;
+                    }
                     int xx = xw + VX * j;
                     xx += xx < 0 ? n1 : (xx >= n1 ? -n1 : 0);
                     VT::get(*reinterpret_cast<const V*>(rp + xx), w + j * VX);

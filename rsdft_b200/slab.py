@@ -39,6 +39,13 @@ every rank and each rank rotates its own rows (subspace_rotv_sl_module.f90:
 The per-slab compute goes through a backend: ``GpuSlabBackend`` calls the
 library's entries on this rank's GPU.  Every rank takes the same collective
 steps in the same order.
+
+A whole iteration (``BandGridIteration``) uses both partitions the
+reference has, each where it needs no exchange: the CG band-parallel (the
+reference's comm_band split; the CG is band by band, so a rank's bands need
+nothing from the others), the Rayleigh-Ritz step grid-parallel (MB x MB
+partial sums), with all-to-all moves of the bands between the two layouts
+(``BandGridLayout``).
 """
 from __future__ import annotations
 
@@ -53,14 +60,25 @@ import numpy as np
 KAPPA_MAX = 1e3
 
 
-def split_planes(n: int, nparts: int):
-    """(counts, offsets) of n points cut into nparts parts
-    (rgrid_sol_module.f90:84-108)."""
+def _split(n: int, nparts: int, what: str):
     if nparts < 1 or n < nparts:
-        raise ValueError(f"cannot cut {n} planes into {nparts} slabs of at least one plane")
+        raise ValueError(f"cannot cut {n} {what} into {nparts} parts of at least one")
     counts = [n // nparts + (1 if p < n % nparts else 0) for p in range(nparts)]
     offsets = [sum(counts[:p]) for p in range(nparts)]
     return counts, offsets
+
+
+def split_planes(n: int, nparts: int):
+    """(counts, offsets) of n points cut into nparts parts
+    (rgrid_sol_module.f90:84-108)."""
+    return _split(n, nparts, "planes")
+
+
+def split_bands(nb: int, nparts: int):
+    """(counts, offsets) of nb bands over nparts ranks: band i counts for rank
+    mod(i, np), each rank's bands contiguous in rank order
+    (parallel_module.f90:366-377, the same rule as the grid split)."""
+    return _split(nb, nparts, "bands")
 
 
 @dataclasses.dataclass(frozen=True)
@@ -306,3 +324,190 @@ class SlabSolver:
         b.rr_reduced(rinv, hsub, esp, w)
         b.rotate(d.own(psi), w)
         return hpsi
+
+
+# ------------------------------------------------- band / grid layouts
+class BandGridLayout:
+    """One band set over N ranks in two layouts.
+
+    band layout  rank r holds bands [b0(r), b0(r) + nb(r)) (split_bands) on
+                 the whole grid, column-major (ML, nb(r));
+    grid layout  rank r holds every band on its own planes [z0(r), z0(r) +
+                 nz(r)) (split_planes), column-major (n1 n2 nz(r), nb).
+
+    to_grid / to_band move the bands between them: rank r sends rank q the
+    rows of q's planes of its own bands as one packed (nb(r), rows(q))
+    message (an all-to-all: NCCL send/recv between GPUs, gloo on the host)."""
+
+    def __init__(self, ngrid, nb: int, rank: int, nranks: int):
+        self.n1, self.n2, self.n3 = (int(v) for v in ngrid)
+        self.nb, self.rank, self.nranks = int(nb), int(rank), int(nranks)
+        self.n12 = self.n1 * self.n2
+        self.ml = self.n12 * self.n3
+        self.pcounts, self.poffsets = split_planes(self.n3, self.nranks)
+        self.bcounts, self.boffsets = split_bands(self.nb, self.nranks)
+        self.rows = [(o * self.n12, (o + c) * self.n12) for c, o in zip(self.pcounts, self.poffsets)]
+        self.b0, self.nb_own = self.boffsets[rank], self.bcounts[rank]
+        self.ml_own = self.pcounts[rank] * self.n12
+
+    @staticmethod
+    def _rows_major(t, rows, cols, what):
+        """The (cols, rows) row-major view of a column-major (rows, cols) array."""
+        if tuple(t.shape) != (rows, cols) or (cols > 1 and t.stride(1) != rows) or t.stride(0) != 1:
+            raise ValueError(f"{what} must be a column-major ({rows}, {cols}) array with leading dimension {rows}")
+        return t.t()
+
+    def _exchange(self, sends, recvs, dist):
+        if not sends and not recvs:
+            return
+        if dist is None:
+            raise ValueError("more than one rank needs a process group")
+        ops = [dist.P2POp(dist.isend, buf, q) for q, buf in sends]
+        ops += [dist.P2POp(dist.irecv, buf, q) for q, buf in recvs]
+        for req in dist.batch_isend_irecv(ops):
+            req.wait()
+
+    def to_grid(self, band, grid, dist=None) -> None:
+        """grid (ml_own, nb) <- the rank's planes of every band, from the band
+        layouts of all ranks."""
+        import torch
+
+        bt = self._rows_major(band, self.ml, self.nb_own, "band-layout array")
+        gt = self._rows_major(grid, self.ml_own, self.nb, "grid-layout array")
+        r0, r1 = self.rows[self.rank]
+        gt[self.b0:self.b0 + self.nb_own].copy_(bt[:, r0:r1])
+        sends, recvs = [], []
+        for q in range(self.nranks):
+            if q == self.rank:
+                continue
+            q0, q1 = self.rows[q]
+            sends.append((q, bt[:, q0:q1].contiguous()))
+            recvs.append((q, torch.empty((self.bcounts[q], r1 - r0), dtype=band.dtype, device=band.device)))
+        self._exchange(sends, recvs, dist)
+        for q, buf in recvs:
+            gt[self.boffsets[q]:self.boffsets[q] + self.bcounts[q]].copy_(buf)
+
+    def to_band(self, grid, band, dist=None) -> None:
+        """band (ML, nb_own) <- the rank's bands on the whole grid, from the
+        grid layouts of all ranks."""
+        import torch
+
+        bt = self._rows_major(band, self.ml, self.nb_own, "band-layout array")
+        gt = self._rows_major(grid, self.ml_own, self.nb, "grid-layout array")
+        r0, r1 = self.rows[self.rank]
+        bt[:, r0:r1].copy_(gt[self.b0:self.b0 + self.nb_own])
+        sends, recvs = [], []
+        for q in range(self.nranks):
+            if q == self.rank:
+                continue
+            q0, q1 = self.rows[q]
+            sends.append((q, gt[self.boffsets[q]:self.boffsets[q] + self.bcounts[q]].contiguous()))
+            recvs.append((q, torch.empty((self.nb_own, q1 - q0), dtype=grid.dtype, device=grid.device)))
+        self._exchange(sends, recvs, dist)
+        for q, buf in recvs:
+            q0, q1 = self.rows[q]
+            bt[:, q0:q1].copy_(buf)
+
+
+class GpuBandBackend:
+    """The whole-grid compute of one rank on its GPU: the library set up on
+    the full cell, CG and H psi on the rank's bands, Gram sums over any rows,
+    the small dense steps, row-block rotations."""
+
+    def __init__(self, gpu, cell):
+        import torch
+
+        self.gpu = gpu
+        self.device = torch.device("cuda", gpu.device)
+        gpu.setup(cell, with_forces=False)
+        self.ml = int(cell.ML)
+        self.dV = float(cell.dV)
+
+    def empty(self, rows, cols):
+        from . import api
+
+        return api.fortran_empty(rows, cols, device=self.device)
+
+    def vector(self, n):
+        import torch
+
+        return torch.zeros(n, dtype=torch.float64, device=self.device)
+
+    def cg(self, psi, esp, res, ncg, mloop, mode):
+        self.gpu.conjugate_gradient(1, self.ml, psi.shape[1], 1, 1, psi, esp, res, ncg=ncg, mloop=mloop, mode=mode)
+
+    def hamiltonian(self, psi, hpsi):
+        self.gpu.hamiltonian(1, 1, psi, hpsi, 1, self.ml, 1, psi.shape[1])
+
+    def gram(self, a, b, out, alpha, sym):
+        self.gpu.gram(a, b, out, alpha=alpha, sym=sym)
+
+    def overlap_cholesky(self, s, rinv) -> float:
+        return self.gpu.overlap_cholesky(s, rinv)
+
+    def rr_reduced(self, rinv, hsub, esp, w):
+        self.gpu.rr_reduced(rinv, hsub, esp, w)
+
+    def rotate(self, psi, w):
+        self.gpu.rotate(psi, w)
+
+
+class BandGridIteration:
+    """One eigensolver iteration as calc_sweep runs it (sweep_module.f90:
+    150-155) over the ranks of ``layout``:
+
+    1. conjugate_gradient on the rank's own bands on the whole grid (band
+       parallel: cg_module.f90:97-430 treats each band alone at SWGS = 0),
+       then H psi of those bands;
+    2. psi and H psi moved to the grid layout;
+    3. gram_schmidt + subspace_diag as one Rayleigh-Ritz step on the grid
+       layout: S = dV psi^T psi and H = dV sym(psi^T H psi) summed over the
+       ranks' planes (the MB x MB all-reduces of gram_schmidt_t_module.f90:
+       194 and subspace_diag_la_module.f90:122), S = R^T R, R^-T H R^-1 =
+       V diag(esp) V^T solved on every rank, the own rows rotated by R^-1 V
+       (a second CholeskyQR pass first when diag(R) spreads beyond
+       KAPPA_MAX, applied to H psi as well since H (psi R^-1) = (H psi) R^-1);
+    4. the bands moved back to the band layout.
+
+    esp (MB) ends up the Rayleigh-Ritz eigenvalues and res (MB) the CG
+    residuals, on every rank."""
+
+    def __init__(self, layout: BandGridLayout, backend, dist=None):
+        self.L, self.b, self.dist = layout, backend, dist
+        if dist is None and layout.nranks != 1:
+            raise ValueError("BandGridIteration: more than one rank needs a process group")
+
+    def _allreduce(self, t):
+        if self.dist is not None:
+            self.dist.all_reduce(t)
+        return t
+
+    def _gram(self, a, c, sym):
+        out = self.b.empty(self.L.nb, self.L.nb)
+        self.b.gram(a, c, out, self.b.dV, sym)
+        return self._allreduce(out)
+
+    def iterate(self, psi, esp, res, ncg=4, mloop=3, mode=0) -> None:
+        L, b = self.L, self.b
+        e_own, r_own = b.vector(L.nb_own), b.vector(L.nb_own)
+        b.cg(psi, e_own, r_own, ncg, mloop, mode)
+        hpsi = b.empty(L.ml, L.nb_own)
+        b.hamiltonian(psi, hpsi)
+        gpsi, ghpsi = b.empty(L.ml_own, L.nb), b.empty(L.ml_own, L.nb)
+        L.to_grid(psi, gpsi, self.dist)
+        L.to_grid(hpsi, ghpsi, self.dist)
+        del hpsi
+        rinv = b.empty(L.nb, L.nb)
+        kappa = b.overlap_cholesky(self._gram(gpsi, gpsi, 0), rinv)
+        if not kappa <= KAPPA_MAX:
+            b.rotate(gpsi, rinv)
+            b.rotate(ghpsi, rinv)
+            kappa = b.overlap_cholesky(self._gram(gpsi, gpsi, 0), rinv)
+        hsub = self._gram(gpsi, ghpsi, 1)
+        w = b.empty(L.nb, L.nb)
+        b.rr_reduced(rinv, hsub, esp, w)
+        b.rotate(gpsi, w)
+        L.to_band(gpsi, psi, self.dist)
+        full = b.vector(L.nb)
+        full[L.b0:L.b0 + L.nb_own] = r_own
+        res.copy_(self._allreduce(full))

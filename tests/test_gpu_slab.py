@@ -1,5 +1,7 @@
 """The z-slab driver on the GPU backend (library entries op_local,
-op_nonlocal_project / _add, gram, overlap_cholesky, rr_reduced, rotate).
+op_nonlocal_project / _add, gram, overlap_cholesky, rr_reduced, rotate), and
+the split iteration (CG on each rank's bands, Rayleigh-Ritz on each rank's
+planes) on the whole-grid backend.
 
 One GPU cannot hold ranks that wait on one another, so the multi-rank cases
 run the ranks one after the other in one process, with the exchanges done on
@@ -14,7 +16,8 @@ import torch
 
 from oracle import oracle as O
 from rsdft_b200 import api
-from rsdft_b200.slab import GpuSlabBackend, SlabDomain, SlabSolver
+from rsdft_b200.slab import (BandGridIteration, BandGridLayout, GpuBandBackend, GpuSlabBackend, SlabDomain,
+                             SlabSolver)
 
 from test_gpu_parity import TOL, dev, host, rel
 
@@ -119,3 +122,77 @@ def test_op_local_rejects_planes_outside_grid(gpu, cells):
     out = api.fortran_empty(c.ML, 2)
     with pytest.raises(api.RsdftError):
         gpu.op_local(1, psi, out, z0=20, nz=10)
+
+
+def test_band_grid_iteration_one_rank_si64(gpu, cells):
+    """The split iteration's driver on one rank (layout moves with no peer)
+    against the library's one-call iteration on the same start: CG
+    residuals 1e-12, Rayleigh-Ritz eigenvalues 1e-12, the same eigenvectors."""
+    c = cells("si64")
+    nb = 32
+    q = np.asfortranarray(O.Oracle(c).gram_schmidt_t(np.asfortranarray(c.psi0(nb))))
+    it = BandGridIteration(BandGridLayout(c.ngrid, nb, 0, 1), GpuBandBackend(gpu, c), None)
+    u = dev(q)
+    esp = torch.zeros(nb, dtype=torch.float64, device="cuda")
+    res = torch.zeros_like(esp)
+    it.iterate(u, esp, res, ncg=4, mloop=3)
+    ref = dev(q)
+    eref, rref = torch.zeros_like(esp), torch.zeros_like(esp)
+    gpu.eigensolver_iteration(ref, eref, rref, ncg=4, mloop=3)
+    torch.cuda.synchronize()
+    assert rel(host(res), host(rref)) <= TOL
+    assert rel(host(esp), host(eref)) <= TOL
+    g, gr = host(u), host(ref)
+    assert np.abs(g.T @ g * c.dV - np.eye(nb)).max() <= 1e-12
+    assert np.abs(np.abs(np.diag(gr.T @ g * c.dV)) - 1.0).max() <= 1e-9
+
+
+@pytest.mark.parametrize("nranks", [2, 3])
+def test_band_grid_iteration_virtual_ranks_si64(gpu, cells, nranks):
+    """The split iteration's per-rank steps for nranks ranks run one after
+    another on the GPU (CG and H psi on each rank's bands, Gram partial sums
+    on each rank's planes, summed here; the layout moves done by slicing on
+    the host) against the library's one-call iteration on all bands."""
+    c = cells("si64")
+    nb = 48
+    q = np.asfortranarray(O.Oracle(c).gram_schmidt_t(np.asfortranarray(c.psi0(nb))))
+    b = GpuBandBackend(gpu, c)
+    lay = [BandGridLayout(c.ngrid, nb, r, nranks) for r in range(nranks)]
+    cg_out, h_out, res = [], [], np.zeros(nb)
+    for L in lay:
+        u = dev(q[:, L.b0:L.b0 + L.nb_own])
+        e, r = b.vector(L.nb_own), b.vector(L.nb_own)
+        b.cg(u, e, r, 4, 3, api.MODE_FP64)
+        h = b.empty(c.ML, L.nb_own)
+        b.hamiltonian(u, h)
+        cg_out.append(host(u))
+        h_out.append(host(h))
+        res[L.b0:L.b0 + L.nb_own] = host(r)
+    psi_all, h_all = np.concatenate(cg_out, axis=1), np.concatenate(h_out, axis=1)
+    grids = [(dev(psi_all[L.rows[L.rank][0]:L.rows[L.rank][1]]), dev(h_all[L.rows[L.rank][0]:L.rows[L.rank][1]]))
+             for L in lay]
+    s = np.zeros((nb, nb))
+    hs = np.zeros((nb, nb))
+    for gp, gh in grids:
+        t = b.empty(nb, nb)
+        b.gram(gp, gp, t, c.dV, 0)
+        s += host(t)
+        b.gram(gp, gh, t, c.dV, 1)
+        hs += host(t)
+    rinv = b.empty(nb, nb)
+    assert b.overlap_cholesky(dev(s), rinv) < 1e3
+    esp = b.vector(nb)
+    w = b.empty(nb, nb)
+    b.rr_reduced(rinv, dev(hs), esp, w)
+    for gp, _ in grids:
+        b.rotate(gp, w)
+    ref = dev(q)
+    eref, rref = b.vector(nb), b.vector(nb)
+    gpu.eigensolver_iteration(ref, eref, rref, ncg=4, mloop=3)
+    torch.cuda.synchronize()
+    assert rel(res, host(rref)) <= TOL
+    assert rel(host(esp), host(eref)) <= TOL
+    g = np.concatenate([host(gp) for gp, _ in grids])
+    gr = host(ref)
+    assert np.abs(g.T @ g * c.dV - np.eye(nb)).max() <= 1e-12
+    assert np.abs(np.abs(np.diag(gr.T @ g * c.dV)) - 1.0).max() <= 1e-9

@@ -1,7 +1,8 @@
 """z-slab decomposition on the host: plane split, halo index maps, projector
 restriction, and world_size 2 / 3 gloo ranks computing H psi, the Gram sums
 and the Rayleigh-Ritz step slab by slab, checked against the single-domain
-oracle.  The per-slab compute here is the oracle (kinetic + local) and numpy
+oracle; the band split, the band <-> grid layout moves and whole iterations
+with the CG band-parallel and the Rayleigh-Ritz step grid-parallel.  The per-slab compute here is the oracle (kinetic + local) and numpy
 (projector partials and scatter, small dense steps); the GPU backend runs the
 same driver in test_gpu_slab.py."""
 import os
@@ -15,7 +16,8 @@ import torch.multiprocessing as mp
 from oracle import oracle as O
 from rsdft_b200 import api
 from rsdft_b200.cell import build_cell
-from rsdft_b200.slab import SlabDomain, SlabSolver, halo_runs, split_planes
+from rsdft_b200.slab import (BandGridIteration, BandGridLayout, SlabDomain, SlabSolver, halo_runs, split_bands,
+                             split_planes)
 
 TOL = 1e-12
 
@@ -90,6 +92,30 @@ class OracleSlabBackend:
     def rotate(self, psi_own, w):
         a = psi_own.numpy()
         a[:] = a @ w.numpy()
+
+
+class OracleBandBackend(OracleSlabBackend):
+    """The whole-grid compute of a rank on the host: the oracle's CG (band
+    by band, cg_module.f90:97-430) and H psi on the rank's bands, numpy Gram
+    sums and small dense steps."""
+
+    def __init__(self, cell):
+        self.oracle = O.Oracle(cell)
+        self.ml = cell.ML
+        self.dV = cell.dV
+        self.device = torch.device("cpu")
+
+    def vector(self, n):
+        return torch.zeros(n, dtype=torch.float64)
+
+    def cg(self, psi, esp, res, ncg, mloop, mode):
+        u, e, r, _ = self.oracle.conjugate_gradient(np.asfortranarray(psi.numpy()), ncg, mloop)
+        psi.numpy()[:] = u
+        esp.numpy()[:] = e
+        res.numpy()[:] = r
+
+    def hamiltonian(self, psi, hpsi):
+        hpsi.numpy()[:] = self.oracle.hamiltonian(np.asfortranarray(psi.numpy()))
 
 
 # ------------------------------------------------------------ index maps
@@ -239,3 +265,103 @@ def test_one_rank_is_its_own_neighbour():
     hpsi = sol.empty_bands(4)
     sol.hamiltonian(psi, hpsi)
     assert rel(d.own(hpsi).numpy(), O.Oracle(cell).hamiltonian(psi_g)) <= TOL
+
+
+@pytest.mark.parametrize("nb,parts", [(32, 2), (480, 8), (160, 3), (7, 7)])
+def test_split_bands_reference_rule(nb, parts):
+    """parallel_module.f90:366-377: rank j holds as many bands as there are
+    i with mod(i, np_band) == j, the ranks' bands contiguous in order."""
+    counts, offsets = split_bands(nb, parts)
+    assert counts == [sum(1 for i in range(nb) if i % parts == j) for j in range(parts)]
+    assert offsets == [sum(counts[:j]) for j in range(parts)]
+
+
+def _layout_rank(rank, world, port, out):
+    import datetime
+
+    import torch.distributed as dist
+
+    torch.set_num_threads(1)
+    os.environ.update({"MASTER_ADDR": "127.0.0.1", "MASTER_PORT": str(port)})
+    dist.init_process_group("gloo", rank=rank, world_size=world, timeout=datetime.timedelta(seconds=120))
+    try:
+        ngrid, nb = (6, 5, 7), 9
+        L = BandGridLayout(ngrid, nb, rank, world)
+        full = np.arange(L.ml * nb, dtype=np.float64).reshape(nb, L.ml).T  # (ML, nb) global
+        band = api.fortran_empty(L.ml, L.nb_own, device="cpu")
+        band.numpy()[:] = full[:, L.b0:L.b0 + L.nb_own]
+        grid = api.fortran_empty(L.ml_own, nb, device="cpu")
+        grid.fill_(float("nan"))
+        L.to_grid(band, grid, dist)
+        r0, r1 = L.rows[rank]
+        grid_ok = np.array_equal(grid.numpy(), full[r0:r1])
+        grid.mul_(-1.0)
+        back = api.fortran_empty(L.ml, L.nb_own, device="cpu")
+        back.fill_(float("nan"))
+        L.to_band(grid, back, dist)
+        out[rank] = (grid_ok, np.array_equal(back.numpy(), -full[:, L.b0:L.b0 + L.nb_own]))
+    finally:
+        dist.destroy_process_group()
+
+
+@pytest.mark.parametrize("world", [2, 3])
+def test_band_grid_layout_moves(world):
+    """to_grid gives each rank its planes of every band; to_band brings each
+    rank's bands back on the whole grid (7 planes and 9 bands on 2 and 3
+    ranks: uneven parts both ways)."""
+    port = _free_port()
+    mgr = mp.get_context("spawn").Manager()
+    out = mgr.dict()
+    mp.spawn(_layout_rank, args=(world, port, out), nprocs=world, join=True)
+    for r in range(world):
+        assert out[r] == (True, True), (r, out[r])
+
+
+def _iter_rank(rank, world, port, name, nb, out):
+    import datetime
+
+    import torch.distributed as dist
+
+    torch.set_num_threads(1)
+    os.environ.update({"MASTER_ADDR": "127.0.0.1", "MASTER_PORT": str(port)})
+    dist.init_process_group("gloo", rank=rank, world_size=world, timeout=datetime.timedelta(seconds=120))
+    try:
+        cell = build_cell(name, with_duv=False)
+        o = O.Oracle(cell)
+        start = o.gram_schmidt_t(np.asfortranarray(cell.psi0(nb)))
+        L = BandGridLayout(cell.ngrid, nb, rank, world)
+        it = BandGridIteration(L, OracleBandBackend(cell), dist)
+        psi = api.fortran_empty(cell.ML, L.nb_own, device="cpu")
+        psi.numpy()[:] = start[:, L.b0:L.b0 + L.nb_own]
+        esp = torch.zeros(nb, dtype=torch.float64)
+        res = torch.zeros(nb, dtype=torch.float64)
+        it.iterate(psi, esp, res, ncg=4, mloop=3)
+        out[rank] = (psi.numpy().copy(), esp.numpy().copy(), res.numpy().copy())
+    finally:
+        dist.destroy_process_group()
+
+
+@pytest.mark.parametrize("world,name", [(2, "si8"), (3, "si8_g12")])
+def test_band_grid_iteration_matches_single_domain(world, name):
+    """One iteration with the CG on each rank's bands and the Rayleigh-Ritz
+    step on each rank's planes against the single-domain oracle iteration
+    (conjugate_gradient -> gram_schmidt_t -> subspace_diag_la): CG residuals
+    bitwise (the CG is band by band), eigenvalues 1e-12, orthonormal bands
+    spanning the same eigenvectors."""
+    nb = 16
+    O.lib()
+    port = _free_port()
+    mgr = mp.get_context("spawn").Manager()
+    out = mgr.dict()
+    mp.spawn(_iter_rank, args=(world, port, name, nb, out), nprocs=world, join=True)
+    cell = build_cell(name, with_duv=False)
+    o = O.Oracle(cell)
+    start = o.gram_schmidt_t(np.asfortranarray(cell.psi0(nb)))
+    u, _, rref, _ = o.conjugate_gradient(start, 4, 3)
+    q, w, _ = o.subspace_diag_la(o.gram_schmidt_t(u))
+    g = np.concatenate([out[r][0] for r in range(world)], axis=1)
+    for r in range(world):
+        assert np.array_equal(out[r][2], rref)
+        assert rel(out[r][1], w) <= TOL
+    assert np.abs(g.T @ g * cell.dV - np.eye(nb)).max() <= 1e-12
+    assert np.abs(np.abs(np.diag(q.T @ g * cell.dV)) - 1.0).max() <= 1e-9
