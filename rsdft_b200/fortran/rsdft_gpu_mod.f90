@@ -18,6 +18,17 @@
 ! gpu_wf_io_write               simple_wf_io_write     io_write_module.f90:19
 ! gpu_wf_io_read                simple_wf_io_read      io_read_module.f90:15
 !
+! Grid split over comm_grid / comm_band (one rank per GPU; the driver keeps
+! its own MPI for the halo planes, the all-reduces and the all-to-alls):
+! gpu_op_local                  op_kinetic + op_localpot on a rank's planes   hamiltonian_module.f90:42,50
+! gpu_op_nonlocal_project       op_ps_nloc2_hp partial projections           ps_nloc2_op_module.f90:161-175
+! gpu_op_nonlocal_add           op_ps_nloc2_hp scatter                       ps_nloc2_op_module.f90:255-263
+! gpu_gram                      the dgemm / dsyr2k partial sums              gram_schmidt_t_module.f90:187,
+!                                                                            subspace_diag_la_module.f90:96
+! gpu_overlap_cholesky          Cholesky of the summed overlap
+! gpu_rr_reduced                reduced eigenproblem, rotation matrix        subspace_diag_la_module.f90:122-200
+! gpu_rotate                    subspace_rotv_sl on a rank's own rows        subspace_rotv_sl_module.f90:92
+!
 ! Real Gamma-point build only (-D_DRSDFT_), one MPI rank per GPU.  Arrays are
 ! passed by address (c_loc); a non-zero status stops the program with the
 ! library's message, the reference's own convention for fatal errors.
@@ -32,7 +43,8 @@ MODULE rsdft_gpu_mod
   PUBLIC :: gpu_init, gpu_setup_grid, gpu_setup_vloc, gpu_setup_nonlocal, gpu_register_wf, gpu_sync_to_host, &
             gpu_sync_to_device, gpu_hamiltonian, gpu_conjugate_gradient, gpu_gram_schmidt, gpu_subspace_diag, &
             gpu_subspace_mate_sl, gpu_subspace_solv_sl, gpu_subspace_rotv_sl, gpu_esp_calc, gpu_calc_force_ps_nloc2, &
-            gpu_calc_density, gpu_wf_io_write, gpu_wf_io_read, gpu_calc_sweep
+            gpu_calc_density, gpu_wf_io_write, gpu_wf_io_read, gpu_calc_sweep, gpu_op_local, &
+            gpu_op_nonlocal_project, gpu_op_nonlocal_add, gpu_gram, gpu_overlap_cholesky, gpu_rr_reduced, gpu_rotate
 
   integer(c_int), parameter, PUBLIC :: RSDFT_MODE_FP64 = 0, RSDFT_MODE_MIXED_BF16X3 = 1, &
                                        RSDFT_MODE_MIXED_TF32 = 2, RSDFT_MODE_MIXED_BF16X2 = 3
@@ -178,6 +190,50 @@ MODULE rsdft_gpu_mod
        integer(c_long), value :: ld
        integer(c_int), value :: mb, mk, ms, io_ctrl
      end function rsdft_gpu_read_wf
+     integer(c_int) function rsdft_gpu_op_local(s, tpsi, htpsi, ld, nb, z0, nz) bind(C, name="rsdft_gpu_op_local")
+       import :: c_int, c_long, c_ptr
+       integer(c_int), value :: s, nb, z0, nz
+       type(c_ptr), value :: tpsi, htpsi
+       integer(c_long), value :: ld
+     end function rsdft_gpu_op_local
+     integer(c_int) function rsdft_gpu_op_nonlocal_project(tpsi, ld, nb, uvunk) &
+          bind(C, name="rsdft_gpu_op_nonlocal_project")
+       import :: c_int, c_long, c_ptr
+       type(c_ptr), value :: tpsi, uvunk
+       integer(c_long), value :: ld
+       integer(c_int), value :: nb
+     end function rsdft_gpu_op_nonlocal_project
+     integer(c_int) function rsdft_gpu_op_nonlocal_add(uvunk, htpsi, ld, nb) bind(C, name="rsdft_gpu_op_nonlocal_add")
+       import :: c_int, c_long, c_ptr
+       type(c_ptr), value :: uvunk, htpsi
+       integer(c_long), value :: ld
+       integer(c_int), value :: nb
+     end function rsdft_gpu_op_nonlocal_add
+     integer(c_int) function rsdft_gpu_gram(a, b, ld, rows, m, n, alpha, sym, c, ldc) bind(C, name="rsdft_gpu_gram")
+       import :: c_int, c_long, c_double, c_ptr
+       type(c_ptr), value :: a, b, c
+       integer(c_long), value :: ld, rows
+       integer(c_int), value :: m, n, sym, ldc
+       real(c_double), value :: alpha
+     end function rsdft_gpu_gram
+     integer(c_int) function rsdft_gpu_overlap_cholesky(mb, s, lds, rinv, ldr, kappa) &
+          bind(C, name="rsdft_gpu_overlap_cholesky")
+       import :: c_int, c_ptr
+       integer(c_int), value :: mb, lds, ldr
+       type(c_ptr), value :: s, rinv, kappa
+     end function rsdft_gpu_overlap_cholesky
+     integer(c_int) function rsdft_gpu_rr_reduced(mb, rinv, ldr, hsub, ldh, esp, w, ldw) &
+          bind(C, name="rsdft_gpu_rr_reduced")
+       import :: c_int, c_ptr
+       integer(c_int), value :: mb, ldr, ldh, ldw
+       type(c_ptr), value :: rinv, hsub, esp, w
+     end function rsdft_gpu_rr_reduced
+     integer(c_int) function rsdft_gpu_rotate(unk, ld, rows, mb, v, ldv) bind(C, name="rsdft_gpu_rotate")
+       import :: c_int, c_long, c_ptr
+       type(c_ptr), value :: unk, v
+       integer(c_long), value :: ld, rows
+       integer(c_int), value :: mb, ldv
+     end function rsdft_gpu_rotate
   end interface
 
 CONTAINS
@@ -292,6 +348,73 @@ CONTAINS
     call check(rsdft_gpu_conjugate_gradient(n1, n2, mb, k, s, c_loc(unk), c_loc(esp), c_loc(res), ncg, mloop, ipc, &
                mode), "conjugate_gradient")
   END SUBROUTINE gpu_conjugate_gradient
+
+  ! Grid split (z planes of a slab extended by Md halo planes either side;
+  ! the halo exchange, the uVunk all-reduce and the MB x MB all-reduces are
+  ! the driver's MPI).  z0 is 0-based: op_local on the own planes of an
+  ! extended slab is z0 = Md, nz = the own plane count.
+  SUBROUTINE gpu_op_local(s, tpsi, htpsi, ld, nb, z0, nz)
+    integer, intent(IN) :: s, ld, nb, z0, nz
+    real(8), intent(IN), target :: tpsi(ld, nb)
+    real(8), intent(INOUT), target :: htpsi(ld, nb)
+    call check(rsdft_gpu_op_local(int(s, c_int), c_loc(tpsi), c_loc(htpsi), int(ld, c_long), int(nb, c_int), &
+               int(z0, c_int), int(nz, c_int)), "op_local")
+  END SUBROUTINE gpu_op_local
+
+  SUBROUTINE gpu_op_nonlocal_project(tpsi, ld, nb, uvunk)
+    integer, intent(IN) :: ld, nb
+    real(8), intent(IN), target :: tpsi(ld, nb)
+    real(8), intent(OUT), target :: uvunk(:, :)
+    call check(rsdft_gpu_op_nonlocal_project(c_loc(tpsi), int(ld, c_long), int(nb, c_int), c_loc(uvunk)), &
+               "op_nonlocal_project")
+  END SUBROUTINE gpu_op_nonlocal_project
+
+  SUBROUTINE gpu_op_nonlocal_add(uvunk, htpsi, ld, nb)
+    integer, intent(IN) :: ld, nb
+    real(8), intent(IN), target :: uvunk(:, :)
+    real(8), intent(INOUT), target :: htpsi(ld, nb)
+    call check(rsdft_gpu_op_nonlocal_add(c_loc(uvunk), c_loc(htpsi), int(ld, c_long), int(nb, c_int)), &
+               "op_nonlocal_add")
+  END SUBROUTINE gpu_op_nonlocal_add
+
+  ! c(1:m, 1:n) = alpha a(1:rows, 1:m)^T b(1:rows, 1:n) (sym = 1: the
+  ! symmetric part of a square product), the partial sum of a rank's rows
+  SUBROUTINE gpu_gram(a, b, ld, rows, m, n, alpha, sym, c)
+    integer, intent(IN) :: ld, rows, m, n, sym
+    real(8), intent(IN) :: alpha
+    real(8), intent(IN), target :: a(ld, m), b(ld, n)
+    real(8), intent(OUT), target :: c(m, n)
+    call check(rsdft_gpu_gram(c_loc(a), c_loc(b), int(ld, c_long), int(rows, c_long), int(m, c_int), &
+               int(n, c_int), alpha, int(sym, c_int), c_loc(c), int(m, c_int)), "gram")
+  END SUBROUTINE gpu_gram
+
+  ! s = R^T R, rinv = R^-1 (upper); kappa = (max diag R / min diag R)^2
+  SUBROUTINE gpu_overlap_cholesky(mb, s, rinv, kappa)
+    integer, intent(IN) :: mb
+    real(8), intent(IN), target :: s(mb, mb)
+    real(8), intent(OUT), target :: rinv(mb, mb)
+    real(8), intent(OUT), target :: kappa
+    call check(rsdft_gpu_overlap_cholesky(int(mb, c_int), c_loc(s), int(mb, c_int), c_loc(rinv), int(mb, c_int), &
+               c_loc(kappa)), "overlap_cholesky")
+  END SUBROUTINE gpu_overlap_cholesky
+
+  ! R^-T hsub R^-1 = V diag(esp) V^T, w = R^-1 V
+  SUBROUTINE gpu_rr_reduced(mb, rinv, hsub, esp, w)
+    integer, intent(IN) :: mb
+    real(8), intent(IN), target :: rinv(mb, mb), hsub(mb, mb)
+    real(8), intent(OUT), target :: esp(mb), w(mb, mb)
+    call check(rsdft_gpu_rr_reduced(int(mb, c_int), c_loc(rinv), int(mb, c_int), c_loc(hsub), int(mb, c_int), &
+               c_loc(esp), c_loc(w), int(mb, c_int)), "rr_reduced")
+  END SUBROUTINE gpu_rr_reduced
+
+  ! unk(1:rows, 1:mb) <- unk v on a registered unk (a rank's own rows)
+  SUBROUTINE gpu_rotate(unk, ld, rows, mb, v)
+    integer, intent(IN) :: ld, rows, mb
+    real(8), intent(INOUT), target :: unk(ld, mb)
+    real(8), intent(IN), target :: v(mb, mb)
+    call check(rsdft_gpu_rotate(c_loc(unk), int(ld, c_long), int(rows, c_long), int(mb, c_int), c_loc(v), &
+               int(mb, c_int)), "rotate")
+  END SUBROUTINE gpu_rotate
 
   ! calc_sweep's loop for one Gamma point: unk(ML, MB, nspin) stays on the
   ! device (register it first); esp holds esp0 on entry; ierr_out is the
