@@ -218,6 +218,15 @@ class SlabDomain:
                 k += r.n
 
 
+def _share_stream(gpu, device) -> None:
+    """Bind the library to torch's current stream on ``device``: the layout
+    moves and the collectives are torch work (NCCL waits on the current
+    stream), so the library's kernels must be ordered on that stream too."""
+    import torch
+
+    gpu.set_stream(torch.cuda.current_stream(device).cuda_stream)
+
+
 class GpuSlabBackend:
     """The per-slab compute on this rank's GPU through the library's entries:
     op_local on the own planes, projection partials and scatter, Gram sums,
@@ -228,6 +237,7 @@ class GpuSlabBackend:
 
         self.gpu, self.domain = gpu, domain
         self.device = torch.device("cuda", gpu.device)
+        _share_stream(gpu, self.device)
         self.cell = domain.slab_cell(cell)
         gpu.setup(self.cell, with_forces=False)
         self.nzlma = self.cell.nzlma
@@ -419,6 +429,7 @@ class GpuBandBackend:
 
         self.gpu = gpu
         self.device = torch.device("cuda", gpu.device)
+        _share_stream(gpu, self.device)
         gpu.setup(cell, with_forces=False)
         self.ml = int(cell.ML)
         self.dV = float(cell.dV)
