@@ -295,9 +295,9 @@ def run_reference(args, rank, world):
 
 # ------------------------------------------------------------- our arm
 # DRAM bytes (read + write) of one hpsi call per band, from the ncu capture of
-# the three hpsi kernels on Si216 with 64 bands (k_nl_project 168.5 MB,
-# k_stencil_tma 380.1 MB, k_nl_scatter 208.8 MB), scaled by the band count.
-HPSI_TRAFFIC_PER_BAND = {"si216": (168.5e6 + 380.1e6 + 208.8e6) / 64}
+# the three hpsi kernels on Si216 with 64 bands (k_nl_project 167.8 MB,
+# k_stencil_tma 379.7 MB, k_nl_scatter 210.8 MB), scaled by the band count.
+HPSI_TRAFFIC_PER_BAND = {"si216": (167.8e6 + 379.7e6 + 210.8e6) / 64}
 
 
 def hpsi_bytes(cell, nb):
