@@ -709,8 +709,25 @@ int cg_device_f32_staged(const double* unk_host, double* unk_dev, long ld, int m
 }
 
 int cg_device(double* unk, long ld, int mb, int spin, double* esp, double* res, int ncg, int mloop, int ipc,
-              int mode) {
-    if (mode == RSDFT_MODE_FP64) return cg_run<double>(unk, ld, mb, spin, esp, res, ncg, mloop, ipc);
+              int mode, const double** hx_out) {
+    if (mode == RSDFT_MODE_FP64) {
+        RS_CHECK(cg_run<double>(unk, ld, mb, spin, esp, res, ncg, mloop, ipc));
+        if (hx_out) {
+            // as in cg_device_f32: the CG's hx is H x unless an update was
+            // rejected (cg_module.f90:359-365)
+            Context& c = ctx();
+            *hx_out = nullptr;
+            double* hx = nullptr;
+            int* flags = nullptr;
+            RS_CHECK(workspace_t("cg_vec", (size_t)ld * mb * 7, &hx));
+            RS_CHECK(workspace_t("cg_flags", (size_t)mb * 4 + 1, &flags));
+            int rej = 1;
+            RS_CUDA(cudaMemcpyAsync(&rej, flags + 4 * mb, sizeof(int), cudaMemcpyDeviceToHost, c.stream));
+            RS_CUDA(cudaStreamSynchronize(c.stream));
+            if (rej == 0) *hx_out = hx;
+        }
+        return RSDFT_OK;
+    }
     Context& c = ctx();
     float* x32 = nullptr;
     const long n = ld * (long)mb;

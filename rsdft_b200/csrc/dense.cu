@@ -244,7 +244,8 @@ static double fused_rr_kappa_max(int mode) {
 // overlap is ill-conditioned (diag(R) spread beyond fused_rr_kappa_max^(1/2); one
 // Cholesky pass then loses orthogonality), the explicit CholeskyQR2 +
 // subspace_diag path runs instead.
-int orth_subspace_diag_device(double* psi, long ld, int mb, int spin, double* esp, int mode) {
+int orth_subspace_diag_device(double* psi, long ld, int mb, int spin, double* esp, int mode,
+                              const double* hpsi_in) {
     Context& c = ctx();
     double *hpsi = nullptr, *S = nullptr, *H = nullptr, *T = nullptr, *mm = nullptr;
     int* dinfo = nullptr;
@@ -255,12 +256,13 @@ int orth_subspace_diag_device(double* psi, long ld, int mb, int spin, double* es
     RS_CHECK(workspace_t("osd_minmax", 2, &mm));
     RS_CHECK(workspace_t("gs_info", 4, &dinfo));
     const void* split = nullptr;
-    RS_CHECK(hpsi_device<double>(psi, hpsi, ld, mb, spin, nullptr));
+    if (!hpsi_in) RS_CHECK(hpsi_device<double>(psi, hpsi, ld, mb, spin, nullptr));
+    const double* hp = hpsi_in ? hpsi_in : hpsi;
     if (mode == RSDFT_MODE_FP64) {
         RS_CHECK(gemm_tn_splitk(psi, psi, ld, mb, mb, c.dV, 0, S));
-        RS_CHECK(gemm_tn_splitk(psi, hpsi, ld, mb, mb, c.dV, 1, H, true));
+        RS_CHECK(gemm_tn_splitk(psi, hp, ld, mb, mb, c.dV, 1, H, true));
     } else {
-        RS_CHECK(gram_mixed_pair(psi, hpsi, ld, mb, c.dV, mode, S, H, &split));
+        RS_CHECK(gram_mixed_pair(psi, hp, ld, mb, c.dV, mode, S, H, &split));
     }
     RS_CHECK(potrf_upper(S, mb, dinfo, "orth_subspace_diag: overlap Cholesky"));
     launch(k_diag_minmax, 1, 256, 0, c.stream, S, mb, mb, mm);
@@ -331,8 +333,11 @@ namespace rsdft {
 
 int sweep_device(double* d, long ld, int mb, int s, double* W, double* R, int ncg, int mloop, int ipc, int mode) {
     if (mode == RSDFT_MODE_FP64) {
-        RS_CHECK(cg_device(d, ld, mb, s, W, R, ncg, mloop, ipc, mode));
-        return orth_subspace_diag_device(d, ld, mb, s, W, mode);
+        // the CG's H x goes on to the Rayleigh-Ritz step, as in the mixed
+        // forms below
+        const double* hx = nullptr;
+        RS_CHECK(cg_device(d, ld, mb, s, W, R, ncg, mloop, ipc, mode, &hx));
+        return orth_subspace_diag_device(d, ld, mb, s, W, mode, hx);
     }
     float* x32 = nullptr;
     const float* hx = nullptr;

@@ -59,8 +59,11 @@ int gram_schmidt_device(double* psi, long ld, int nb, int mode);
 // Rayleigh-Ritz (subspace_diag_la) on device data.
 int subspace_diag_device(double* psi, long ld, int mb, int spin, double* esp_dev, int mode);
 
-// Gram-Schmidt + Rayleigh-Ritz as one step (device data).
-int orth_subspace_diag_device(double* psi, long ld, int mb, int spin, double* esp_dev, int mode);
+// Gram-Schmidt + Rayleigh-Ritz as one step (device data).  hpsi, when
+// given, is H psi already formed (leading dimension ld); else it is formed
+// here.
+int orth_subspace_diag_device(double* psi, long ld, int mb, int spin, double* esp_dev, int mode,
+                              const double* hpsi_in = nullptr);
 
 // One calc_sweep step for spin `spin` on device bands: conjugate_gradient,
 // then gram_schmidt + subspace_diag as one Rayleigh-Ritz step; W, R receive
@@ -96,8 +99,10 @@ int orth_subspace_diag_f32(const float* x32, const float* h32, double* psi, long
 // available, so the caller takes cuSOLVER's syevd.
 int syevd_fast(double* A, int n, double* W, cublasFillMode_t uplo);
 
-// CG over all bands (device data).
+// CG over all bands (device data).  hx_out (FP64 only, if given) receives
+// the sweep's H x (in the CG workspace), or null when an update was rejected
+// and H x must be formed again.
 int cg_device(double* unk, long ld, int mb, int spin, double* esp_dev, double* res_dev, int ncg, int mloop,
-              int ipc, int mode);
+              int ipc, int mode, const double** hx_out = nullptr);
 
 }  // namespace rsdft

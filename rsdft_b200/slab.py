@@ -218,6 +218,23 @@ class SlabDomain:
                 k += r.n
 
 
+def _all_reduce(dist, t):
+    """Sum t over the ranks in place (no process group: t as it is).  NCCL
+    takes contiguous tensors only, so a column-major matrix is reduced
+    through its storage (the row-major transpose view)."""
+    if dist is None:
+        return t
+    if t.is_contiguous():
+        dist.all_reduce(t)
+    elif t.dim() == 2 and t.t().is_contiguous():
+        dist.all_reduce(t.t())
+    else:
+        buf = t.contiguous()
+        dist.all_reduce(buf)
+        t.copy_(buf)
+    return t
+
+
 def _share_stream(gpu, device) -> None:
     """Bind the library to torch's current stream on ``device``: the layout
     moves and the collectives are torch work (NCCL waits on the current
@@ -286,9 +303,7 @@ class SlabSolver:
             raise ValueError("SlabSolver: more than one rank needs a process group")
 
     def _allreduce(self, t):
-        if self.dist is not None:
-            self.dist.all_reduce(t)
-        return t
+        return _all_reduce(self.dist, t)
 
     def empty_bands(self, nb):
         """Extended-slab bands (ml_ext, nb), column-major."""
@@ -489,9 +504,7 @@ class BandGridIteration:
             raise ValueError("BandGridIteration: more than one rank needs a process group")
 
     def _allreduce(self, t):
-        if self.dist is not None:
-            self.dist.all_reduce(t)
-        return t
+        return _all_reduce(self.dist, t)
 
     def _gram(self, a, c, sym):
         out = self.b.empty(self.L.nb, self.L.nb)

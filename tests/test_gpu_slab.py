@@ -196,3 +196,37 @@ def test_band_grid_iteration_virtual_ranks_si64(gpu, cells, nranks):
     gr = host(ref)
     assert np.abs(g.T @ g * c.dV - np.eye(nb)).max() <= 1e-12
     assert np.abs(np.abs(np.diag(gr.T @ g * c.dV)) - 1.0).max() <= 1e-9
+
+
+def test_band_grid_iteration_nccl_one_rank(gpu, cells):
+    """The split iteration's driver over a real NCCL process group of one
+    rank: its all-reduces of the Gram sums and the residuals run on the
+    library's stream (the backend binds the library to torch's current
+    stream), same result as without a process group."""
+    import datetime
+    import socket
+
+    import torch.distributed as dist
+
+    c = cells("si8")
+    nb = 16
+    q = np.asfortranarray(O.Oracle(c).gram_schmidt_t(np.asfortranarray(c.psi0(nb))))
+    with socket.socket() as s:
+        s.bind(("127.0.0.1", 0))
+        port = s.getsockname()[1]
+    dist.init_process_group("nccl", init_method=f"tcp://127.0.0.1:{port}", rank=0, world_size=1,
+                            timeout=datetime.timedelta(seconds=60))
+    try:
+        out = []
+        for group in (dist, None):
+            it = BandGridIteration(BandGridLayout(c.ngrid, nb, 0, 1), GpuBandBackend(gpu, c), group)
+            u = dev(q)
+            esp = torch.zeros(nb, dtype=torch.float64, device="cuda")
+            res = torch.zeros_like(esp)
+            it.iterate(u, esp, res, ncg=4, mloop=3)
+            torch.cuda.synchronize()
+            out.append((host(u), host(esp), host(res)))
+    finally:
+        dist.destroy_process_group()
+    for a, b in zip(out[0], out[1]):
+        assert np.array_equal(a, b)
