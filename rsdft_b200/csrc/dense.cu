@@ -31,12 +31,6 @@ __global__ void k_zero_upper(double* a, int n, int lda) {
     if (i < n && i < j) a[(long)j * lda + i] = 0.0;
 }
 
-__global__ void k_zero_lower(double* a, int n, int lda) {
-    int i = blockIdx.x * blockDim.x + threadIdx.x;  // row
-    int j = blockIdx.y;                              // column
-    if (i < n && i > j) a[(long)j * lda + i] = 0.0;
-}
-
 __global__ void k_widen(const float* __restrict__ a, double* __restrict__ b, long n) {
     for (long i = (long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long)gridDim.x * blockDim.x)
         b[i] = (double)a[i];
@@ -80,30 +74,86 @@ static int check_info(int* dinfo, const char* what) {
 }
 
 // S (nb x nb) = R^T R in place: the upper triangle becomes R
-static int potrf_upper(double* S, int nb, int* dinfo, const char* what) {
+// (check = false: the caller reads *dinfo back itself, with its next read)
+static int potrf_upper(double* S, int nb, int* dinfo, const char* what, bool check = true) {
     Context& c = ctx();
     int lwork = 0;
     RS_SOLVER(cusolverDnDpotrf_bufferSize(c.solver, CUBLAS_FILL_MODE_UPPER, nb, S, nb, &lwork));
     double* work = nullptr;
     RS_CHECK(workspace_t("gs_potrf", (size_t)lwork + 1, &work));
     RS_SOLVER(cusolverDnDpotrf(c.solver, CUBLAS_FILL_MODE_UPPER, nb, S, nb, work, lwork, dinfo));
-    return check_info(dinfo, what);
+    return check ? check_info(dinfo, what) : RSDFT_OK;
+}
+
+// One read-back of the Cholesky status and of diag(R)'s min and max (the
+// spread that picks the one-step Rayleigh-Ritz or the explicit path).
+static int read_cholesky(const int* dinfo, const double* mm, double* hmm, const char* what) {
+    Context& c = ctx();
+    int info = 0;
+    RS_CUDA(cudaMemcpyAsync(hmm, mm, 2 * sizeof(double), cudaMemcpyDeviceToHost, c.stream));
+    RS_CUDA(cudaMemcpyAsync(&info, dinfo, sizeof(int), cudaMemcpyDeviceToHost, c.stream));
+    RS_CUDA(cudaStreamSynchronize(c.stream));
+    if (info != 0) {
+        set_error("%s: info=%d", what, info);
+        return RSDFT_ESOLVER;
+    }
+    return RSDFT_OK;
+}
+
+// X = R^-1 for the upper triangular R (n x n, column-major, leading
+// dimension n), X R = I read row by row: one warp per row i of X,
+//   X(i, j) = 0 (j < i),  X(i, i) = 1 / R(i, i),
+//   X(i, j) = -(sum_{l=i}^{j-1} X(i, l) R(l, j)) / R(j, j)   (j > i),
+// each sum split over the lanes (l = i + lane, i + lane + 32, ..., then a
+// fixed xor tree), the row kept in shared memory, R's columns read straight
+// from global memory (each column is shared by the warps of every row).
+// The callers factor R from an overlap whose Cholesky succeeded, so its
+// diagonal is positive.
+constexpr int TI_W = 4;  // rows (warps) per CTA
+
+__global__ void __launch_bounds__(32 * TI_W) k_trtri_rows(const double* __restrict__ R, int n,
+                                                         double* __restrict__ X) {
+    extern __shared__ double ti_sm[];
+    double* dinv = ti_sm;                // 1 / R(j, j)
+    const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    double* xr = ti_sm + n + (size_t)w * n;  // this warp's row of X
+    for (int j = threadIdx.x; j < n; j += blockDim.x) dinv[j] = 1.0 / R[(long)j * n + j];
+    __syncthreads();
+    const int i = blockIdx.x * TI_W + w;
+    if (i >= n) return;
+    for (int j = lane; j < i; j += 32) X[(long)j * n + i] = 0.0;
+    if (lane == 0) {
+        xr[i] = dinv[i];
+        X[(long)i * n + i] = dinv[i];
+    }
+    __syncwarp();
+    for (int j = i + 1; j < n; ++j) {
+        const double* rc = R + (long)j * n;
+        double s = 0.0;
+        for (int l = i + lane; l < j; l += 32) s = fma(xr[l], rc[l], s);
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+        if (lane == 0) {
+            const double v = -s * dinv[j];
+            xr[j] = v;
+            X[(long)j * n + i] = v;
+        }
+        __syncwarp();
+    }
 }
 
 // R (upper triangle of S) -> R^-1 in place, the lower triangle zeroed
 static int trtri_upper(double* S, int nb, int* dinfo, const char* what) {
+    (void)dinfo;
+    (void)what;
     Context& c = ctx();
-    size_t dws = 0, hws = 0;
-    RS_SOLVER(cusolverDnXtrtri_bufferSize(c.solver, CUBLAS_FILL_MODE_UPPER, CUBLAS_DIAG_NON_UNIT, nb, CUDA_R_64F, S,
-                                          nb, &dws, &hws));
-    void* dw = nullptr;
-    RS_CHECK(workspace("gs_trtri", dws + 16, &dw));
-    char* hw = host_workspace(hws + 16);
-    RS_SOLVER(cusolverDnXtrtri(c.solver, CUBLAS_FILL_MODE_UPPER, CUBLAS_DIAG_NON_UNIT, nb, CUDA_R_64F, S, nb, dw,
-                               dws, hw, hws, dinfo));
-    RS_CHECK(check_info(dinfo, what));
-    launch(k_zero_lower, dim3(div_up(nb, 128), nb), 128, 0, c.stream, S, nb, nb);
+    double* X = nullptr;
+    RS_CHECK(workspace_t("gs_trtri_x", (size_t)nb * nb, &X));
+    const size_t smem = (size_t)(TI_W + 1) * nb * sizeof(double);
+    RS_CHECK(set_smem_optin((const void*)k_trtri_rows, (int)smem));
+    launch(k_trtri_rows, div_up(nb, TI_W), 32 * TI_W, smem, c.stream, (const double*)S, nb, X);
     RS_LAUNCH();
+    RS_CUDA(cudaMemcpyAsync(S, X, sizeof(double) * (size_t)nb * nb, cudaMemcpyDeviceToDevice, c.stream));
     return RSDFT_OK;
 }
 
@@ -264,12 +314,11 @@ int orth_subspace_diag_device(double* psi, long ld, int mb, int spin, double* es
     } else {
         RS_CHECK(gram_mixed_pair(psi, hp, ld, mb, c.dV, mode, S, H, &split));
     }
-    RS_CHECK(potrf_upper(S, mb, dinfo, "orth_subspace_diag: overlap Cholesky"));
+    RS_CHECK(potrf_upper(S, mb, dinfo, "orth_subspace_diag: overlap Cholesky", false));
     launch(k_diag_minmax, 1, 256, 0, c.stream, S, mb, mb, mm);
     RS_LAUNCH();
     double hmm[2] = {0.0, 0.0};
-    RS_CUDA(cudaMemcpyAsync(hmm, mm, sizeof(hmm), cudaMemcpyDeviceToHost, c.stream));
-    RS_CUDA(cudaStreamSynchronize(c.stream));
+    RS_CHECK(read_cholesky(dinfo, mm, hmm, "orth_subspace_diag: overlap Cholesky"));
     if (!(hmm[0] > 0.0) || (hmm[1] / hmm[0]) * (hmm[1] / hmm[0]) > fused_rr_kappa_max(mode)) {
         RS_CHECK(gram_schmidt_device(psi, ld, mb, mode));
         return subspace_diag_device(psi, ld, mb, spin, esp, mode);
@@ -310,12 +359,11 @@ int orth_subspace_diag_f32(const float* x32, const float* hx, double* psi, long 
     }
     const void* split = nullptr;
     RS_CHECK(gram_mixed_pair(x32, h32, ld, mb, c.dV, mode, S, H, &split));
-    RS_CHECK(potrf_upper(S, mb, dinfo, "eigensolver_sweep: overlap Cholesky"));
+    RS_CHECK(potrf_upper(S, mb, dinfo, "eigensolver_sweep: overlap Cholesky", false));
     launch(k_diag_minmax, 1, 256, 0, c.stream, S, mb, mb, mm);
     RS_LAUNCH();
     double hmm[2] = {0.0, 0.0};
-    RS_CUDA(cudaMemcpyAsync(hmm, mm, sizeof(hmm), cudaMemcpyDeviceToHost, c.stream));
-    RS_CUDA(cudaStreamSynchronize(c.stream));
+    RS_CHECK(read_cholesky(dinfo, mm, hmm, "eigensolver_sweep: overlap Cholesky"));
     if (!(hmm[0] > 0.0) || (hmm[1] / hmm[0]) * (hmm[1] / hmm[0]) > fused_rr_kappa_max(mode)) {
         launch(k_widen, 4 * c.num_sms, 256, 0, c.stream, x32, psi, ld * (long)mb);
         RS_LAUNCH();

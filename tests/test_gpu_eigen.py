@@ -66,3 +66,23 @@ def test_subspace_solv_repeatable(gpu):
     w1, v1 = solve(gpu, a)
     w2, v2 = solve(gpu, a)
     assert np.array_equal(w1, w2) and np.array_equal(v1, v2)
+
+
+@pytest.mark.parametrize("n,spread", [(1, 1.0), (37, 1.0), (480, 30.0), (600, 300.0)])
+def test_overlap_cholesky_inverse(gpu, n, spread):
+    """rsdft_gpu_overlap_cholesky: S = R^T R and rinv = R^-1 (upper, the
+    lower triangle zero) against LAPACK's Cholesky and an explicit inverse,
+    and kappa = (max diag R / min diag R)^2, for overlaps of the shapes a CG
+    sweep leaves (near the identity, columns of spread norms)."""
+    rng = np.random.default_rng(n)
+    b = rng.standard_normal((4 * n + 8, n)) * np.linspace(1.0, np.sqrt(spread), n)
+    s = np.asfortranarray(b.T @ b / (4 * n + 8))
+    rinv = np.zeros((n, n), order="F")
+    kappa = gpu.overlap_cholesky(s, rinv)
+    r = np.linalg.cholesky(s).T
+    ref = np.linalg.inv(r)
+    assert np.abs(rinv - ref).max() <= 1e-12 * np.abs(ref).max() * max(1.0, np.linalg.cond(r))
+    assert np.abs(np.tril(rinv, -1)).max() == 0.0
+    assert np.abs(rinv @ r - np.eye(n)).max() <= 1e-12 * max(1.0, np.linalg.cond(r))
+    d = np.diag(r)
+    assert abs(kappa - (d.max() / d.min()) ** 2) <= 1e-12 * kappa
