@@ -3,7 +3,7 @@
 ``python -m rsdft_b200.build`` compiles every ``.cu`` file with nvcc for
 ``-gencode arch=compute_100a,code=sm_100a`` into ``rsdft_b200/_build`` and
 links the shared library in-tree (``rsdft_b200/librsdft_gpu.so``) against
-cuBLAS and cuSOLVER.  Objects are rebuilt when their source or a header is
+cuSOLVER.  Objects are rebuilt when their source or a header is
 newer.
 """
 from __future__ import annotations
@@ -39,7 +39,7 @@ def _cuda_lib_dir() -> str:
     root = os.path.dirname(os.path.dirname(os.path.realpath(nvcc)))
     for d in ("lib64", os.path.join("targets", "x86_64-linux", "lib")):
         p = os.path.join(root, d)
-        if os.path.exists(os.path.join(p, "libcublas.so")):
+        if os.path.exists(os.path.join(p, "libcusolver.so")):
             return p
     return os.path.join(root, "lib64")
 
@@ -87,7 +87,7 @@ def build(verbose: bool = False, extra_flags=None) -> str:
         list(ex.map(run, jobs))
     if jobs or not os.path.exists(LIB) or any(os.path.getmtime(o) > os.path.getmtime(LIB) for o in objs):
         libdir = _cuda_lib_dir()
-        link = [nvcc, *ARCH, "-shared", "-o", LIB, *objs, "-L", libdir, "-lcublas", "-lcusolver",
+        link = [nvcc, *ARCH, "-shared", "-o", LIB, *objs, "-L", libdir, "-lcusolver",
                 "-Xlinker", "-rpath=" + libdir]
         run(link)
     return LIB

@@ -240,9 +240,6 @@ int rsdft_gpu_init(int device) {
     RS_CUDA(cudaSetDevice(device));
     RS_CUDA(cudaStreamCreateWithFlags(&c.stream, cudaStreamNonBlocking));
     c.own_stream = true;
-    RS_BLAS(cublasCreate(&c.blas));
-    RS_BLAS(cublasSetStream(c.blas, c.stream));
-    RS_BLAS(cublasSetPointerMode(c.blas, CUBLAS_POINTER_MODE_HOST));
     RS_SOLVER(cusolverDnCreate(&c.solver));
     RS_SOLVER(cusolverDnSetStream(c.solver, c.stream));
     RS_CUDA(cudaDeviceGetAttribute(&c.num_sms, cudaDevAttrMultiProcessorCount, device));
@@ -283,7 +280,6 @@ int rsdft_gpu_finalize(void) {
                     c.gpt_ptr, c.gpt_grp, c.gpt_uv4, c.gpt_uv4_32, c.nl_pts, c.nl_ptr};
     for (void* p : ptrs)
         if (p) cudaFree(p);
-    if (c.blas) cublasDestroy(c.blas);
     if (c.solver) cusolverDnDestroy(c.solver);
     if (c.own_stream && c.stream) cudaStreamDestroy(c.stream);
     c = Context();
@@ -315,7 +311,6 @@ int rsdft_gpu_set_stream(void* stream) {
         RS_CUDA(cudaStreamCreateWithFlags(&c.stream, cudaStreamNonBlocking));
         c.own_stream = true;
     }
-    RS_BLAS(cublasSetStream(c.blas, c.stream));
     RS_SOLVER(cusolverDnSetStream(c.solver, c.stream));
     return RSDFT_OK;
 }

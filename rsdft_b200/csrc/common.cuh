@@ -4,7 +4,6 @@
 #pragma once
 
 #include <cuda_runtime.h>
-#include <cublas_v2.h>
 #include <cusolverDn.h>
 
 #include <cstdint>
@@ -64,7 +63,6 @@ struct Context {
     cudaStream_t copy_stream = nullptr;  // host<->device staging that overlaps compute
     static constexpr int NEV = 16;
     cudaEvent_t ev[NEV] = {};
-    cublasHandle_t blas = nullptr;
     cusolverDnHandle_t solver = nullptr;
     int num_sms = 0;
     int* err_flag = nullptr;  // set by kernels whose bounded waits ran out
@@ -133,16 +131,6 @@ const char* get_error();
         if (_e != cudaSuccess) {                                                      \
             ::rsdft::set_error("%s:%d %s: %s", __FILE__, __LINE__, #call,             \
                                cudaGetErrorString(_e));                               \
-            return RSDFT_ECUDA;                                                       \
-        }                                                                             \
-    } while (0)
-
-#define RS_BLAS(call)                                                                 \
-    do {                                                                              \
-        cublasStatus_t _s = (call);                                                   \
-        if (_s != CUBLAS_STATUS_SUCCESS) {                                            \
-            ::rsdft::set_error("%s:%d %s: cublas status %d", __FILE__, __LINE__,     \
-                               #call, (int)_s);                                       \
             return RSDFT_ECUDA;                                                       \
         }                                                                             \
     } while (0)

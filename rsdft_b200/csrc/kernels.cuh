@@ -53,7 +53,8 @@ __device__ __forceinline__ void block_sum_n(double (&v)[K], double* sh) {
 }
 
 // Symmetric-positive-definite orthonormalisation (CholeskyQR2 in the dV
-// metric) of nb columns, FP64 (cuBLAS/cuSOLVER) or mixed (tensor cores).
+// metric) of nb columns, FP64 (DMMA Gram and rotation, cuSOLVER Cholesky,
+// hand-written triangular inverse) or mixed (tcgen05 tensor cores).
 int gram_schmidt_device(double* psi, long ld, int nb, int mode);
 
 // Rayleigh-Ritz (subspace_diag_la) on device data.
