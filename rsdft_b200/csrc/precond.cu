@@ -400,6 +400,12 @@ __global__ void __launch_bounds__(384, PcStep<K, STORE>::CTAS) k_pc_tma(const __
                 T w[NV * VX];
 #pragma unroll
                 for (int j = 0; j < NV; ++j) {
+                    if (j == 1) {
+                        // the centre vector: the row's own, read with the y window
+#pragma unroll
+                        for (int e = 0; e < VX; ++e) w[VX + e] = c[r * VX + e];
+                        continue;
+                    }
                     int xx = xw + VX * j;
                     xx += xx < 0 ? n1 : (xx >= n1 ? -n1 : 0);
                     VT::get(*reinterpret_cast<const V*>(rp + xx), w + j * VX);
