@@ -338,6 +338,32 @@ int rsdft_gpu_write_wf(const char *path, const double *unk, long ld, int mb, int
 int rsdft_gpu_read_wf(const char *path, double *unk, long ld, int mb, int mk, int ms, int io_ctrl,
                       const int *ngrid, double *occ, int *info);
 
+/* ------------------------------------------ density and potential file */
+
+/* Write the density/potential file of RSDFT (vrho.dat1) record for record:
+ * the version record, ML and ngrid, LL2(3,ML) (x fastest), the lattice
+ * aa(3,3), Nelement and Natom, aa_atom(3,natom), ki_atom(natom),
+ * zn_atom(nelement), efermi, then for each spin s rho(:,s), vloc(:,s), vh
+ * (s = 1 only) and vxc(:,s).  rho, vloc and vxc are (ML, nspin) arrays, vh
+ * is (ML); each may be a host array, a registered one (its device mirror is
+ * written) or device memory.
+ * (replaces the density/potential branch of write_data, io_module.f90:97-226,
+ * for one process) */
+int rsdft_gpu_write_vrho(const char *path, const int *ngrid, const double *aa, int nelement, int natom,
+                         const double *aa_atom, const int *ki_atom, const int *zn_atom, double efermi, int nspin,
+                         const double *rho, const double *vloc, const double *vh, const double *vxc);
+
+/* Read a density/potential file written by RSDFT (with or without the
+ * version record) into rho, vloc, vxc (ML, nspin) and vh (ML), each a host
+ * array, a registered one or device memory, or NULL to skip it; the grid must
+ * match ngrid and the values are placed through the file's LL2 map.
+ * *efermi (if not NULL) receives the Fermi energy of a versioned file and is
+ * left untouched for an unversioned one, as in the reference.
+ * (replaces the VRHO branch of read_data, io_module.f90:283-432, for one
+ * process) */
+int rsdft_gpu_read_vrho(const char *path, const int *ngrid, int nspin, double *rho, double *vloc, double *vh,
+                        double *vxc, double *efermi);
+
 #ifdef __cplusplus
 }
 #endif

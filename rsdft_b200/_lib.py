@@ -61,6 +61,9 @@ SIGNATURES = {
     "rsdft_gpu_write_wf": (_c_int, [ctypes.c_char_p, _vp, _c_long, _c_int, _c_int, _c_int, _c_int, _c_int, _c_int,
                                     _c_int, _vp, _vp, _vp, _vp, _c_int, _vp]),
     "rsdft_gpu_read_wf": (_c_int, [ctypes.c_char_p, _vp, _c_long, _c_int, _c_int, _c_int, _c_int, _vp, _vp, _vp]),
+    "rsdft_gpu_write_vrho": (_c_int, [ctypes.c_char_p, _vp, _vp, _c_int, _c_int, _vp, _vp, _vp, ctypes.c_double,
+                                      _c_int, _vp, _vp, _vp, _vp]),
+    "rsdft_gpu_read_vrho": (_c_int, [ctypes.c_char_p, _vp, _c_int, _vp, _vp, _vp, _vp, _vp]),
 }
 
 STATUS = {0: "OK", -1: "EINVAL", -2: "ENOTINIT", -3: "ECUDA", -4: "ESOLVER", -5: "ENOMEM", -6: "EUNSUP", -7: "ETIMEOUT"}

@@ -19,6 +19,8 @@ replace (j-iwata/RSDFT v1.3.0, src/):
 ``calc_sweep(unk, esp, res, occ,..)``  sweep_module.f90:60 (calc_sweep's loop)
 ``write_wf(path, unk, ngrid, ...)``   io_write_module.f90:19 (simple_wf_io_write)
 ``read_wf(path, unk, ngrid, ...)``    io_read_module.f90:15 (simple_wf_io_read)
+``write_vrho(path, ngrid, ...)``      io_module.f90:97 (write_data, density/potentials)
+``read_vrho(path, ngrid, ...)``       io_module.f90:283 (read_data, VRHO branch)
 ====================================  ==========================================
 
 The reference routines read module state (``unk``, ``Vloc``, the projector
@@ -152,6 +154,57 @@ def read_wf(path, unk, ngrid, *, mk=1, ms=1, io_ctrl=0, occ=None) -> dict:
     _lib.call("rsdft_gpu_read_wf", os.fsencode(path), _ptr(unk, name="unk"), ld, mb, mk, ms, io_ctrl, ng.ctypes.data,
               None if occ is None else occ.ctypes.data, info.ctypes.data)
     return dict(zip(HEADER_FIELDS, (int(v) for v in info)))
+
+
+def _field(a, n, name):
+    """Address of an ML * nspin field stored without gaps (host or device)."""
+    if a is None:
+        return None
+    size = a.numel() if _is_torch(a) else a.size
+    if size != n:
+        raise ValueError(f"{name}: {size} values, expected {n}")
+    if _is_torch(a) and a.dim() == 2 and a.shape[1] > 1 and a.stride(1) != a.shape[0]:
+        raise ValueError(f"{name}: columns must be stored without gaps")
+    return _ptr(a, name=name)
+
+
+def write_vrho(path, ngrid, rho, vloc, vh, vxc, *, aa=None, aa_atom=None, ki_atom=None, zn_atom=None,
+               efermi=0.0) -> None:
+    """The density/potential branch of write_data (io_module.f90:97-226) for
+    one process.  rho, vloc, vxc are (ML, nspin) Fortran-ordered (or (ML,) for
+    one spin), vh is (ML,); each a host array, a registered one or a device
+    tensor.  aa(3, 3) is the lattice, aa_atom(3, Natom) the fractional atom
+    positions, ki_atom(Natom) the element index of each atom (1-based, as in
+    the reference) and zn_atom(Nelement) the atomic numbers."""
+    ng = np.ascontiguousarray(ngrid, dtype=np.int32)
+    ml = int(np.prod(ng))
+    nspin = (rho.numel() if _is_torch(rho) else rho.size) // ml
+    aa = np.zeros((3, 3), order="F") if aa is None else _f64(aa, (3, 3), "aa")
+    aa_atom = np.zeros((3, 0), order="F") if aa_atom is None else np.asfortranarray(
+        np.asarray(aa_atom, dtype=np.float64).reshape(3, -1, order="F"))
+    natom = aa_atom.shape[1]
+    ki_atom = np.ones(natom, dtype=np.int32) if ki_atom is None else np.ascontiguousarray(ki_atom, dtype=np.int32)
+    zn_atom = np.zeros(0, dtype=np.int32) if zn_atom is None else np.ascontiguousarray(zn_atom, dtype=np.int32)
+    if ki_atom.size != natom:
+        raise ValueError(f"ki_atom: {ki_atom.size} values for {natom} atoms")
+    _lib.call("rsdft_gpu_write_vrho", os.fsencode(path), ng.ctypes.data, aa.ctypes.data, zn_atom.size, natom,
+              aa_atom.ctypes.data, ki_atom.ctypes.data, zn_atom.ctypes.data, float(efermi), nspin,
+              _field(rho, ml * nspin, "rho"), _field(vloc, ml * nspin, "vloc"), _field(vh, ml, "vh"),
+              _field(vxc, ml * nspin, "vxc"))
+
+
+def read_vrho(path, ngrid, *, rho=None, vloc=None, vh=None, vxc=None, nspin=1):
+    """The VRHO branch of read_data (io_module.f90:283-432) for one process:
+    fills the fields given (shapes as for write_vrho) by the file's LL2 map;
+    returns the file's Fermi energy (None for an unversioned file, which
+    holds none)."""
+    ng = np.ascontiguousarray(ngrid, dtype=np.int32)
+    ml = int(np.prod(ng))
+    ef = ctypes.c_double(np.nan)
+    _lib.call("rsdft_gpu_read_vrho", os.fsencode(path), ng.ctypes.data, nspin, _field(rho, ml * nspin, "rho"),
+              _field(vloc, ml * nspin, "vloc"), _field(vh, ml, "vh"), _field(vxc, ml * nspin, "vxc"),
+              ctypes.addressof(ef))
+    return None if np.isnan(ef.value) else ef.value
 
 
 class RsdftGpu:
@@ -343,6 +396,14 @@ class RsdftGpu:
     def read_wf(self, path, unk, *, io_ctrl=0, occ=None, mk=1, ms=1) -> dict:
         """read_wf on this context's grid (see the module function)."""
         return read_wf(path, unk, self.cell.ngrid, mk=mk, ms=ms, io_ctrl=io_ctrl, occ=occ)
+
+    def write_vrho(self, path, rho, vloc, vh, vxc, **kw) -> None:
+        """write_vrho on this context's grid (see the module function)."""
+        write_vrho(path, self.cell.ngrid, rho, vloc, vh, vxc, **kw)
+
+    def read_vrho(self, path, **kw):
+        """read_vrho on this context's grid (see the module function)."""
+        return read_vrho(path, self.cell.ngrid, **kw)
 
     # --------------------------------------------------------- composite
     def finalize_fp64(self, unk, esp, res) -> None:

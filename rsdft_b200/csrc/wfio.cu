@@ -417,3 +417,193 @@ extern "C" int rsdft_gpu_read_wf(const char* path, double* unk, long ld, int mb,
     if (b.dev) RS_CUDA(cudaStreamSynchronize(st));
     return RSDFT_OK;
 }
+
+
+// ----------------------------------------------------------------- vrho
+// RSDFT's density/potential file (vrho.dat1), one process.  Format
+// (write_data, io_module.f90:97-226; read back by read_data,
+// io_module.f90:283-432), sequential unformatted records as above:
+//   version (character(64) "version3.0, comment_length=64") |
+//   ML, ML1, ML2, ML3 | LL2(3, ML) | comment | aa(3, 3) | comment |
+//   Nelement, Natom | aa_atom(3, Natom) | ki_atom(Natom) | zn_atom(Nelement) |
+//   comment | efermi |
+//   then for s = 1..MSP: rho(:, s) | Vloc(:, s) | Vh (s = 1 only) | Vxc(:, s).
+// Files without the version record (the reference's older writer) hold no
+// comment, lattice, atom or Fermi records: the fields follow LL2.  The
+// reader places each value by the file's LL2 map, so a file written under
+// any grid-point order of the same grid reads back.
+
+namespace rsdft {
+namespace {
+
+std::vector<char> text64(const char* s) {
+    std::vector<char> t(64, ' ');
+    std::memcpy(t.data(), s, std::min<size_t>(64, std::strlen(s)));
+    return t;
+}
+
+// n doubles of a host array or of device memory (a registered array's
+// mirror, or a device pointer) into v.
+int fetch_field(const double* p, size_t n, std::vector<double>& v) {
+    void* d = nullptr;
+    const int r = resolve(p, n * sizeof(double), &d);
+    if (r < 0) return r;
+    v.resize(n);
+    if (!r) {
+        std::memcpy(v.data(), p, n * sizeof(double));
+        return RSDFT_OK;
+    }
+    RS_CHECK(require_init());
+    RS_CUDA(cudaMemcpyAsync(v.data(), d, n * sizeof(double), cudaMemcpyDeviceToHost, ctx().stream));
+    RS_CUDA(cudaStreamSynchronize(ctx().stream));
+    return RSDFT_OK;
+}
+
+// v into a host array or device memory at p.
+int store_field(double* p, const std::vector<double>& v) {
+    void* d = nullptr;
+    const int r = resolve(p, v.size() * sizeof(double), &d);
+    if (r < 0) return r;
+    if (!r) {
+        std::memcpy(p, v.data(), v.size() * sizeof(double));
+        return RSDFT_OK;
+    }
+    RS_CHECK(require_init());
+    RS_CUDA(cudaMemcpyAsync(d, v.data(), v.size() * sizeof(double), cudaMemcpyHostToDevice, ctx().stream));
+    RS_CUDA(cudaStreamSynchronize(ctx().stream));
+    return RSDFT_OK;
+}
+
+}  // namespace
+}  // namespace rsdft
+
+extern "C" int rsdft_gpu_write_vrho(const char* path, const int* ngrid, const double* aa, int nelement, int natom,
+                                    const double* aa_atom, const int* ki_atom, const int* zn_atom, double efermi,
+                                    int nspin, const double* rho, const double* vloc, const double* vh,
+                                    const double* vxc) {
+    RS_ENTRY();
+    if (!path || !ngrid || !aa || !rho || !vloc || !vh || !vxc || nspin < 1 || nelement < 0 || natom < 0 ||
+        (natom > 0 && (!aa_atom || !ki_atom)) || (nelement > 0 && !zn_atom)) {
+        set_error("write_vrho: NULL argument or bad counts");
+        return RSDFT_EINVAL;
+    }
+    const int n1 = ngrid[0], n2 = ngrid[1], n3 = ngrid[2];
+    if (n1 < 1 || n2 < 1 || n3 < 1) {
+        set_error("write_vrho: bad grid %d x %d x %d", n1, n2, n3);
+        return RSDFT_EINVAL;
+    }
+    const long ml = (long)n1 * n2 * n3;
+    std::vector<double> f_rho, f_vloc, f_vh, f_vxc;
+    RS_CHECK(fetch_field(rho, (size_t)ml * nspin, f_rho));
+    RS_CHECK(fetch_field(vloc, (size_t)ml * nspin, f_vloc));
+    RS_CHECK(fetch_field(vh, (size_t)ml, f_vh));
+    RS_CHECK(fetch_field(vxc, (size_t)ml * nspin, f_vxc));
+
+    File out;
+    RS_CHECK(out.open(path, "wb"));
+    RS_CHECK(write_values(out, text64("version3.0, comment_length=64")));
+    RS_CHECK(write_values(out, std::vector<int32_t>{(int32_t)ml, n1, n2, n3}));
+    std::vector<int32_t> ll2((size_t)3 * ml);
+    for (long i = 0; i < ml; ++i) {
+        ll2[3 * i] = (int32_t)(i % n1);
+        ll2[3 * i + 1] = (int32_t)((i / n1) % n2);
+        ll2[3 * i + 2] = (int32_t)(i / ((long)n1 * n2));
+    }
+    RS_CHECK(write_values(out, ll2));
+    RS_CHECK(write_values(out, text64("lattice aa(3,3)")));
+    RS_CHECK(write_values(out, std::vector<double>(aa, aa + 9)));
+    RS_CHECK(write_values(out, text64("atom: Nelement Natom / aa_atom / ki_atom /zn_atom")));
+    RS_CHECK(write_values(out, std::vector<int32_t>{nelement, natom}));
+    RS_CHECK(write_record(out, {{aa_atom, sizeof(double) * 3 * (size_t)natom}}));
+    RS_CHECK(write_record(out, {{ki_atom, sizeof(int32_t) * (size_t)natom}}));
+    RS_CHECK(write_record(out, {{zn_atom, sizeof(int32_t) * (size_t)nelement}}));
+    RS_CHECK(write_values(out, text64("Fermi energy")));
+    RS_CHECK(write_values(out, std::vector<double>{efermi}));
+    const size_t bytes = sizeof(double) * (size_t)ml;
+    for (int s = 0; s < nspin; ++s) {
+        const size_t o = (size_t)ml * s;
+        RS_CHECK(write_record(out, {{f_rho.data() + o, bytes}}));
+        RS_CHECK(write_record(out, {{f_vloc.data() + o, bytes}}));
+        if (s == 0) RS_CHECK(write_record(out, {{f_vh.data(), bytes}}));
+        RS_CHECK(write_record(out, {{f_vxc.data() + o, bytes}}));
+    }
+    return out.close();
+}
+
+extern "C" int rsdft_gpu_read_vrho(const char* path, const int* ngrid, int nspin, double* rho, double* vloc,
+                                   double* vh, double* vxc, double* efermi) {
+    RS_ENTRY();
+    if (!path || !ngrid || nspin < 1) {
+        set_error("read_vrho: NULL path/ngrid or bad nspin");
+        return RSDFT_EINVAL;
+    }
+    const int n1 = ngrid[0], n2 = ngrid[1], n3 = ngrid[2];
+    if (n1 < 1 || n2 < 1 || n3 < 1) {
+        set_error("read_vrho: bad grid %d x %d x %d", n1, n2, n3);
+        return RSDFT_EINVAL;
+    }
+    const long ml = (long)n1 * n2 * n3;
+    File in;
+    RS_CHECK(in.open(path, "rb"));
+    // the version record, if any (read_data, io_module.f90:288-296)
+    size_t len = 0;
+    RS_CHECK(record_head(in, &len, "first"));
+    const long body = ftell(in.f);
+    char head[7] = {0};
+    const bool versioned = len >= 7 && fread(head, 1, 7, in.f) == 7 && std::memcmp(head, "version", 7) == 0;
+    if (fseek(in.f, versioned ? body + (long)len : body - 4, SEEK_SET) != 0) {
+        set_error("'%s': seek failed in the first record", path);
+        return RSDFT_EINVAL;
+    }
+    if (versioned) RS_CHECK(record_tail(in, len, "version"));
+    int32_t dims[4];
+    RS_CHECK(read_record(in, dims, sizeof(dims), "grid size"));
+    if (dims[0] != ml || dims[1] != n1 || dims[2] != n2 || dims[3] != n3) {
+        set_error("read_vrho: '%s' holds a %d x %d x %d grid (ML %d); the caller's is %d x %d x %d", path, dims[1],
+                  dims[2], dims[3], dims[0], n1, n2, n3);
+        return RSDFT_EINVAL;
+    }
+    std::vector<int32_t> ll2((size_t)3 * ml);
+    RS_CHECK(read_record(in, ll2.data(), ll2.size() * sizeof(int32_t), "LL2"));
+    std::vector<long> dst((size_t)ml);
+    std::vector<char> seen((size_t)ml, 0);
+    for (long i = 0; i < ml; ++i) {
+        const int32_t i1 = ll2[3 * i], i2 = ll2[3 * i + 1], i3 = ll2[3 * i + 2];
+        if (i1 < 0 || i1 >= n1 || i2 < 0 || i2 >= n2 || i3 < 0 || i3 >= n3) {
+            set_error("read_vrho: '%s': LL2(:, %ld) = (%d, %d, %d) is off the grid", path, i + 1, i1, i2, i3);
+            return RSDFT_EINVAL;
+        }
+        dst[i] = i1 + (long)n1 * (i2 + (long)n2 * i3);
+        if (seen[dst[i]]++) {
+            set_error("read_vrho: '%s': LL2 lists grid point (%d, %d, %d) twice", path, i1, i2, i3);
+            return RSDFT_EINVAL;
+        }
+    }
+    double ef = 0.0;
+    if (versioned) {
+        for (const char* w :
+             {"lattice comment", "aa", "atom comment", "Nelement", "aa_atom", "ki_atom", "zn_atom", "Fermi comment"})
+            RS_CHECK(skip_record(in, w));
+        RS_CHECK(read_record(in, &ef, sizeof(ef), "efermi"));
+    }
+    std::vector<double> buf((size_t)ml), f_rho((size_t)ml * nspin), f_vloc((size_t)ml * nspin), f_vh((size_t)ml),
+        f_vxc((size_t)ml * nspin);
+    auto take = [&](std::vector<double>& f, size_t o, const char* what) -> int {
+        RS_CHECK(read_record(in, buf.data(), sizeof(double) * (size_t)ml, what));
+        for (long i = 0; i < ml; ++i) f[o + dst[i]] = buf[i];
+        return RSDFT_OK;
+    };
+    for (int s = 0; s < nspin; ++s) {
+        const size_t o = (size_t)ml * s;
+        RS_CHECK(take(f_rho, o, "rho"));
+        RS_CHECK(take(f_vloc, o, "Vloc"));
+        if (s == 0) RS_CHECK(take(f_vh, 0, "Vh"));
+        RS_CHECK(take(f_vxc, o, "Vxc"));
+    }
+    if (rho) RS_CHECK(store_field(rho, f_rho));
+    if (vloc) RS_CHECK(store_field(vloc, f_vloc));
+    if (vh) RS_CHECK(store_field(vh, f_vh));
+    if (vxc) RS_CHECK(store_field(vxc, f_vxc));
+    if (efermi && versioned) *efermi = ef;
+    return RSDFT_OK;
+}

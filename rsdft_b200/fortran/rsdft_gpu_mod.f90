@@ -44,7 +44,8 @@ MODULE rsdft_gpu_mod
             gpu_sync_to_device, gpu_hamiltonian, gpu_conjugate_gradient, gpu_gram_schmidt, gpu_subspace_diag, &
             gpu_subspace_mate_sl, gpu_subspace_solv_sl, gpu_subspace_rotv_sl, gpu_esp_calc, gpu_calc_force_ps_nloc2, &
             gpu_calc_density, gpu_wf_io_write, gpu_wf_io_read, gpu_calc_sweep, gpu_op_local, &
-            gpu_op_nonlocal_project, gpu_op_nonlocal_add, gpu_gram, gpu_overlap_cholesky, gpu_rr_reduced, gpu_rotate
+            gpu_op_nonlocal_project, gpu_op_nonlocal_add, gpu_gram, gpu_overlap_cholesky, gpu_rr_reduced, gpu_rotate, &
+            gpu_write_vrho, gpu_read_vrho
 
   integer(c_int), parameter, PUBLIC :: RSDFT_MODE_FP64 = 0, RSDFT_MODE_MIXED_BF16X3 = 1, &
                                        RSDFT_MODE_MIXED_TF32 = 2, RSDFT_MODE_MIXED_BF16X2 = 3
@@ -190,6 +191,19 @@ MODULE rsdft_gpu_mod
        integer(c_long), value :: ld
        integer(c_int), value :: mb, mk, ms, io_ctrl
      end function rsdft_gpu_read_wf
+     integer(c_int) function rsdft_gpu_write_vrho(path, ngrid, aa, nelement, natom, aa_atom, ki_atom, zn_atom, &
+          efermi, nspin, rho, vloc, vh, vxc) bind(C, name="rsdft_gpu_write_vrho")
+       import :: c_int, c_double, c_ptr
+       type(c_ptr), value :: path, ngrid, aa, aa_atom, ki_atom, zn_atom, rho, vloc, vh, vxc
+       integer(c_int), value :: nelement, natom, nspin
+       real(c_double), value :: efermi
+     end function rsdft_gpu_write_vrho
+     integer(c_int) function rsdft_gpu_read_vrho(path, ngrid, nspin, rho, vloc, vh, vxc, efermi) &
+          bind(C, name="rsdft_gpu_read_vrho")
+       import :: c_int, c_ptr
+       type(c_ptr), value :: path, ngrid, rho, vloc, vh, vxc, efermi
+       integer(c_int), value :: nspin
+     end function rsdft_gpu_read_vrho
      integer(c_int) function rsdft_gpu_op_local(s, tpsi, htpsi, ld, nb, z0, nz) bind(C, name="rsdft_gpu_op_local")
        import :: c_int, c_long, c_ptr
        integer(c_int), value :: s, nb, z0, nz
@@ -565,5 +579,44 @@ CONTAINS
                int(size(unk, 3), c_int), int(size(unk, 4), c_int), int(io_ctrl, c_int), c_loc(ng), c_loc(occ), &
                c_loc(info)), "wf_io_read")
   END SUBROUTINE gpu_wf_io_read
+
+  ! The density/potential branch of write_data (io_module.f90:97-226) for one
+  ! process: rho, Vloc, Vxc (ML, MSP) and Vh (ML) from the modules the
+  ! reference writer reads (host arrays or registered ones, whose device
+  ! mirrors are written), with the lattice, atoms and Fermi energy.
+  SUBROUTINE gpu_write_vrho(file_vrho, ngrid, aa, aa_atom, ki_atom, zn_atom, efermi, rho, vloc, vh, vxc)
+    character(*), intent(IN) :: file_vrho
+    integer, intent(IN) :: ngrid(3), ki_atom(:), zn_atom(:)
+    real(8), intent(IN) :: aa(3, 3), efermi
+    real(8), intent(IN), target :: aa_atom(:, :), rho(:, :), vloc(:, :), vh(:), vxc(:, :)
+    character(kind=c_char), allocatable, target :: cpath(:)
+    integer(c_int), target :: ng(3)
+    integer(c_int), allocatable, target :: ki(:), zn(:)
+    real(c_double), target :: a(3, 3)
+    ng = ngrid
+    a = aa
+    ki = ki_atom
+    zn = zn_atom
+    call c_path(file_vrho, cpath)
+    call check(rsdft_gpu_write_vrho(c_loc(cpath), c_loc(ng), c_loc(a), int(size(zn), c_int), int(size(ki), c_int), &
+               c_loc(aa_atom), c_loc(ki), c_loc(zn), real(efermi, c_double), int(size(rho, 2), c_int), &
+               c_loc(rho), c_loc(vloc), c_loc(vh), c_loc(vxc)), "write_vrho")
+  END SUBROUTINE gpu_write_vrho
+
+  ! The VRHO branch of read_data (io_module.f90:283-432) for one process:
+  ! fills rho, Vloc, Vxc (ML, MSP) and Vh (ML) through the file's LL2 map;
+  ! efermi is set from a versioned file and left as it is otherwise.
+  SUBROUTINE gpu_read_vrho(file_vrho, ngrid, rho, vloc, vh, vxc, efermi)
+    character(*), intent(IN) :: file_vrho
+    integer, intent(IN) :: ngrid(3)
+    real(8), intent(INOUT), target :: rho(:, :), vloc(:, :), vh(:), vxc(:, :)
+    real(8), intent(INOUT), target :: efermi
+    character(kind=c_char), allocatable, target :: cpath(:)
+    integer(c_int), target :: ng(3)
+    ng = ngrid
+    call c_path(file_vrho, cpath)
+    call check(rsdft_gpu_read_vrho(c_loc(cpath), c_loc(ng), int(size(rho, 2), c_int), c_loc(rho), c_loc(vloc), &
+               c_loc(vh), c_loc(vxc), c_loc(efermi)), "read_vrho")
+  END SUBROUTINE gpu_read_vrho
 
 END MODULE rsdft_gpu_mod

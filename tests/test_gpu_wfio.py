@@ -55,3 +55,32 @@ def test_registered_array_uses_its_mirror(gpu, tmp_path):
         assert np.array_equal(host, other)
     finally:
         gpu.unregister_wf(host)
+
+
+def test_vrho_from_device_fields(gpu, tmp_path):
+    """The density/potential file from device tensors equals the one from
+    host arrays, and reading fills device tensors (format checked on the CPU
+    in tests/test_vrho.py)."""
+    import torch
+
+    rng = np.random.default_rng(21)
+    host = [np.asfortranarray(rng.standard_normal((ML, 2))) for _ in range(3)] + [rng.standard_normal(ML)]
+    rho, vloc, vxc, vh = host
+
+    def to_dev(a):
+        if a.ndim == 1:
+            return torch.from_numpy(a).cuda()
+        d = api.fortran_empty(ML, a.shape[1])
+        d.copy_(torch.from_numpy(np.ascontiguousarray(a.T)).t())
+        return d
+
+    kw = dict(aa=np.diag([10.26] * 3), aa_atom=np.full((3, 2), 0.25), ki_atom=[1, 1], zn_atom=[14], efermi=0.3)
+    api.write_vrho(tmp_path / "h.dat1", NG, rho, vloc, vh, vxc, **kw)
+    api.write_vrho(tmp_path / "d.dat1", NG, *(to_dev(a) for a in (rho, vloc, vh, vxc)), **kw)
+    assert (tmp_path / "d.dat1").read_bytes() == (tmp_path / "h.dat1").read_bytes()
+    back = [api.fortran_empty(ML, 2).zero_() for _ in range(3)] + [torch.zeros(ML, dtype=torch.float64, device="cuda")]
+    ef = api.read_vrho(tmp_path / "d.dat1", NG, rho=back[0], vloc=back[1], vxc=back[2], vh=back[3], nspin=2)
+    torch.cuda.synchronize()
+    assert ef == 0.3
+    for a, b in zip(host, back):
+        assert np.array_equal(b.cpu().numpy(), a)
