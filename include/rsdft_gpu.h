@@ -37,6 +37,7 @@ extern "C" {
 #define RSDFT_ENOMEM (-5)    /* device allocation failed */
 #define RSDFT_EUNSUP (-6)    /* unsupported option (k != 1, Md > 8, ...) */
 #define RSDFT_ETIMEOUT (-7)  /* a kernel's bounded wait ran out (reported at the next sync) */
+#define RSDFT_ECHECK (-8)    /* debug build: an in-kernel index check failed (reported at the next sync) */
 
 /* precision modes of the eigensolver entries; the name gives the operand
  * split of the tensor-core contractions (CG sweeps run in FP32 in every
@@ -57,7 +58,8 @@ const char *rsdft_gpu_last_error(void);
 /* Launch on this cudaStream_t from now on (NULL: the library's own stream). */
 int rsdft_gpu_set_stream(void *stream);
 /* Wait for the stream; reports RSDFT_ETIMEOUT if a kernel aborted on a
- * bounded wait since the last check. */
+ * bounded wait since the last check, RSDFT_ECHECK if (debug build) an
+ * in-kernel index check failed. */
 int rsdft_gpu_synchronize(void);
 /* Number of this library's own kernels launched since it was loaded
  * (diagnostics; library calls such as cuBLAS are not counted).  (no
@@ -73,6 +75,20 @@ long long rsdft_gpu_workspace_bytes(void);
  * the next rsdft_gpu_synchronize returns RSDFT_ETIMEOUT, later calls work.
  * (no reference counterpart: the reference stops the program on errors) */
 int rsdft_gpu_selftest_timeout(long long cycles);
+/* 1 if this library is the debug build (compiled with RSDFT_GPU_CHECK): the
+ * kernels that index memory through stored tables (nonlocal projection,
+ * scatter and force gathers) check every such index against its array and,
+ * where one is out of range, skip that access and record the check's site,
+ * the index and a count in the error word; the next rsdft_gpu_synchronize
+ * returns RSDFT_ECHECK and clears it.  0 for the normal build, whose kernels
+ * carry no checks.  (the role of the reference's -C bounds-checked build,
+ * make.inc.org:62,76) */
+int rsdft_gpu_checked_build(void);
+/* Debug-build self test: launch one kernel whose check of an index one past
+ * the end of an n-element device buffer fails (the access is skipped);
+ * the next rsdft_gpu_synchronize returns RSDFT_ECHECK, later calls work.
+ * RSDFT_EUNSUP in the normal build, which launches nothing. */
+int rsdft_gpu_selftest_check(void);
 
 /* Grid and FD kinetic coefficients: Ngrid(1:3), Md, coef_lap0, coef_lap(3,Md)
  * (axis-major: coef_lap[axis*Md + m-1]), Hgrid(1:3), ggg(1:3), dV.

@@ -2,7 +2,9 @@
 
 Importing this module never compiles anything; ``load()`` raises if the
 library has not been built (``python -m rsdft_b200.build``).  There is no CPU
-fallback.
+fallback.  With ``RSDFT_GPU_CHECK=1`` in the environment the debug build
+``librsdft_gpu_check.so`` (in-kernel index checks; ``python -m
+rsdft_b200.build --check``) is loaded instead.
 """
 from __future__ import annotations
 
@@ -10,7 +12,8 @@ import ctypes
 import os
 
 HERE = os.path.dirname(os.path.abspath(__file__))
-LIB_PATH = os.path.join(HERE, "librsdft_gpu.so")
+LIB_PATH = os.path.join(HERE, "librsdft_gpu_check.so" if os.environ.get("RSDFT_GPU_CHECK") == "1"
+                        else "librsdft_gpu.so")
 
 _c_int, _c_long, _c_double, _vp = ctypes.c_int, ctypes.c_long, ctypes.c_double, ctypes.c_void_p
 
@@ -24,6 +27,8 @@ SIGNATURES = {
     "rsdft_gpu_kernel_launches": (ctypes.c_longlong, []),
     "rsdft_gpu_workspace_bytes": (ctypes.c_longlong, []),
     "rsdft_gpu_selftest_timeout": (_c_int, [ctypes.c_longlong]),
+    "rsdft_gpu_checked_build": (_c_int, []),
+    "rsdft_gpu_selftest_check": (_c_int, []),
     "rsdft_gpu_set_grid": (_c_int, [_vp, _c_int, _c_double, _vp, _vp, _vp, _c_double]),
     "rsdft_gpu_set_vloc": (_c_int, [_vp, _c_long, _c_int]),
     "rsdft_gpu_set_nonlocal": (_c_int, [_c_int, _vp, _vp, _vp, _vp, _vp, _c_int, _vp]),
@@ -66,7 +71,7 @@ SIGNATURES = {
     "rsdft_gpu_read_vrho": (_c_int, [ctypes.c_char_p, _vp, _c_int, _vp, _vp, _vp, _vp, _vp]),
 }
 
-STATUS = {0: "OK", -1: "EINVAL", -2: "ENOTINIT", -3: "ECUDA", -4: "ESOLVER", -5: "ENOMEM", -6: "EUNSUP", -7: "ETIMEOUT"}
+STATUS = {0: "OK", -1: "EINVAL", -2: "ENOTINIT", -3: "ECUDA", -4: "ESOLVER", -5: "ENOMEM", -6: "EUNSUP", -7: "ETIMEOUT", -8: "ECHECK"}
 
 _lib = None
 

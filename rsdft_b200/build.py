@@ -4,7 +4,10 @@
 ``-gencode arch=compute_100a,code=sm_100a`` into ``rsdft_b200/_build`` and
 links the shared library in-tree (``rsdft_b200/librsdft_gpu.so``) against
 cuSOLVER.  Objects are rebuilt when their source or a header is
-newer.
+newer.  ``build(check=True)`` (``python -m rsdft_b200.build --check``) makes
+the debug build ``librsdft_gpu_check.so`` with ``-DRSDFT_GPU_CHECK`` (in-kernel
+index checks; objects under ``rsdft_b200/_build_check``), which
+``rsdft_b200._lib`` loads when ``RSDFT_GPU_CHECK=1`` is set.
 """
 from __future__ import annotations
 
@@ -20,6 +23,7 @@ ROOT = os.path.dirname(HERE)
 CSRC = os.path.join(HERE, "csrc")
 BUILD = os.path.join(HERE, "_build")
 LIB = os.path.join(HERE, "librsdft_gpu.so")
+LIB_CHECK = os.path.join(HERE, "librsdft_gpu_check.so")
 INCLUDE = os.path.join(ROOT, "include")
 
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
@@ -55,21 +59,22 @@ def _stale(obj: str, src: str) -> bool:
     return any(os.path.getmtime(d) > t for d in [src] + _headers())
 
 
-def build(verbose: bool = False, extra_flags=None) -> str:
+def build(verbose: bool = False, extra_flags=None, check: bool = False) -> str:
+    lib, objdir = (LIB_CHECK, BUILD + "_check") if check else (LIB, BUILD)
     srcs = sorted(glob.glob(os.path.join(CSRC, "*.cu")))
-    if not extra_flags and os.path.exists(LIB):
+    if not extra_flags and os.path.exists(lib):
         # the linked library is newer than every source and header: nothing
         # to do, even where the object files did not travel with it
-        t = os.path.getmtime(LIB)
+        t = os.path.getmtime(lib)
         if all(os.path.getmtime(d) <= t for d in srcs + _headers()):
-            return LIB
-    os.makedirs(BUILD, exist_ok=True)
+            return lib
+    os.makedirs(objdir, exist_ok=True)
     nvcc = _nvcc()
-    flags = NVCC_FLAGS + list(extra_flags or [])
+    flags = NVCC_FLAGS + (["-DRSDFT_GPU_CHECK"] if check else []) + list(extra_flags or [])
     jobs = []
     objs = []
     for s in srcs:
-        o = os.path.join(BUILD, os.path.basename(s)[:-3] + ".o")
+        o = os.path.join(objdir, os.path.basename(s)[:-3] + ".o")
         objs.append(o)
         if _stale(o, s):
             jobs.append([nvcc, *ARCH, *flags, "-c", s, "-o", o])
@@ -85,13 +90,13 @@ def build(verbose: bool = False, extra_flags=None) -> str:
 
     with cf.ThreadPoolExecutor(max_workers=max(1, min(len(jobs), os.cpu_count() or 4))) as ex:
         list(ex.map(run, jobs))
-    if jobs or not os.path.exists(LIB) or any(os.path.getmtime(o) > os.path.getmtime(LIB) for o in objs):
+    if jobs or not os.path.exists(lib) or any(os.path.getmtime(o) > os.path.getmtime(lib) for o in objs):
         libdir = _cuda_lib_dir()
-        link = [nvcc, *ARCH, "-shared", "-o", LIB, *objs, "-L", libdir, "-lcusolver",
+        link = [nvcc, *ARCH, "-shared", "-o", lib, *objs, "-L", libdir, "-lcusolver",
                 "-Xlinker", "-rpath=" + libdir]
         run(link)
-    return LIB
+    return lib
 
 
 if __name__ == "__main__":
-    print(build(verbose="-v" in sys.argv))
+    print(build(verbose="-v" in sys.argv, check="--check" in sys.argv))

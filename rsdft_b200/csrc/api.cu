@@ -319,12 +319,16 @@ int rsdft_gpu_synchronize(void) {
     RS_ENTRY();
     RS_CHECK(require_init());
     RS_CUDA(cudaStreamSynchronize(g_ctx.stream));
-    int flag = 0;
-    RS_CUDA(cudaMemcpy(&flag, g_ctx.err_flag, sizeof(int), cudaMemcpyDeviceToHost));
-    if (flag) {
-        RS_CUDA(cudaMemset(g_ctx.err_flag, 0, sizeof(int)));
-        set_error("a kernel's bounded wait for a bulk copy ran out (code %d)", flag);
+    int word[4] = {0, 0, 0, 0};
+    RS_CUDA(cudaMemcpy(word, g_ctx.err_flag, sizeof(word), cudaMemcpyDeviceToHost));
+    if (word[0] || word[1]) RS_CUDA(cudaMemset(g_ctx.err_flag, 0, sizeof(word)));
+    if (word[0]) {
+        set_error("a kernel's bounded wait for a bulk copy ran out (code %d)", word[0]);
         return RSDFT_ETIMEOUT;
+    }
+    if (word[1]) {
+        set_error("in-kernel index check failed: site %d, index %d (%d failed checks)", word[1], word[2], word[3]);
+        return RSDFT_ECHECK;
     }
     return RSDFT_OK;
 }

@@ -65,7 +65,10 @@ struct Context {
     cudaEvent_t ev[NEV] = {};
     cusolverDnHandle_t solver = nullptr;
     int num_sms = 0;
-    int* err_flag = nullptr;  // set by kernels whose bounded waits ran out
+    // error word (4 ints): [0] code of a bounded wait that ran out; debug
+    // build: [1] site of the first failed index check, [2] its index, [3]
+    // the number of failed checks
+    int* err_flag = nullptr;
 
     // grid
     bool grid_set = false;
@@ -160,6 +163,31 @@ const char* get_error();
             return RSDFT_ECUDA;                                                       \
         }                                                                             \
     } while (0)
+
+// In-kernel index checks of the debug build (-DRSDFT_GPU_CHECK).  A check
+// that fails records its site (first failure only), the index and a count in
+// the context's error word and yields false, so the caller skips the access;
+// rsdft_gpu_synchronize then reports RSDFT_ECHECK.  In the normal build a
+// check is the constant true and the compiler removes it.
+enum CheckSite : int {
+    CK_NL_PROJECT_POINT = 1,  // k_nl_project: grid point of a sphere entry
+    CK_NL_SCATTER_POINT = 2,  // k_nl_scatter: grid point of a scatter row
+    CK_NL_SCATTER_GROUP = 3,  // k_nl_scatter: projector group of an entry
+    CK_NL_GRAD_POINT = 4,     // k_nl_grad: grid point of a sphere entry
+    CK_SELFTEST = 99,         // rsdft_gpu_selftest_check
+};
+
+#ifdef RSDFT_GPU_CHECK
+__device__ __forceinline__ bool dev_check(bool ok, int site, long idx, int* err) {
+    if (ok) return true;
+    if (atomicCAS(err + 1, 0, site) == 0) atomicExch(err + 2, (int)idx);
+    atomicAdd(err + 3, 1);
+    return false;
+}
+#define RS_DCHECK(ok, site, idx, err) ::rsdft::dev_check((ok), (site), (long)(idx), (err))
+#else
+#define RS_DCHECK(ok, site, idx, err) ((void)(err), true)
+#endif
 
 // Number of this library's kernel launches since load (diagnostics).
 extern long long g_kernel_launches;

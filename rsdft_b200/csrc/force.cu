@@ -29,7 +29,7 @@ __global__ void __launch_bounds__(FW * 32) k_nl_grad(const double* __restrict__ 
                                                      const int* __restrict__ lma_ptr, const int* __restrict__ jjp,
                                                      const double* __restrict__ uv, const double* __restrict__ duv,
                                                      const int* __restrict__ iuv, double dV,
-                                                     double* __restrict__ out) {
+                                                     double* __restrict__ out, int* __restrict__ err) {
     __shared__ double sh[FW][4][3];
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int g = blockIdx.x;
@@ -59,6 +59,7 @@ __global__ void __launch_bounds__(FW * 32) k_nl_grad(const double* __restrict__ 
         }
         for (int j = lane; j < n; j += 32) {
             const int jj = jjp[js + j];
+            if (!RS_DCHECK(jj >= 0 && jj < ld, CK_NL_GRAD_POINT, jj, err)) continue;
             const double v = __ldg(p + jj);
             const double xv = CHI ? __ldg(x + jj) : 0.0;
 #pragma unroll
@@ -178,10 +179,10 @@ static int nl_grad(const double* psi, const double* chi, long ld, int nb, const 
     RS_CHECK(atom_tables(&aptr, &alma));
     if (chi)
         launch(k_nl_grad<true>, c.ngroup, FW * 32, 0, c.stream, psi, chi, ld, nb, occ, cscale, c.grp_lma0, c.grp_cnt,
-                                                            c.lma_ptr, c.jjp, c.uv, c.duv, c.iuv, c.dV, per);
+                                                            c.lma_ptr, c.jjp, c.uv, c.duv, c.iuv, c.dV, per, c.err_flag);
     else
         launch(k_nl_grad<false>, c.ngroup, FW * 32, 0, c.stream, psi, chi, ld, nb, occ, cscale, c.grp_lma0, c.grp_cnt,
-                                                             c.lma_ptr, c.jjp, c.uv, c.duv, c.iuv, c.dV, per);
+                                                             c.lma_ptr, c.jjp, c.uv, c.duv, c.iuv, c.dV, per, c.err_flag);
     RS_LAUNCH();
     launch(k_atom_sum, div_up(c.natom * 3, 128), 128, 0, c.stream, per, aptr, alma, c.natom, f_dev);
     RS_LAUNCH();

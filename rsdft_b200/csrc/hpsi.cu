@@ -47,7 +47,7 @@ __global__ void __launch_bounds__(256) k_nl_project(const T* __restrict__ psi, l
                                                     const double* __restrict__ uv,
                                                     const int* __restrict__ iuv, double dV,
                                                     double* __restrict__ uvunk, int nzlma,
-                                                    const int* __restrict__ band_active) {
+                                                    const int* __restrict__ band_active, int* __restrict__ err) {
     __shared__ int s_j[PJ_CH];
     __shared__ double s_u[4][PJ_CH];
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -83,9 +83,10 @@ __global__ void __launch_bounds__(256) k_nl_project(const T* __restrict__ psi, l
 #pragma unroll 2
         for (int j = lane; j < m; j += 32) {
             const int jj = s_j[j];
+            const bool in = RS_DCHECK(jj >= 0 && jj < ld, CK_NL_PROJECT_POINT, jj, err);
             double v[PJ_BW];
 #pragma unroll
-            for (int w = 0; w < PJ_BW; ++w) v[w] = act[w] ? (double)__ldg(p[w] + jj) : 0.0;
+            for (int w = 0; w < PJ_BW; ++w) v[w] = act[w] && in ? (double)__ldg(p[w] + jj) : 0.0;
 #pragma unroll
             for (int q = 0; q < 4; ++q) {
                 if (q < cnt) {
@@ -118,7 +119,7 @@ static int launch_project(const T* psi, long ld, int nb, double* uvunk, const in
     const Context& c = ctx();
     dim3 grid(c.ngroup, div_up(nb, PJ_WARPS * PJ_BW));
     launch(k_nl_project<T>, grid, 256, 0, st, psi, ld, nb, c.grp_lma0, c.grp_cnt, c.lma_ptr, c.jjp, c.uv, c.iuv,
-           c.dV, uvunk, c.nzlma, band_active);
+           c.dV, uvunk, c.nzlma, band_active, c.err_flag);
     RS_LAUNCH();
     return RSDFT_OK;
 }
@@ -545,10 +546,12 @@ __global__ void __launch_bounds__(128) k_nl_scatter(T* __restrict__ hpsi, long l
                                                    const int* __restrict__ nl_pts, const int* __restrict__ nl_ptr,
                                                    int npt, const int* __restrict__ gpt_grp,
                                                    const T* __restrict__ gpt_uv4, const double* __restrict__ uvunk,
-                                                   int nzlma, const int* __restrict__ band_active) {
+                                                   int nzlma, const int* __restrict__ band_active,
+                                                   int* __restrict__ err) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= npt) return;
     const int p = nl_pts[i];
+    if (!RS_DCHECK(p >= 0 && p < ld, CK_NL_SCATTER_POINT, p, err)) return;
     const int e0 = nl_ptr[i], e1 = nl_ptr[i + 1];
     const int b0 = blockIdx.y * bchunk, b1 = min(nb, b0 + bchunk);
     for (int b = b0; b < b1; b += SC_BU) {
@@ -564,6 +567,7 @@ __global__ void __launch_bounds__(128) k_nl_scatter(T* __restrict__ hpsi, long l
             // a group holds 1..4 projectors; missing ones have zero values
             // and must not be read past the end of uVunk
             const int g = __ldg(gpt_grp + e);
+            if (!RS_DCHECK(g >= 0 && g < nzlma, CK_NL_SCATTER_GROUP, g, err)) continue;
             T uq[4];
 #pragma unroll
             for (int q = 0; q < 4; ++q) uq[q] = __ldg(gpt_uv4 + 4L * e + q);
@@ -696,7 +700,8 @@ static int launch_stencil_md2(StencilArgs<T> a, const StencilCoef& cf, int nb, c
             constexpr int BCH = 32;
             dim3 grid(div_up(c.nl_npt, 128), div_up(nb, BCH));
             launch(k_nl_scatter<T>, grid, 128, 0, st, a.hpsi, a.ld, nb, BCH, (const int*)c.nl_pts,
-                   (const int*)c.nl_ptr, c.nl_npt, a.gpt_grp, a.gpt_uv4, a.uvunk, a.nzlma, a.band_active);
+                   (const int*)c.nl_ptr, c.nl_npt, a.gpt_grp, a.gpt_uv4, a.uvunk, a.nzlma, a.band_active,
+                   c.err_flag);
             RS_LAUNCH();
         }
         return RSDFT_OK;
@@ -907,7 +912,8 @@ extern "C" int rsdft_gpu_op_nonlocal_add(const double* uvunk, double* htpsi, lon
     constexpr int BCH = 32;
     dim3 grid(div_up(c.nl_npt, 128), div_up(nb, BCH));
     launch(k_nl_scatter<double>, grid, 128, 0, c.stream, dh, ld, nb, BCH, (const int*)c.nl_pts, (const int*)c.nl_ptr,
-           c.nl_npt, (const int*)c.gpt_grp, (const double*)c.gpt_uv4, (const double*)du, c.nzlma, (const int*)nullptr);
+           c.nl_npt, (const int*)c.gpt_grp, (const double*)c.gpt_uv4, (const double*)du, c.nzlma, (const int*)nullptr,
+           c.err_flag);
     RS_LAUNCH();
     RS_CHECK(wf_release(htpsi, dh, ld, nb, sh));
     return RSDFT_OK;

@@ -40,6 +40,22 @@ def test_binding_table_matches_header():
     assert sorted(_lib.SIGNATURES) == declared()
 
 
+def test_debug_build_exports_the_same_entries(lib):
+    """The debug build (-DRSDFT_GPU_CHECK, in-kernel index checks) is built
+    beside the normal one, exports every declared entry and says which it is;
+    rsdft_gpu_checked_build touches no device."""
+    import ctypes
+
+    from rsdft_b200 import build
+
+    path = build.build(check=True)
+    dbg = ctypes.CDLL(path)
+    for n in declared():
+        assert hasattr(dbg, n), f"{n} missing from the debug build"
+    assert dbg.rsdft_gpu_checked_build() == 1
+    assert lib.rsdft_gpu_checked_build() == 0
+
+
 def test_calls_without_context_fail_cleanly(lib):
     L = _lib.load()
     rc = L.rsdft_gpu_hamiltonian(1, 1, None, None, 1, 10, 1, 1)
@@ -62,14 +78,15 @@ def test_init_reports_missing_device(lib):
 
 def test_every_entry_is_defined_once_and_opens_a_trace_range():
     """Each C-ABI entry is defined once in csrc and starts with RS_ENTRY() (an
-    NVTX range named after it), except the two plain getters."""
+    NVTX range named after it), except the plain getters."""
     import glob
 
     src = "".join(open(f).read() for f in sorted(glob.glob(os.path.join(ROOT, "rsdft_b200", "csrc", "*.cu"))))
     defs = re.findall(r'(?m)^(?:extern "C" )?(?:int|long long|const char\*) (rsdft_gpu_\w+)\([^)]*\)\s*\{\s*(\S+)', src)
     names = [n for n, _ in defs]
     assert sorted(names) == declared()
-    getters = {"rsdft_gpu_last_error", "rsdft_gpu_kernel_launches", "rsdft_gpu_workspace_bytes"}
+    getters = {"rsdft_gpu_last_error", "rsdft_gpu_kernel_launches", "rsdft_gpu_workspace_bytes",
+               "rsdft_gpu_checked_build"}
     for name, first in defs:
         if name not in getters:
             assert first == "RS_ENTRY();", f"{name} does not open with RS_ENTRY()"
