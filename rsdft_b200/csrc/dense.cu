@@ -79,12 +79,7 @@ static int check_info(int* dinfo, const char* what) {
 // S (nb x nb) = R^T R in place: the upper triangle becomes R
 // (check = false: the caller reads *dinfo back itself, with its next read)
 static int potrf_upper(double* S, int nb, int* dinfo, const char* what, bool check = true) {
-    Context& c = ctx();
-    int lwork = 0;
-    RS_SOLVER(cusolverDnDpotrf_bufferSize(c.solver, CUBLAS_FILL_MODE_UPPER, nb, S, nb, &lwork));
-    double* work = nullptr;
-    RS_CHECK(workspace_t("gs_potrf", (size_t)lwork + 1, &work));
-    RS_SOLVER(cusolverDnDpotrf(c.solver, CUBLAS_FILL_MODE_UPPER, nb, S, nb, work, lwork, dinfo));
+    RS_CHECK(potrf_upper_device(S, nb, dinfo));
     return check ? check_info(dinfo, what) : RSDFT_OK;
 }
 
@@ -145,17 +140,24 @@ __global__ void __launch_bounds__(32 * TI_W) k_trtri_rows(const double* __restri
     }
 }
 
-// R (upper triangle of S) -> R^-1 in place, the lower triangle zeroed
+// R (upper triangle of S) -> R^-1 in place, the lower triangle zeroed:
+// trtri_upper_device (staged columns, eight columns per reduction), or for
+// orders whose staged rows exceed shared memory the row-per-warp kernel above
 static int trtri_upper(double* S, int nb, int* dinfo, const char* what) {
     (void)dinfo;
     (void)what;
     Context& c = ctx();
     double* X = nullptr;
     RS_CHECK(workspace_t("gs_trtri_x", (size_t)nb * nb, &X));
-    const size_t smem = (size_t)(TI_W + 1) * nb * sizeof(double);
-    RS_CHECK(set_smem_optin((const void*)k_trtri_rows, (int)smem));
-    launch(k_trtri_rows, div_up(nb, TI_W), 32 * TI_W, smem, c.stream, (const double*)S, nb, X);
-    RS_LAUNCH();
+    const int r = trtri_upper_device(S, nb, X);
+    if (r == RSDFT_EUNSUP) {
+        const size_t smem = (size_t)(TI_W + 1) * nb * sizeof(double);
+        RS_CHECK(set_smem_optin((const void*)k_trtri_rows, (int)smem));
+        launch(k_trtri_rows, div_up(nb, TI_W), 32 * TI_W, smem, c.stream, (const double*)S, nb, X);
+        RS_LAUNCH();
+    } else if (r != RSDFT_OK) {
+        return r;
+    }
     RS_CUDA(cudaMemcpyAsync(S, X, sizeof(double) * (size_t)nb * nb, cudaMemcpyDeviceToDevice, c.stream));
     return RSDFT_OK;
 }

@@ -29,7 +29,7 @@
 //     steps Z <- Z (3 I - Z^T Z) / 2 (four DGEMMs) make the basis orthonormal
 //     to rounding; they mix vectors i, j by ~eps |T| / |l_i - l_j|, which
 //     moves the residuals by ~eps |T| only.
-//  3. cusolverDnDormtr applies Q to the eigenvectors of T.
+//  3. ormtr_lower_device (factor.cu) applies Q to the eigenvectors of T.
 //
 // cuSOLVER's one-stage syevd spends ~80 % of its time in sytrd for these
 // sizes (3.9 of 5.0 ms at n = 480 on B200), one short kernel per column;
@@ -38,6 +38,7 @@
 
 #include "common.cuh"
 #include "dmma.cuh"
+#include "cluster.cuh"
 #include "kernels.cuh"
 #include "tma.cuh"
 
@@ -47,50 +48,6 @@ constexpr int TD_C = 16;          // CTAs in the cluster
 constexpr int TD_T = 512;         // threads per CTA
 constexpr int TD_W = TD_T / 32;
 
-__device__ __forceinline__ uint32_t cluster_rank() {
-    uint32_t r;
-    asm volatile("mov.u32 %0, %%cluster_ctarank;" : "=r"(r));
-    return r;
-}
-
-// all threads of all CTAs of the cluster; orders shared-memory writes before
-// the barrier against reads after it, cluster-wide
-__device__ __forceinline__ void cluster_sync() {
-    asm volatile(
-        "barrier.cluster.arrive.release.aligned;\n"
-        "barrier.cluster.wait.acquire.aligned;\n" ::
-            : "memory");
-}
-
-// load of the double at the same shared-memory offset as p in CTA `rank`
-__device__ __forceinline__ double dsmem_ld(const double* p, uint32_t rank) {
-    const uint32_t a = (uint32_t)__cvta_generic_to_shared(p);
-    uint32_t r;
-    asm volatile("mapa.shared::cluster.u32 %0, %1, %2;" : "=r"(r) : "r"(a), "r"(rank));
-    double v;
-    asm volatile("ld.shared::cluster.f64 %0, [%1];" : "=d"(v) : "r"(r) : "memory");
-    return v;
-}
-
-__device__ __forceinline__ double warp_sum_d(double v) {
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
-    return v;
-}
-
-// 1/q for normal q by Newton-Raphson iteration for the reciprocal
-// (r <- r + r (1 - q r), quadratic convergence) from the PTX approximate
-// reciprocal: two steps take the ~2^-22 seed past double precision (checked
-// against 1/q on 7.6e7 samples spanning exponents +-1000: no difference).
-// A dependent IEEE division costs ~310 cycles on B200, this ~60, and the
-// serial chains below (Sturm counts, pivots, reflector scalars) are made of
-// them.
-__device__ __forceinline__ double rcp_nr(double q) {
-    double r;
-    asm("rcp.approx.ftz.f64 %0, %1;" : "=d"(r) : "d"(q));
-    r = fma(r, fma(-q, r, 1.0), r);
-    return fma(r, fma(-q, r, 1.0), r);
-}
 
 // Shared-memory layout of k_sytrd (doubles; every array an even count, so
 // each starts 16-byte aligned for the bulk copies): own rows R x np, the
@@ -697,7 +654,7 @@ int syevd_fast(double* A, int n, double* W, cublasFillMode_t uplo) {
     const size_t smem = td_smem_bytes(n);
     if (c.max_smem_optin < 0)
         RS_CUDA(cudaDeviceGetAttribute(&c.max_smem_optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, c.device));
-    if (smem > (size_t)c.max_smem_optin) return RSDFT_EUNSUP;
+    if (smem > (size_t)c.max_smem_optin || ormtr_smem_bytes(n) > (size_t)c.max_smem_optin) return RSDFT_EUNSUP;
     if ((int)smem > c.smem_optin[(const void*)k_sytrd]) {
         RS_CUDA(cudaFuncSetAttribute(k_sytrd, cudaFuncAttributeNonPortableClusterSizeAllowed, 1));
         RS_CHECK(set_smem_optin((const void*)k_sytrd, (int)smem));
@@ -723,12 +680,10 @@ int syevd_fast(double* A, int n, double* W, cublasFillMode_t uplo) {
     }
     if (c.sytrd_clusters < 1) return RSDFT_EUNSUP;
 
-    double *Q = nullptr, *dd = nullptr, *ws = nullptr, *work = nullptr;
-    int* dinfo = nullptr;
+    double *Q = nullptr, *dd = nullptr, *ws = nullptr;
     RS_CHECK(workspace_t("eig_Q", (size_t)n * n, &Q));
     RS_CHECK(workspace_t("eig_dd", (size_t)4 * n + 8, &dd));
     RS_CHECK(workspace_t("eig_ws", (size_t)2 * n * n, &ws));
-    RS_CHECK(workspace_t("eig_info", 4, &dinfo));
     double* d = dd;
     double* e = dd + n;
     double* tau = dd + 2 * n;
@@ -760,13 +715,7 @@ int syevd_fast(double* A, int n, double* W, cublasFillMode_t uplo) {
         }
         (void)src;  // two steps: the result is back in A
     }
-    int lwork = 0;
-    RS_SOLVER(cusolverDnDormtr_bufferSize(c.solver, CUBLAS_SIDE_LEFT, CUBLAS_FILL_MODE_LOWER, CUBLAS_OP_N, n, n, Q, n,
-                                          tau, A, n, &lwork));
-    RS_CHECK(workspace_t("eig_work", (size_t)lwork + 1, &work));
-    RS_SOLVER(cusolverDnDormtr(c.solver, CUBLAS_SIDE_LEFT, CUBLAS_FILL_MODE_LOWER, CUBLAS_OP_N, n, n, Q, n, tau, A, n,
-                               work, lwork, dinfo));
-    return RSDFT_OK;
+    return ormtr_lower_device(Q, tau, n, A);
 }
 
 }  // namespace rsdft

@@ -100,6 +100,23 @@ int orth_subspace_diag_f32(const float* x32, const float* h32, double* psi, long
 // available, so the caller takes cuSOLVER's syevd.
 int syevd_fast(double* A, int n, double* W, cublasFillMode_t uplo);
 
+// C (n x n, ld n) <- Q C for the Q of a lower Householder tridiagonalisation
+// (reflectors below the subdiagonal of Q's columns, scalars tau; LAPACK
+// dormtr with side 'L', uplo 'L', trans 'N'), factor.cu; the dynamic shared
+// memory it needs for n (RSDFT_EUNSUP above the device's limit).
+int ormtr_lower_device(const double* Q, const double* tau, int n, double* C);
+size_t ormtr_smem_bytes(int n);
+
+// S (n x n, column-major, ld n) = R^T R in place, R in the upper triangle
+// (LAPACK dpotrf, uplo 'U'; the strictly lower triangle untouched); dinfo
+// (device) receives dpotrf's info.  factor.cu.
+int potrf_upper_device(double* S, int n, int* dinfo);
+
+// X = R^-1 for the upper-triangular R (n x n, column-major, ld n; X's lower
+// triangle zero), factor.cu; RSDFT_EUNSUP when the staged rows do not fit
+// shared memory (n above ~1700).
+int trtri_upper_device(const double* R, int n, double* X);
+
 // CG over all bands (device data).  hx_out (FP64 only, if given) receives
 // the sweep's H x (in the CG workspace), or null when an update was rejected
 // and H x must be formed again.

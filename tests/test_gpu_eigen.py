@@ -68,7 +68,8 @@ def test_subspace_solv_repeatable(gpu):
     assert np.array_equal(w1, w2) and np.array_equal(v1, v2)
 
 
-@pytest.mark.parametrize("n,spread", [(1, 1.0), (37, 1.0), (480, 30.0), (600, 300.0)])
+@pytest.mark.parametrize("n,spread", [(1, 1.0), (31, 1.0), (32, 3.0), (33, 1.0), (37, 1.0), (64, 10.0), (97, 1.0),
+                                      (480, 30.0), (600, 300.0), (1088, 30.0)])
 def test_overlap_cholesky_inverse(gpu, n, spread):
     """rsdft_gpu_overlap_cholesky: S = R^T R and rinv = R^-1 (upper, the
     lower triangle zero) against LAPACK's Cholesky and an explicit inverse,
@@ -86,3 +87,24 @@ def test_overlap_cholesky_inverse(gpu, n, spread):
     assert np.abs(rinv @ r - np.eye(n)).max() <= 1e-12 * max(1.0, np.linalg.cond(r))
     d = np.diag(r)
     assert abs(kappa - (d.max() / d.min()) ** 2) <= 1e-12 * kappa
+
+
+@pytest.mark.parametrize("n,bad", [(8, 1), (100, 41), (480, 480), (130, 97)])
+def test_overlap_cholesky_reports_the_failing_pivot(gpu, n, bad):
+    """A matrix whose leading minor of order `bad` is the first not positive
+    definite: the Cholesky stops with dpotrf's info = bad, and the context
+    factors the next matrix normally."""
+    from rsdft_b200._lib import RsdftError
+
+    rng = np.random.default_rng(n + bad)
+    b = rng.standard_normal((2 * n, n))
+    s = b.T @ b / (2 * n)
+    r = np.linalg.cholesky(s).T  # s = r^T r; make pivot `bad` negative
+    r[bad - 1, bad - 1] = 0.0
+    s_bad = r.T @ r
+    s_bad[bad - 1, bad - 1] -= 0.5
+    rinv = np.zeros((n, n), order="F")
+    with pytest.raises(RsdftError, match=f"info={bad}"):
+        gpu.overlap_cholesky(np.asfortranarray(s_bad), rinv)
+    gpu.overlap_cholesky(np.asfortranarray(s), rinv)
+    assert np.abs(rinv @ np.linalg.cholesky(s).T - np.eye(n)).max() <= 1e-11
