@@ -119,7 +119,6 @@ struct Context {
     std::map<const void*, int> smem_optin;   // dynamic shared memory opted in, per kernel
     int max_smem_optin = -1;                 // device limit (cudaDevAttrMaxSharedMemoryPerBlockOptin)
     int sytrd_clusters = -1;                 // active 16-CTA clusters of the eigensolver kernel
-    int potrf_cluster = 0;                   // CTAs per cluster of the Cholesky kernel (0: not chosen yet)
     double* noalloc_scratch = nullptr;       // device address of the static scratch array
 };
 

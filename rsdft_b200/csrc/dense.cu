@@ -13,9 +13,9 @@
 // (subspace_mate_sl, subspace_solv_sl, subspace_rotv_sl).
 //
 // FP64 form: the Gram matrices and rotations on the FP64 tensor pipe
-// (dmma.cu), the overlap's Cholesky factor by cuSOLVER DPOTRF and its inverse
-// by k_trtri_rows, the eigensolve in eigen.cu (cuSOLVER DSYEVD only above its
-// shared-memory limit).  Mixed forms: the contractions go to the split-BF16 /
+// (dmma.cu), the overlap's Cholesky factor and its inverse by the tile-step
+// and staged-column kernels of factor.cu, the eigensolve in eigen.cu
+// (cuSOLVER DSYEVD only above its shared-memory limit).  Mixed forms: the contractions go to the split-BF16 /
 // split-TF32 tensor-core kernels of mixed.cu; FP64 stays in the Cholesky
 // factor, its inverse and the eigensolve.
 #include <algorithm>

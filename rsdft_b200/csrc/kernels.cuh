@@ -53,8 +53,8 @@ __device__ __forceinline__ void block_sum_n(double (&v)[K], double* sh) {
 }
 
 // Symmetric-positive-definite orthonormalisation (CholeskyQR2 in the dV
-// metric) of nb columns, FP64 (DMMA Gram and rotation, cuSOLVER Cholesky,
-// hand-written triangular inverse) or mixed (tcgen05 tensor cores).
+// metric) of nb columns, FP64 (DMMA Gram and rotation, the Cholesky factor
+// and its inverse by factor.cu) or mixed (tcgen05 tensor cores).
 int gram_schmidt_device(double* psi, long ld, int nb, int mode);
 
 // Rayleigh-Ritz (subspace_diag_la) on device data.
@@ -95,9 +95,10 @@ int orth_subspace_diag_f32(const float* x32, const float* h32, double* psi, long
 // Eigen-decomposition of the symmetric n x n A (column-major, ld n; the
 // `uplo` triangle is read): W ascending, A overwritten by the eigenvectors.
 // Cluster-resident tridiagonalisation + bisection / inverse iteration +
-// cuSOLVER ormtr; RSDFT_EUNSUP when n is outside its range (n < 3, or the
-// rows do not fit the cluster's shared memory) or 16-CTA clusters are not
-// available, so the caller takes cuSOLVER's syevd.
+// the compact-WY back-transformation of factor.cu; RSDFT_EUNSUP when n is
+// outside its range (n < 3, or the rows do not fit the cluster's shared
+// memory) or 16-CTA clusters are not available, so the caller takes
+// cuSOLVER's syevd.
 int syevd_fast(double* A, int n, double* W, cublasFillMode_t uplo);
 
 // C (n x n, ld n) <- Q C for the Q of a lower Householder tridiagonalisation
