@@ -163,10 +163,14 @@ __device__ int chol_tile_warp(double* T, int kk, double* dinv) {
             T[j * CF_P + lane] = rjl;
         }
         __syncwarp();
-        // the trailing triangle j < i <= l < kk: row by row, lane l on column l
+        // the trailing triangle j < i <= l < kk: row by row, lane l on column
+        // l; R(j, i) comes from lane i's register (a shuffle, not a shared
+        // load, so no shared-memory access orders the rows' updates)
 #pragma unroll 4
-        for (int i = j + 1; i < kk; ++i)
-            if (lane >= i && lane < kk) T[i * CF_P + lane] = fma(-T[j * CF_P + i], rjl, T[i * CF_P + lane]);
+        for (int i = j + 1; i < kk; ++i) {
+            const double rji = __shfl_sync(FULL, rjl, i);
+            if (lane >= i && lane < kk) T[i * CF_P + lane] = fma(-rji, rjl, T[i * CF_P + lane]);
+        }
         __syncwarp();
     }
     return 0;
@@ -174,7 +178,7 @@ __device__ int chol_tile_warp(double* T, int kk, double* dinv) {
 
 // X = R^-1 of the kk x kk upper factor in T (dinv = 1 / diag) by one warp,
 // row by row from the last: X(i, i) = dinv[i], X(i, l) = -(sum_{m=i+1}^{l}
-// R(i, m) X(m, l)) dinv[i] (l > i), lane l forming X(i, l) with two
+// R(i, m) X(m, l)) dinv[i] (l > i), lane l forming X(i, l) with four
 // partial sums; written to xs (pitch CF_P) and xg (32 x 32, row-major),
 // zero below the diagonal and outside kk.
 __device__ void inv_tile_warp(const double* T, int kk, const double* dinv, double* xs, double* __restrict__ xg) {
@@ -185,14 +189,16 @@ __device__ void inv_tile_warp(const double* T, int kk, const double* dinv, doubl
             if (i == l) {
                 x = dinv[i];
             } else {
-                double s0 = 0.0, s1 = 0.0;
+                double s0 = 0.0, s1 = 0.0, s2 = 0.0, s3 = 0.0;
                 int m = i + 1;
-                for (; m + 1 <= l; m += 2) {
+                for (; m + 3 <= l; m += 4) {
                     s0 = fma(T[i * CF_P + m], xs[m * CF_P + l], s0);
                     s1 = fma(T[i * CF_P + m + 1], xs[(m + 1) * CF_P + l], s1);
+                    s2 = fma(T[i * CF_P + m + 2], xs[(m + 2) * CF_P + l], s2);
+                    s3 = fma(T[i * CF_P + m + 3], xs[(m + 3) * CF_P + l], s3);
                 }
-                if (m <= l) s0 = fma(T[i * CF_P + m], xs[m * CF_P + l], s0);
-                x = -(s0 + s1) * dinv[i];
+                for (; m <= l; ++m) s0 = fma(T[i * CF_P + m], xs[m * CF_P + l], s0);
+                x = -((s0 + s1) + (s2 + s3)) * dinv[i];
             }
         }
         xs[i * CF_P + l] = x;
