@@ -20,11 +20,12 @@
 //    it needs, R(k, i) = X^T S(k, i) with X = R(k, k)^-1 published by the
 //    step before (so no CTA waits on another), and subtracts R(k, i)^T
 //    R(k, j) from S(i, j).  The CTA of (k+1, k+1) keeps its updated tile,
-//    factors it by one warp in dpotf2's order (r = sqrt(d), the row scaled
-//    by 1 / r; 1 / sqrt(d) by Newton-Raphson) and inverts the factor for the next step.  The panels go to a
-//    side buffer (S's row block k is still being read during step k) and
-//    into S at the end.  A pivot that is not positive (or NaN) sets info to
-//    its 1-based index as dpotrf does, and the later launches stop.
+//    factors it by one warp in dpotf2's order (r = d times 1 / sqrt(d),
+//    the row scaled by 1 / r, 1 / sqrt(d) by Newton-Raphson) and inverts
+//    the factor for the next step.  The panels go to a side buffer (S's row
+//    block k is still being read during step k) and into S at the end.  A
+//    pivot that is not positive (or NaN) sets info to its 1-based index as
+//    dpotrf does, and the later launches stop.
 //  ormtr_lower_device: C <- Q C for Q = H(0) H(1) ... H(n-2) of the lower
 //    Householder tridiagonalisation (LAPACK dormtr with side 'L', uplo 'L',
 //    trans 'N'; H(i) = I - tau_i v_i v_i^T, v_i(i+1) = 1 and v_i(i+2:n-1)
@@ -34,14 +35,13 @@
 //    columns of C (one per warp) and applies the blocks from the last to the
 //    first: the block's V staged in shared memory once (cp.async), W = V^T c
 //    (a butterfly reduce-transpose over the lanes), W <- T W, c -= V W.
-#include "cluster.cuh"
 #include "common.cuh"
 #include "kernels.cuh"
 
 namespace rsdft {
 
 constexpr unsigned FULL = 0xffffffffu;
-constexpr int CF_P = 33;  // shared-memory pitch of k_larft's 32-column tiles (doubles)
+constexpr int CF_P = 33;  // shared-memory pitch of the 32-column tiles (doubles)
 
 // 8-byte global -> shared copy, asynchronous (completed by cp_async_wait)
 __device__ __forceinline__ void cp_async8(double* dst, const double* src) {
